@@ -1,0 +1,170 @@
+/* swl_b200 -- B200-native curvilinear velocity-stress engine, C ABI.
+ *
+ * Drop-in compute backend for SeisWave Lab (Curvilinear).  Two levels:
+ *
+ *  - Engine level: replaces the reference's private CUDA engines.  The caller builds the
+ *    model arrays exactly as the reference's Simulation::initialize does and hands them
+ *    over as a mesh; the engine copies them to the GPU and advances RK4 steps there.
+ *      2D: Seis2D::Curvilinear::CudaEngine        (src/two_d/CudaEngine2D.hpp:5-24)
+ *      3D: Seis3D::Curvilinear::CudaEngine3D      (src/three_d/CudaEngine3D.hpp:7-24)
+ *  - Session level: the whole Simulation (model build from parameters, dt plan, receivers,
+ *    records, fault policy) with the engine underneath.
+ *      2D: Seis2D::Curvilinear::Simulation        (include/Seis2D/CurvilinearSolver2D.hpp:93-123)
+ *      3D: Seis3D::Curvilinear::ISimulationBackend3D (include/Seis3D/CurvilinearSolver.hpp:165-185)
+ *
+ * Conventions: every call returns an swl_status (0 = success) and never throws across this
+ * boundary; the message of the last failure on the calling thread is available from
+ * swl_last_error().  A failed step leaves a sticky fault (the reference's `fault` string)
+ * that only reset or rebuild clears.  An engine is driven by one thread at a time.
+ * Arrays are padded (ghost width 3), x fastest, structure of arrays.
+ */
+#ifndef SWL_B200_H
+#define SWL_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t swl_status;
+enum {
+    SWL_OK = 0,
+    SWL_ERR_INVALID = -1,     /* bad argument or configuration */
+    SWL_ERR_CUDA = -2,        /* CUDA runtime failure (message names the action) */
+    SWL_ERR_MEMORY = -3,      /* allocation refused or over the memory budget */
+    SWL_ERR_FAULT = -4,       /* step rejected (non-finite or energy growth); sticky */
+    SWL_ERR_UNAVAILABLE = -5, /* no usable sm_100 device */
+    SWL_ERR_STATE = -6        /* call out of order, or refused while an earlier rejected step is held */
+};
+enum { SWL_FP64 = 0, SWL_FP32 = 1 };
+
+/* Message of the last failed call on this thread ("" when none). */
+const char *swl_last_error(void);
+/* Library version string. */
+const char *swl_version(void);
+/* Number of usable sm_100 devices (0 when none); mirrors queryBackend3D
+ * (src/common/ComputeDevices.cpp:98-102). */
+int32_t swl_device_count(void);
+
+/* ---------------------------------------------------------------- engine, 2D ---- */
+
+/* POD mirror of Point::MeshT<Real> (src/two_d/PointKernels2D.hpp:14-27).  `array_precision`
+ * says whether the pointers reference double or float arrays (the reference converts its
+ * StoredArrays before building the mesh); `precision` selects the compute precision.
+ * Non-owning: the engine copies everything at create. */
+typedef struct swl_mesh2d {
+    int32_t nx, nz;  /* padded node counts (computational + 6) */
+    int64_t count;   /* nx * nz */
+    double h;
+    const void *a, *b, *jac, *normals, *lambda, *mu, *rho, *source, *damping;
+    double source_direction[3];
+    const void *source_gradient[2]; /* both null for a directional force */
+    int32_t mechanisms, field_count; /* GSLS mechanisms 0..3; 5 or 6+4*mechanisms fields */
+    const void *cpml_x, *cpml_z;     /* (d, kappa, alpha) per computational node, or null */
+    int32_t cpml_width_x, cpml_width_z;
+    int64_t cpml_count;              /* compact ADE scalars, 0 without CFS-PML */
+    double rates[3];
+    const void *delta_p[3], *delta_s[3];
+    int32_t precision, array_precision;
+} swl_mesh2d;
+
+/* Per-step diagnostics, mirror of the GPU-relevant part of Diagnostics
+ * (include/Seis2D/CurvilinearSolver2D.hpp:75-86). */
+typedef struct swl_diag2d {
+    double energy, peak_energy, max_velocity, traction_relative;
+    int32_t finite;
+    int32_t rhs_registers;
+    int64_t rhs_local_bytes;
+    int64_t resident_bytes;
+} swl_diag2d;
+
+typedef struct swl2d_engine swl2d_engine;
+
+/* CudaEngine::CudaEngine(mesh, receivers, device) (src/two_d/CudaEngine2D.cu:127-142).
+ * receiver_nodes are padded node indices (i + nx*k).  device < 0 picks the device with
+ * the most memory. */
+swl_status swl2d_create(const swl_mesh2d *mesh, const int64_t *receiver_nodes, int32_t n_receivers, int32_t device,
+                        swl2d_engine **out);
+void swl2d_destroy(swl2d_engine *engine);
+
+/* CudaEngine::step(time, dt, frequency, scale, step) (src/two_d/CudaEngine2D.cu:143-152):
+ * one accepted classic-RK4 step; the Ricker force scale*ricker(t) is evaluated at
+ * step*dt, (step+0.5)*dt and (step+1)*dt as the reference CPU driver does.  The previous
+ * state stays resident for swl2d_rollback.  Asynchronous. */
+swl_status swl2d_step(swl2d_engine *engine, double time, double dt, double frequency, double scale, int32_t step);
+
+/* Batched form of `count` calls to step + diagnostics + sample: steps first..first+count-1
+ * run from a CUDA graph; after every step the device checks finiteness and the late energy
+ * growth rule of Simulation::advance (src/two_d/CurvilinearSolver2D.cpp:576-590) and, on a
+ * failure, stops advancing and keeps the failed step's starting state.  Receiver samples go
+ * to a device trace buffer read with swl2d_traces.  Returns SWL_ERR_FAULT when a step was
+ * rejected; *accepted receives the number of accepted steps.  check_growth_after is the
+ * time (s) after which the 1e4 x peak energy rule applies (3/f in the reference). */
+swl_status swl2d_advance(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
+                         double scale, double check_growth_after, int32_t *accepted);
+
+swl_status swl2d_rollback(swl2d_engine *engine);    /* CudaEngine::rollback */
+swl_status swl2d_reset(swl2d_engine *engine);       /* CudaEngine::reset: zero fields, memories, traces */
+swl_status swl2d_diagnostics(swl2d_engine *engine, swl_diag2d *out); /* CudaEngine::diagnostics */
+/* CudaEngine::sample: Vx, Vz of the current state at every receiver (FP64). */
+swl_status swl2d_sample(swl2d_engine *engine, double *vx, double *vz);
+/* Raw per-step receiver samples recorded by swl2d_advance for steps
+ * [first, first+count) of the current run: receivers x count, row-major. */
+swl_status swl2d_traces(swl2d_engine *engine, int32_t first, int32_t count, double *vx, double *vz);
+/* Whole padded field `field` (0..field_count-1) of the current state, as FP64; field -1
+ * reads the compact CFS-PML memories (cpml_count values).  CudaEngine::snapshot. */
+swl_status swl2d_snapshot(swl2d_engine *engine, int32_t field, double *out);
+/* Overwrite field `field` (or -1: memories) of the current state from FP64 values. */
+swl_status swl2d_load_field(swl2d_engine *engine, int32_t field, const double *values);
+/* CudaEngine::probes: Vx, Vz, Sxx, Szz, Sxz at padded node indices, 5 per node. */
+swl_status swl2d_probes(swl2d_engine *engine, const int64_t *nodes, int32_t n, double *out5);
+int64_t swl2d_resident_bytes(const swl2d_engine *engine);
+
+/* ---------------------------------------------------------------- engine, 3D ---- */
+
+/* POD mirror of Seis3D::Curvilinear::Point::Mesh (src/three_d/PointKernels3D.hpp:13-21),
+ * FP64 arrays; `precision` selects the compute precision of the engine. */
+typedef struct swl_mesh3d {
+    int32_t nx, ny, nz;
+    int64_t count;
+    double h, lambda, mu, density;
+    const double *metrics;  /* 9 per node: d(xi,eta,zeta)/d(x,y,z) rows */
+    const double *normals;  /* 3 per node (surface row used) */
+    const double *jacobian, *source, *damping;
+    const double *material_lambda, *material_mu, *material_density; /* null for uniform */
+    double source_direction[3], source_amplitude;
+    const double *source_gradient[3];
+    int32_t precision;
+} swl_mesh3d;
+
+typedef struct swl_diag3d {
+    double energy, peak_energy, max_velocity, traction_rate_relative;
+    double peaks[5]; /* |Vz|, |Vx|, |Vy|, |V|, |mean stress| */
+    int32_t finite;
+    int32_t rhs_registers;
+    int64_t resident_bytes;
+} swl_diag3d;
+
+typedef struct swl3d_engine swl3d_engine;
+
+/* CudaEngine3D::CudaEngine3D(mesh, receivers, device) (src/three_d/CudaEngine3D.cu:80-103). */
+swl_status swl3d_create(const swl_mesh3d *mesh, const int64_t *receiver_nodes, int32_t n_receivers, int32_t device,
+                        swl3d_engine **out);
+void swl3d_destroy(swl3d_engine *engine);
+/* CudaEngine3D::step(time, dt, frequency, step) (src/three_d/CudaEngine3D.cu:113-124). */
+swl_status swl3d_step(swl3d_engine *engine, double time, double dt, double frequency, int32_t step);
+swl_status swl3d_advance(swl3d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
+                         double check_growth_after, int32_t *accepted);
+swl_status swl3d_rollback(swl3d_engine *engine);
+swl_status swl3d_reset(swl3d_engine *engine);
+swl_status swl3d_diagnostics(swl3d_engine *engine, swl_diag3d *out);
+swl_status swl3d_sample(swl3d_engine *engine, double *vx, double *vy, double *vz);
+swl_status swl3d_traces(swl3d_engine *engine, int32_t first, int32_t count, double *vx, double *vy, double *vz);
+swl_status swl3d_snapshot(swl3d_engine *engine, int32_t field, double *out);
+swl_status swl3d_load_field(swl3d_engine *engine, int32_t field, const double *values);
+int64_t swl3d_resident_bytes(const swl3d_engine *engine);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,79 @@
+"""Build libswl_b200.so in-tree: every CUDA unit for sm_100a only (no PTX for other targets).
+
+FP64 units are compiled with --fmad=false so the plain path reproduces the reference
+arithmetic; FP32 units keep FMA contraction.  Objects are cached in _build/ by modification
+time; `python build.py` or ``build()`` from Python.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+SRC = PKG / "csrc"
+OUT = PKG / "_build"
+LIB = PKG / "libswl_b200.so"
+INCLUDE = PKG.parent / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-strict-aliasing",
+          "--expt-relaxed-constexpr", f"-I{INCLUDE}", f"-I{SRC}"]
+UNITS = {
+    "runtime.cu": [],
+    "engine2d_f64.cu": ["--fmad=false"],
+    "engine2d_f32.cu": [],
+    "engine3d_f64.cu": ["--fmad=false"],
+    "engine3d_f32.cu": [],
+    "abi.cpp": ["-x", "cu"],
+}
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if c and Path(c).exists():
+            return c
+    raise FileNotFoundError("nvcc not found")
+
+
+def _deps() -> float:
+    """Newest modification time among headers (any header change rebuilds everything)."""
+    stamps = [p.stat().st_mtime for p in list(SRC.glob("*.cuh")) + list(SRC.glob("*.h")) + list(INCLUDE.glob("*.h"))]
+    return max(stamps) if stamps else 0.0
+
+
+def _compile(unit: str, flags: list[str], verbose: bool, newest: float) -> Path:
+    src = SRC / unit
+    obj = OUT / (unit + ".o")
+    if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest):
+        return obj
+    cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {unit}:\n{proc.stdout}\n{proc.stderr}")
+    if verbose and proc.stderr.strip():
+        print(proc.stderr, flush=True)
+    return obj
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> Path:
+    OUT.mkdir(exist_ok=True)
+    newest = _deps()
+    jobs = jobs or min(len(UNITS), os.cpu_count() or 4)
+    with ThreadPoolExecutor(jobs) as pool:
+        objs = list(pool.map(lambda kv: _compile(kv[0], kv[1], verbose, newest), UNITS.items()))
+    if not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,484 @@
+// Host side of the 2D engine (the B200 replacement of src/two_d/CudaEngine2D.cu:107-184).
+//
+// State layout in HBM: four structure-of-arrays sets of field_count*count values -- two
+// alternating "state / accumulator" sets and two stage sets -- plus the same four sets of
+// compact CFS-PML memories.  A step reads the state set and leaves the new state in the
+// accumulator set; the sets then swap roles, so the state at the start of the last step stays
+// resident and rollback is a role swap (no per-step D2D copy).
+//
+// A batch of steps (swl2d_advance) is recorded once per (step phase mod 8, role parity) into a
+// CUDA graph of eight steps; each step is 4 fused stage kernels + a diagnostics reduction +
+// a one-block verdict that applies the reference's acceptance rule on the device, records the
+// receivers and advances a device-resident step clock.  The host synchronises once per batch.
+#pragma once
+#include "../../include/swl_b200.h"
+#include "runtime.cuh"
+#include "stage2d.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+namespace swl {
+
+class Engine2D {
+  public:
+    virtual ~Engine2D() = default;
+    virtual void step(double dt, double frequency, double scale, int step) = 0;
+    virtual int advance(int first, int count, double dt, double frequency, double scale, double growthAfter) = 0;
+    virtual void rollback() = 0;
+    virtual void reset() = 0;
+    virtual void diagnostics(swl_diag2d &) = 0;
+    virtual void sample(double *vx, double *vz) = 0;
+    virtual void traces(int first, int count, double *vx, double *vz) = 0;
+    virtual void snapshot(int field, double *out) = 0;
+    virtual void load(int field, const double *in) = 0;
+    virtual void probes(const int64_t *nodes, int n, double *out5) = 0;
+    virtual int64_t residentBytes() const = 0;
+    virtual bool faulted() const = 0;
+};
+
+std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &, const int64_t *, int, int);
+std::unique_ptr<Engine2D> makeEngine2D32(const swl_mesh2d &, const int64_t *, int, int);
+
+namespace detail2 {
+
+template <class Real> struct Launch {
+    template <int DX, int DZ, int MECH, int ST> static void go(dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
+        k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, 0, s>>>(a);
+    }
+    template <int DX, int DZ, int MECH> static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
+        switch (stage) {
+        case 0: go<DX, DZ, MECH, 0>(g, b, s, a); break;
+        case 1: go<DX, DZ, MECH, 1>(g, b, s, a); break;
+        case 2: go<DX, DZ, MECH, 2>(g, b, s, a); break;
+        default: go<DX, DZ, MECH, 3>(g, b, s, a); break;
+        }
+    }
+    template <int DX, int DZ> static void mech(int mech, int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
+        switch (mech) {
+        case 0: st<DX, DZ, 0>(stage, g, b, s, a); break;
+        case 1: st<DX, DZ, 1>(stage, g, b, s, a); break;
+        case 2: st<DX, DZ, 2>(stage, g, b, s, a); break;
+        default: st<DX, DZ, 3>(stage, g, b, s, a); break;
+        }
+    }
+    static void stage(int dx, int dz, int mechs, int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
+        if (dx == 0 && dz == 0) mech<0, 0>(mechs, stage, g, b, s, a);
+        else if (dx == 0) mech<0, 1>(mechs, stage, g, b, s, a);
+        else if (dz == 0) mech<1, 0>(mechs, stage, g, b, s, a);
+        else mech<1, 1>(mechs, stage, g, b, s, a);
+    }
+};
+
+template <class Real> std::vector<Real> convert(const void *src, std::size_t n, int arrayPrecision, const char *name) {
+    std::vector<Real> out(n);
+    if (!src) throw Error(SWL_ERR_INVALID, std::string("mesh array ") + name + " is null");
+    if (arrayPrecision == SWL_FP32) {
+        const float *s = static_cast<const float *>(src);
+        for (std::size_t i = 0; i < n; ++i) out[i] = static_cast<Real>(s[i]);
+    } else {
+        const double *s = static_cast<const double *>(src);
+        for (std::size_t i = 0; i < n; ++i) out[i] = static_cast<Real>(s[i]);
+    }
+    for (std::size_t i = 0; i < n; ++i)
+        if (!std::isfinite(static_cast<double>(out[i])))
+            throw Error(SWL_ERR_INVALID, std::string("mesh array ") + name +
+                                             " is not finite in the engine precision; select FP64 or revise the model");
+    return out;
+}
+
+} // namespace detail2
+
+template <class Real> class TypedEngine2D final : public Engine2D {
+    int device_{};
+    cudaStream_t stream_{};
+    k2::Mesh<Real> m_{};
+    int mech_{}, fc_{};
+    long long count_{}, pcount_{};
+    bool cpml_{};
+    std::vector<DeviceBuffer> model_;
+    DeviceBuffer sets_, psets_, recIdx_, traces_, forcing_, clock_, partials_;
+    Real *set_[4]{}, *pset_[4]{};
+    int u_{0}, a_{1};       // state / accumulator roles among set 0 and 1
+    bool previous_{false};  // set a_ holds the state before the last step
+    int nrec_{}, traceCap_{}, forcingCap_{};
+    dim3 grid_, block_{32, 8};
+    int nparts_{};
+    k2::Clock hostClock_{};
+    PinnedBuffer pinnedForcing_, pinnedClock_;
+    std::map<int, cudaGraphExec_t> graphs_;
+    bool faulted_{false};
+    int registers_{};
+    int64_t localBytes_{};
+
+    Real *upload(const std::vector<Real> &v) {
+        model_.emplace_back(v.size() * sizeof(Real));
+        check(cudaMemcpy(model_.back().ptr, v.data(), v.size() * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
+        return model_.back().template as<Real>();
+    }
+    void dropGraphs() {
+        for (auto &g : graphs_) cudaGraphExecDestroy(g.second);
+        graphs_.clear();
+    }
+    k2::StageArgs<Real> args(int stage) const {
+        k2::StageArgs<Real> p{};
+        p.m = m_;
+        Real *U = set_[u_], *A = set_[a_], *S1 = set_[2], *S2 = set_[3];
+        Real *PU = pset_[u_], *PA = pset_[a_], *PS1 = pset_[2], *PS2 = pset_[3];
+        p.base = U;
+        p.acc = A;
+        p.pbase = PU;
+        p.pacc = PA;
+        switch (stage) {
+        case 0: p.in = U, p.out = S1, p.pin = PU, p.pout = PS1; break;
+        case 1: p.in = S1, p.out = S2, p.pin = PS1, p.pout = PS2; break;
+        case 2: p.in = S2, p.out = S1, p.pin = PS2, p.pout = PS1; break;
+        default: p.in = S1, p.out = nullptr, p.pin = PS1, p.pout = nullptr; break;
+        }
+        p.forcing = forcing_.as<Real>();
+        p.clock = clock_.as<k2::Clock>();
+        p.weight = stage == 2 ? static_cast<Real>(dt_) : static_cast<Real>(dt_ / 2);
+        p.delta = static_cast<Real>(dt_);
+        return p;
+    }
+    double dt_{};
+    // Enqueue one step: 4 stages (+ diagnostics and verdict when `verdict`).  Swaps roles.
+    void enqueueStep(int step, bool verdict) {
+        for (int s = 0; s < 4; ++s)
+            detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, grid_, block_, stream_, args(s));
+        check(cudaGetLastError(), "2D stage launch");
+        if (verdict) {
+            Real *fresh = set_[a_];
+            k2::stats2d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, pset_[a_], clock_.as<k2::Clock>(), partials_.as<k2::Partial>());
+            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), nparts_, fresh, count_, recIdx_.as<long long>(),
+                                                         nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
+            check(cudaGetLastError(), "2D verdict launch");
+        }
+        std::swap(u_, a_);
+    }
+    void ensureCapacity(int steps) {
+        if (steps > forcingCap_) {
+            forcing_.allocate(std::size_t(steps) * 3 * sizeof(Real));
+            forcingCap_ = steps;
+            dropGraphs();
+        }
+        if (steps > traceCap_) {
+            traces_.allocate(std::max<std::size_t>(1, std::size_t(steps) * nrec_ * 2) * sizeof(double));
+            traceCap_ = steps;
+            dropGraphs();
+        }
+        pinnedForcing_.reserve(std::size_t(steps) * 3 * sizeof(Real));
+    }
+    void fillForcing(int first, int count, double dt, double frequency, double scale) {
+        Real *f = pinnedForcing_.as<Real>();
+        for (int j = 0; j < count; ++j) {
+            const int s = first + j;
+            // src/two_d/CurvilinearSolver2D.cpp:73,268-274: Real(amplitude/h^2 * ricker(t))
+            f[3 * j] = static_cast<Real>(scale * ricker(s * dt, frequency));
+            f[3 * j + 1] = static_cast<Real>(scale * ricker((s + .5) * dt, frequency));
+            f[3 * j + 2] = static_cast<Real>(scale * ricker((s + 1) * dt, frequency));
+        }
+        check(cudaMemcpyAsync(forcing_.ptr, f, std::size_t(count) * 3 * sizeof(Real), cudaMemcpyHostToDevice, stream_),
+              "upload forcing");
+    }
+    void pushClock() {
+        *pinnedClock_.as<k2::Clock>() = hostClock_;
+        check(cudaMemcpyAsync(clock_.ptr, pinnedClock_.ptr, sizeof(k2::Clock), cudaMemcpyHostToDevice, stream_), "set clock");
+    }
+    void pullClock() {
+        check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
+        check(cudaStreamSynchronize(stream_), "2D batch completion");
+        hostClock_ = *pinnedClock_.as<k2::Clock>();
+    }
+
+  public:
+    TypedEngine2D(const swl_mesh2d &g, const int64_t *rec, int nrec, int device) : device_(device) {
+        DeviceScope scope(device_);
+        if (g.nx < 14 || g.nz < 14 || g.count != int64_t(g.nx) * g.nz)
+            throw Error(SWL_ERR_INVALID, "2D mesh needs nx, nz >= 14 padded nodes and count = nx*nz");
+        if (g.mechanisms < 0 || g.mechanisms > 3 || g.field_count != (g.mechanisms ? 6 + 4 * g.mechanisms : 5))
+            throw Error(SWL_ERR_INVALID, "2D mesh field_count must be 5 (elastic) or 6 + 4*mechanisms (GSLS)");
+        if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
+        const std::size_t n = std::size_t(g.count);
+        count_ = g.count;
+        mech_ = g.mechanisms;
+        fc_ = g.field_count;
+        nrec_ = nrec;
+        const int ap = g.array_precision;
+        auto arr = [&](const void *src, std::size_t len, const char *name) {
+            return upload(detail2::convert<Real>(src, len, ap, name));
+        };
+        m_.nx = g.nx;
+        m_.nz = g.nz;
+        m_.count = g.count;
+        m_.h = static_cast<Real>(g.h);
+        m_.a = arr(g.a, n, "a");
+        m_.b = arr(g.b, n, "b");
+        m_.jac = arr(g.jac, n, "jac");
+        m_.normals = arr(g.normals, 2 * n, "normals");
+        m_.lambda = arr(g.lambda, n, "lambda");
+        m_.mu = arr(g.mu, n, "mu");
+        m_.rho = arr(g.rho, n, "rho");
+        const auto damping = detail2::convert<Real>(g.damping, n, ap, "damping");
+        m_.damping = upload(damping);
+        const auto source = detail2::convert<Real>(g.source, n, ap, "source");
+        m_.source = upload(source);
+        std::vector<Real> sg[2];
+        if (g.source_gradient[0] || g.source_gradient[1]) {
+            sg[0] = detail2::convert<Real>(g.source_gradient[0], n, ap, "source_gradient[0]");
+            sg[1] = detail2::convert<Real>(g.source_gradient[1], n, ap, "source_gradient[1]");
+            m_.sgx = upload(sg[0]);
+            m_.sgz = upload(sg[1]);
+        }
+        m_.sdx = static_cast<Real>(g.source_direction[0]);
+        m_.sdz = static_cast<Real>(g.source_direction[2]);
+        // Box of the source support (the force is exactly zero outside).
+        int i0 = g.nx, i1 = 0, k0 = g.nz, k1 = 0;
+        for (int k = 0; k < g.nz; ++k)
+            for (int i = 0; i < g.nx; ++i) {
+                const std::size_t q = i + std::size_t(g.nx) * k;
+                const bool nz = m_.sgx ? (sg[0][q] != Real(0) || sg[1][q] != Real(0)) : source[q] != Real(0);
+                if (nz) i0 = std::min(i0, i), i1 = std::max(i1, i + 1), k0 = std::min(k0, k), k1 = std::max(k1, k + 1);
+            }
+        m_.src_i0 = i0, m_.src_i1 = i1, m_.src_k0 = k0, m_.src_k1 = k1;
+        // Box [i0,i1) x [0,k1) in which the sponge rate is exactly zero (verified).
+        {
+            auto D = [&](int i, int k) { return damping[i + std::size_t(g.nx) * k]; };
+            int a0 = 3, a1 = g.nx - 3;
+            while (a0 < a1 && D(a0, 3) != Real(0)) ++a0;
+            while (a1 > a0 && D(a1 - 1, 3) != Real(0)) --a1;
+            int kk = 3;
+            const int mid = (a0 + a1) / 2;
+            if (a0 < a1)
+                while (kk < g.nz - 3 && D(mid, kk) == Real(0)) ++kk;
+            bool ok = a0 < a1;
+            for (int k = 0; ok && k < kk; ++k)
+                for (int i = a0; i < a1; ++i)
+                    if (D(i, k) != Real(0)) {
+                        ok = false;
+                        break;
+                    }
+            if (ok) m_.dmp_i0 = a0, m_.dmp_i1 = a1, m_.dmp_k1 = (kk >= g.nz - 3 ? g.nz : kk);
+            else m_.dmp_i0 = m_.dmp_i1 = m_.dmp_k1 = 0;
+        }
+        cpml_ = g.cpml_count > 0;
+        pcount_ = g.cpml_count;
+        if (cpml_) {
+            if (g.cpml_width_x < 0 || g.cpml_width_z < 1 ||
+                g.cpml_count != 4 * (2 * int64_t(g.cpml_width_x) * (g.nz - 6) + int64_t(g.cpml_width_z) * (g.nx - 6)))
+                throw Error(SWL_ERR_INVALID, "CFS-PML count must be 4*(2*wx*(nz-6) + wz*(nx-6))");
+            m_.cpx = arr(g.cpml_x, 3 * std::size_t(g.nx - 6), "cpml_x");
+            m_.cpz = arr(g.cpml_z, 3 * std::size_t(g.nz - 6), "cpml_z");
+            m_.wx = g.cpml_width_x;
+            m_.wz = g.cpml_width_z;
+        }
+        for (int l = 0; l < mech_; ++l) {
+            m_.rates[l] = static_cast<Real>(g.rates[l]);
+            m_.dP[l] = arr(g.delta_p[l], n, "delta_p");
+            m_.dS[l] = arr(g.delta_s[l], n, "delta_s");
+        }
+        m_.fc = fc_;
+        sets_.allocate(4 * std::size_t(fc_) * n * sizeof(Real));
+        for (int s = 0; s < 4; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * fc_ * n;
+        psets_.allocate(4 * std::size_t(std::max<long long>(pcount_, 1)) * sizeof(Real));
+        for (int s = 0; s < 4; ++s) pset_[s] = psets_.as<Real>() + std::size_t(s) * std::max<long long>(pcount_, 1);
+        std::vector<long long> idx(nrec);
+        for (int r = 0; r < nrec; ++r) {
+            if (rec[r] < 0 || rec[r] >= g.count) throw Error(SWL_ERR_INVALID, "receiver node outside the padded grid");
+            idx[r] = rec[r];
+        }
+        recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
+        if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
+        grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.nz - 6 + block_.y - 1) / block_.y);
+        nparts_ = grid_.x * grid_.y;
+        partials_.allocate(nparts_ * sizeof(k2::Partial));
+        clock_.allocate(sizeof(k2::Clock));
+        pinnedClock_.reserve(sizeof(k2::Clock));
+        ensureCapacity(8);
+        cudaFuncAttributes attr{};
+        check(cudaFuncGetAttributes(&attr, k2::stage2d<Real, 0, 0, 0, 1>), "2D kernel compatibility");
+        registers_ = attr.numRegs;
+        localBytes_ = attr.localSizeBytes;
+    }
+    ~TypedEngine2D() override {
+        dropGraphs();
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+    bool faulted() const override { return faulted_; }
+
+    void step(double dt, double frequency, double scale, int step) override {
+        DeviceScope scope(device_);
+        dt_ = dt;
+        ensureCapacity(1);
+        hostClock_.step = step;
+        hostClock_.first = step;
+        hostClock_.faulted = 0;
+        hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_;
+        pushClock();
+        fillForcing(step, 1, dt, frequency, scale);
+        enqueueStep(step, false);
+        previous_ = true;
+        check(cudaStreamSynchronize(stream_), "2D step completion");
+    }
+
+    int advance(int first, int count, double dt, double frequency, double scale, double growthAfter) override {
+        DeviceScope scope(device_);
+        if (count <= 0) return 0;
+        if (dt != dt_) dropGraphs(), dt_ = dt;
+        ensureCapacity(count);
+        hostClock_.step = first;
+        hostClock_.first = first;
+        hostClock_.faulted = 0;
+        hostClock_.fault_step = -1;
+        hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_;
+        hostClock_.dt = dt;
+        hostClock_.growth_after = growthAfter;
+        pushClock();
+        fillForcing(first, count, dt, frequency, scale);
+        const int u0 = u_;
+        int done = 0;
+        while (count - done >= 8) {
+            const int key = ((first + done) % 8) * 2 + (u_ == 0 ? 0 : 1);
+            auto it = graphs_.find(key);
+            if (it == graphs_.end()) {
+                cudaGraph_t graph;
+                const int su = u_, sa = a_;
+                check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+                for (int j = 0; j < 8; ++j) enqueueStep(first + done + j, true);
+                check(cudaStreamEndCapture(stream_, &graph), "end graph capture");
+                u_ = su, a_ = sa;
+                cudaGraphExec_t exec;
+                check(cudaGraphInstantiate(&exec, graph, 0), "instantiate step graph");
+                cudaGraphDestroy(graph);
+                it = graphs_.emplace(key, exec).first;
+            }
+            check(cudaGraphLaunch(it->second, stream_), "launch step graph");
+            done += 8; // eight role swaps: roles are back where they started
+        }
+        for (; done < count; ++done) enqueueStep(first + done, true);
+        pullClock();
+        const int accepted = hostClock_.accepted;
+        // Roles after `accepted` steps; a rejected step leaves its starting state current.
+        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+        return accepted;
+    }
+    void rollback() override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "2D rollback");
+        if (previous_) std::swap(u_, a_), previous_ = false;
+    }
+    void reset() override {
+        DeviceScope scope(device_);
+        check(cudaMemsetAsync(sets_.ptr, 0, sets_.bytes, stream_), "2D reset");
+        check(cudaMemsetAsync(psets_.ptr, 0, psets_.bytes, stream_), "2D PML reset");
+        if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "2D trace reset");
+        hostClock_ = k2::Clock{};
+        pushClock();
+        check(cudaStreamSynchronize(stream_), "2D clear completion");
+        u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
+    }
+    void diagnostics(swl_diag2d &d) override {
+        DeviceScope scope(device_);
+        k2::stats2d<Real><<<grid_, block_, 0, stream_>>>(m_, set_[u_], pset_[u_], nullptr, partials_.as<k2::Partial>());
+        check(cudaGetLastError(), "2D diagnostics");
+        std::vector<k2::Partial> parts(nparts_);
+        check(cudaMemcpyAsync(parts.data(), partials_.ptr, nparts_ * sizeof(k2::Partial), cudaMemcpyDeviceToHost, stream_),
+              "2D diagnostics readback");
+        check(cudaStreamSynchronize(stream_), "2D diagnostics completion");
+        d.energy = d.max_velocity = d.traction_relative = 0;
+        d.finite = 1;
+        for (const auto &p : parts) {
+            d.energy += p.energy;
+            d.max_velocity = std::max(d.max_velocity, p.velocity);
+            d.traction_relative = std::max(d.traction_relative, p.traction);
+            d.finite &= !p.bad;
+        }
+        d.finite &= std::isfinite(d.energy) ? 1 : 0;
+        d.peak_energy = hostClock_.peak_energy;
+        d.rhs_registers = registers_;
+        d.rhs_local_bytes = localBytes_;
+        d.resident_bytes = residentBytes();
+    }
+    void gather(const int64_t *nodes, int n, int fields, double *out) {
+        if (n <= 0) return;
+        std::vector<long long> idx(nodes, nodes + n);
+        for (auto q : idx)
+            if (q < 0 || q >= count_) throw Error(SWL_ERR_INVALID, "probe node outside the padded grid");
+        DeviceBuffer dIdx(n * sizeof(long long)), dOut(std::size_t(n) * fields * sizeof(double));
+        check(cudaMemcpyAsync(dIdx.ptr, idx.data(), n * sizeof(long long), cudaMemcpyHostToDevice, stream_), "probe upload");
+        k2::gather2d<Real><<<(n + 127) / 128, 128, 0, stream_>>>(set_[u_], count_, dIdx.as<long long>(), n, fields, dOut.as<double>());
+        check(cudaGetLastError(), "probe launch");
+        check(cudaMemcpyAsync(out, dOut.ptr, std::size_t(n) * fields * sizeof(double), cudaMemcpyDeviceToHost, stream_), "probe readback");
+        check(cudaStreamSynchronize(stream_), "probe completion");
+    }
+    void sample(double *vx, double *vz) override {
+        DeviceScope scope(device_);
+        if (!nrec_) return;
+        std::vector<int64_t> idx(nrec_);
+        check(cudaMemcpy(idx.data(), recIdx_.ptr, nrec_ * sizeof(long long), cudaMemcpyDeviceToHost), "receiver index readback");
+        std::vector<double> v(2 * std::size_t(nrec_));
+        gather(idx.data(), nrec_, 2, v.data());
+        for (int r = 0; r < nrec_; ++r) vx[r] = v[2 * r], vz[r] = v[2 * r + 1];
+    }
+    void traces(int first, int count, double *vx, double *vz) override {
+        DeviceScope scope(device_);
+        const int row0 = first - hostClock_.first;
+        if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
+            throw Error(SWL_ERR_INVALID, "requested trace rows were not recorded by the last advance");
+        std::vector<double> buf(std::size_t(count) * nrec_ * 2);
+        if (!buf.empty())
+            check(cudaMemcpy(buf.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 2, buf.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost),
+                  "trace readback");
+        for (int r = 0; r < nrec_; ++r)
+            for (int j = 0; j < count; ++j) {
+                vx[std::size_t(r) * count + j] = buf[(std::size_t(j) * nrec_ + r) * 2];
+                vz[std::size_t(r) * count + j] = buf[(std::size_t(j) * nrec_ + r) * 2 + 1];
+            }
+    }
+    void snapshot(int field, double *out) override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "snapshot ordering");
+        const Real *src;
+        std::size_t len;
+        if (field == -1) src = pset_[u_], len = std::size_t(pcount_);
+        else if (field >= 0 && field < fc_) src = set_[u_] + std::size_t(field) * count_, len = std::size_t(count_);
+        else throw Error(SWL_ERR_INVALID, "snapshot field out of range");
+        std::vector<Real> tmp(len);
+        if (len) check(cudaMemcpy(tmp.data(), src, len * sizeof(Real), cudaMemcpyDeviceToHost), "snapshot download");
+        for (std::size_t i = 0; i < len; ++i) out[i] = double(tmp[i]);
+    }
+    void load(int field, const double *in) override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "load ordering");
+        Real *dst;
+        std::size_t len;
+        if (field == -1) dst = pset_[u_], len = std::size_t(pcount_);
+        else if (field >= 0 && field < fc_) dst = set_[u_] + std::size_t(field) * count_, len = std::size_t(count_);
+        else throw Error(SWL_ERR_INVALID, "load field out of range");
+        std::vector<Real> tmp(in, in + len);
+        if (len) check(cudaMemcpy(dst, tmp.data(), len * sizeof(Real), cudaMemcpyHostToDevice), "field upload");
+        previous_ = false;
+    }
+    void probes(const int64_t *nodes, int n, double *out5) override {
+        DeviceScope scope(device_);
+        gather(nodes, n, 5, out5);
+    }
+    int64_t residentBytes() const override {
+        int64_t b = 0;
+        for (const auto &x : model_) b += x.bytes;
+        for (const auto *x : {&sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_}) b += x->bytes;
+        return b;
+    }
+};
+
+} // namespace swl

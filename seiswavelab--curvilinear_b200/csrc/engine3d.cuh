@@ -1,0 +1,433 @@
+// Host side of the 3D engine (the B200 replacement of src/three_d/CudaEngine3D.cu:68-150).
+// Same state scheme as the 2D engine: two alternating state/accumulator sets and two stage
+// sets of nine fields, CUDA-graph batches of eight steps, a device-side acceptance verdict.
+#pragma once
+#include "../../include/swl_b200.h"
+#include "runtime.cuh"
+#include "stage3d.cuh"
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <vector>
+
+namespace swl {
+
+class Engine3D {
+  public:
+    virtual ~Engine3D() = default;
+    virtual void step(double dt, double frequency, int step) = 0;
+    virtual int advance(int first, int count, double dt, double frequency, double growthAfter) = 0;
+    virtual void rollback() = 0;
+    virtual void reset() = 0;
+    virtual void diagnostics(swl_diag3d &) = 0;
+    virtual void sample(double *vx, double *vy, double *vz) = 0;
+    virtual void traces(int first, int count, double *vx, double *vy, double *vz) = 0;
+    virtual void snapshot(int field, double *out) = 0;
+    virtual void load(int field, const double *in) = 0;
+    virtual int64_t residentBytes() const = 0;
+    virtual bool faulted() const = 0;
+};
+
+std::unique_ptr<Engine3D> makeEngine3D64(const swl_mesh3d &, const int64_t *, int, int);
+std::unique_ptr<Engine3D> makeEngine3D32(const swl_mesh3d &, const int64_t *, int, int);
+
+namespace detail3 {
+template <class Real> struct Launch {
+    template <int DX, int DY, int DZ>
+    static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
+        switch (stage) {
+        case 0: k3::stage3d<Real, DX, DY, DZ, 0><<<g, b, 0, s>>>(a); break;
+        case 1: k3::stage3d<Real, DX, DY, DZ, 1><<<g, b, 0, s>>>(a); break;
+        case 2: k3::stage3d<Real, DX, DY, DZ, 2><<<g, b, 0, s>>>(a); break;
+        default: k3::stage3d<Real, DX, DY, DZ, 3><<<g, b, 0, s>>>(a); break;
+        }
+    }
+    static void stage(int dx, int dy, int dz, int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
+        switch (dx * 4 + dy * 2 + dz) {
+        case 0: st<0, 0, 0>(stage, g, b, s, a); break;
+        case 1: st<0, 0, 1>(stage, g, b, s, a); break;
+        case 2: st<0, 1, 0>(stage, g, b, s, a); break;
+        case 3: st<0, 1, 1>(stage, g, b, s, a); break;
+        case 4: st<1, 0, 0>(stage, g, b, s, a); break;
+        case 5: st<1, 0, 1>(stage, g, b, s, a); break;
+        case 6: st<1, 1, 0>(stage, g, b, s, a); break;
+        default: st<1, 1, 1>(stage, g, b, s, a); break;
+        }
+    }
+};
+} // namespace detail3
+
+template <class Real> class TypedEngine3D final : public Engine3D {
+    int device_{};
+    cudaStream_t stream_{};
+    k3::Mesh<Real> m_{};
+    long long count_{};
+    std::vector<DeviceBuffer> model_;
+    DeviceBuffer sets_, recIdx_, traces_, forcing_, clock_, partials_, surfRate_;
+    Real *set_[4]{};
+    int u_{0}, a_{1};
+    bool previous_{false};
+    int nrec_{}, traceCap_{}, forcingCap_{};
+    dim3 grid_, block_{32, 8, 1};
+    int nparts_{};
+    k2::Clock hostClock_{};
+    PinnedBuffer pinnedForcing_, pinnedClock_;
+    std::map<int, cudaGraphExec_t> graphs_;
+    bool faulted_{false};
+    int registers_{};
+    double dt_{}, amplitudeScale_{};
+    double hostDensity_{}, hostH_{}, amplitude_{};
+
+    Real *upload(const std::vector<Real> &v) {
+        model_.emplace_back(std::max<std::size_t>(1, v.size()) * sizeof(Real));
+        if (!v.empty())
+            check(cudaMemcpy(model_.back().ptr, v.data(), v.size() * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
+        return model_.back().template as<Real>();
+    }
+    static std::vector<Real> conv(const double *src, std::size_t n, std::size_t stride = 1, std::size_t offset = 0) {
+        std::vector<Real> out(n);
+        for (std::size_t i = 0; i < n; ++i) {
+            out[i] = static_cast<Real>(src[i * stride + offset]);
+            if (!std::isfinite(double(out[i])))
+                throw Error(SWL_ERR_INVALID, "3D mesh value is not finite in the engine precision");
+        }
+        return out;
+    }
+    void dropGraphs() {
+        for (auto &g : graphs_) cudaGraphExecDestroy(g.second);
+        graphs_.clear();
+    }
+    k3::StageArgs<Real> args(int stage) const {
+        k3::StageArgs<Real> p{};
+        p.m = m_;
+        Real *U = set_[u_], *A = set_[a_], *S1 = set_[2], *S2 = set_[3];
+        p.base = U;
+        p.acc = A;
+        switch (stage) {
+        case 0: p.in = U, p.out = S1; break;
+        case 1: p.in = S1, p.out = S2; break;
+        case 2: p.in = S2, p.out = S1; break;
+        default: p.in = S1, p.out = nullptr; break;
+        }
+        p.forcing = forcing_.as<Real>();
+        p.clock = clock_.as<k2::Clock>();
+        p.weight = stage == 2 ? static_cast<Real>(dt_) : static_cast<Real>(0.5 * dt_);
+        p.w6 = static_cast<Real>(dt_ / 6.0);
+        p.w3 = static_cast<Real>(dt_ / 3.0);
+        p.surfRate = surfRate_.as<double>();
+        return p;
+    }
+    void enqueueStep(int step, bool verdict) {
+        for (int s = 0; s < 4; ++s)
+            detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, grid_, block_,
+                                         stream_, args(s));
+        check(cudaGetLastError(), "3D stage launch");
+        if (verdict) {
+            Real *fresh = set_[a_];
+            k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, surfRate_.as<double>(), clock_.as<k2::Clock>(),
+                                                             partials_.as<k3::Partial>());
+            k3::verdict3d<Real><<<1, 512, 0, stream_>>>(partials_.as<k3::Partial>(), nparts_, fresh, count_,
+                                                         recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>());
+            check(cudaGetLastError(), "3D verdict launch");
+        }
+        std::swap(u_, a_);
+    }
+    void ensureCapacity(int steps) {
+        if (steps > forcingCap_) {
+            forcing_.allocate(std::size_t(steps) * 3 * sizeof(Real));
+            forcingCap_ = steps;
+            dropGraphs();
+        }
+        if (steps > traceCap_) {
+            traces_.allocate(std::max<std::size_t>(1, std::size_t(steps) * nrec_ * 3) * sizeof(double));
+            traceCap_ = steps;
+            dropGraphs();
+        }
+        pinnedForcing_.reserve(std::size_t(steps) * 3 * sizeof(Real));
+    }
+    // src/three_d/CurvilinearSolver.cpp:75-77 (scale = amplitude / (rho0 h^3)).
+    double source(double t, double f) const {
+        const double scale = amplitude_ / (hostDensity_ * hostH_ * hostH_ * hostH_);
+        const double tau = 3.14159265358979323846 * f * (t - 1.5 / f);
+        return scale * (1.0 - 2.0 * tau * tau) * std::exp(-tau * tau);
+    }
+    void fillForcing(int first, int count, double dt, double frequency) {
+        Real *f = pinnedForcing_.as<Real>();
+        for (int j = 0; j < count; ++j) {
+            const double t = (first + j) * dt;
+            f[3 * j] = static_cast<Real>(source(t, frequency));
+            f[3 * j + 1] = static_cast<Real>(source(t + 0.5 * dt, frequency));
+            f[3 * j + 2] = static_cast<Real>(source(t + dt, frequency));
+        }
+        check(cudaMemcpyAsync(forcing_.ptr, f, std::size_t(count) * 3 * sizeof(Real), cudaMemcpyHostToDevice, stream_),
+              "upload source");
+    }
+    void pushClock() {
+        *pinnedClock_.as<k2::Clock>() = hostClock_;
+        check(cudaMemcpyAsync(clock_.ptr, pinnedClock_.ptr, sizeof(k2::Clock), cudaMemcpyHostToDevice, stream_), "set clock");
+    }
+    void pullClock() {
+        check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
+        check(cudaStreamSynchronize(stream_), "3D batch completion");
+        hostClock_ = *pinnedClock_.as<k2::Clock>();
+    }
+
+  public:
+    TypedEngine3D(const swl_mesh3d &g, const int64_t *rec, int nrec, int device) : device_(device) {
+        DeviceScope scope(device_);
+        if (g.nx < 14 || g.ny < 14 || g.nz < 14 || g.count != int64_t(g.nx) * g.ny * g.nz)
+            throw Error(SWL_ERR_INVALID, "3D mesh needs nx, ny, nz >= 14 padded nodes and count = nx*ny*nz");
+        if (!g.metrics || !g.jacobian || !g.source || !g.damping || !g.normals)
+            throw Error(SWL_ERR_INVALID, "3D mesh arrays (metrics, jacobian, source, damping, normals) are required");
+        if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
+        const std::size_t n = std::size_t(g.count);
+        count_ = g.count;
+        nrec_ = nrec;
+        hostDensity_ = g.density, hostH_ = g.h, amplitude_ = g.source_amplitude;
+        m_.nx = g.nx, m_.ny = g.ny, m_.nz = g.nz;
+        m_.count = g.count;
+        m_.plane = (long long)g.nx * g.ny;
+        m_.h = static_cast<Real>(g.h);
+        m_.lambda = static_cast<Real>(g.lambda), m_.mu = static_cast<Real>(g.mu), m_.density = static_cast<Real>(g.density);
+        for (int c = 0; c < 9; ++c) m_.metric[c] = upload(conv(g.metrics, n, 9, c));
+        m_.jac = upload(conv(g.jacobian, n));
+        const auto damping = conv(g.damping, n);
+        m_.damping = upload(damping);
+        const auto src = conv(g.source, n);
+        m_.source = upload(src);
+        std::vector<Real> sg[3];
+        const bool moment = g.source_gradient[0] != nullptr;
+        for (int a = 0; a < 3; ++a) {
+            if (moment) {
+                if (!g.source_gradient[a]) throw Error(SWL_ERR_INVALID, "moment source needs three gradient arrays");
+                sg[a] = conv(g.source_gradient[a], n);
+                m_.sg[a] = upload(sg[a]);
+            }
+            m_.sdir[a] = static_cast<Real>(g.source_direction[a]);
+        }
+        if (g.material_lambda || g.material_mu || g.material_density) {
+            if (!g.material_lambda || !g.material_mu || !g.material_density)
+                throw Error(SWL_ERR_INVALID, "layered material needs lambda, mu and density arrays");
+            m_.mlambda = upload(conv(g.material_lambda, n));
+            m_.mmu = upload(conv(g.material_mu, n));
+            m_.mdensity = upload(conv(g.material_density, n));
+        }
+        {
+            std::vector<Real> nrm(3 * std::size_t(m_.plane));
+            const std::size_t top = std::size_t(3) * m_.plane;
+            for (std::size_t s = 0; s < std::size_t(m_.plane); ++s)
+                for (int c = 0; c < 3; ++c) nrm[3 * s + c] = static_cast<Real>(g.normals[3 * (top + s) + c]);
+            m_.normals = upload(nrm);
+        }
+        // boxes of the source support and of the zero sponge rate
+        int b[6] = {g.nx, 0, g.ny, 0, g.nz, 0};
+        for (int k = 0; k < g.nz; ++k)
+            for (int j = 0; j < g.ny; ++j)
+                for (int i = 0; i < g.nx; ++i) {
+                    const std::size_t q = i + std::size_t(g.nx) * (j + std::size_t(g.ny) * k);
+                    const bool nz = moment ? (sg[0][q] != Real(0) || sg[1][q] != Real(0) || sg[2][q] != Real(0)) : src[q] != Real(0);
+                    if (nz)
+                        b[0] = std::min(b[0], i), b[1] = std::max(b[1], i + 1), b[2] = std::min(b[2], j), b[3] = std::max(b[3], j + 1),
+                        b[4] = std::min(b[4], k), b[5] = std::max(b[5], k + 1);
+                }
+        m_.src_i0 = b[0], m_.src_i1 = b[1], m_.src_j0 = b[2], m_.src_j1 = b[3], m_.src_k0 = b[4], m_.src_k1 = b[5];
+        {
+            auto D = [&](int i, int j, int k) { return damping[i + std::size_t(g.nx) * (j + std::size_t(g.ny) * k)]; };
+            const int jm = g.ny / 2, im = g.nx / 2;
+            int i0 = 3, i1 = g.nx - 3, j0 = 3, j1 = g.ny - 3, kk = 3;
+            while (i0 < i1 && D(i0, jm, 3) != Real(0)) ++i0;
+            while (i1 > i0 && D(i1 - 1, jm, 3) != Real(0)) --i1;
+            while (j0 < j1 && D(im, j0, 3) != Real(0)) ++j0;
+            while (j1 > j0 && D(im, j1 - 1, 3) != Real(0)) --j1;
+            if (i0 < i1 && j0 < j1)
+                while (kk < g.nz - 3 && D((i0 + i1) / 2, (j0 + j1) / 2, kk) == Real(0)) ++kk;
+            bool ok = i0 < i1 && j0 < j1;
+            for (int k = 0; ok && k < kk; ++k)
+                for (int j = j0; ok && j < j1; ++j)
+                    for (int i = i0; i < i1; ++i)
+                        if (D(i, j, k) != Real(0)) {
+                            ok = false;
+                            break;
+                        }
+            if (ok) m_.dmp_i0 = i0, m_.dmp_i1 = i1, m_.dmp_j0 = j0, m_.dmp_j1 = j1, m_.dmp_k1 = kk >= g.nz - 3 ? g.nz : kk;
+        }
+        sets_.allocate(4 * 9 * n * sizeof(Real));
+        for (int s = 0; s < 4; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * 9 * n;
+        surfRate_.allocate(2 * std::size_t(m_.plane) * sizeof(double));
+        std::vector<long long> idx(nrec);
+        for (int r = 0; r < nrec; ++r) {
+            if (rec[r] < 0 || rec[r] >= g.count) throw Error(SWL_ERR_INVALID, "receiver node outside the padded grid");
+            idx[r] = rec[r];
+        }
+        recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
+        if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
+        grid_ = dim3((g.nx - 6 + 31) / 32, (g.ny - 6 + 7) / 8, g.nz - 6);
+        nparts_ = grid_.x * grid_.y * grid_.z;
+        partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
+        clock_.allocate(sizeof(k2::Clock));
+        pinnedClock_.reserve(sizeof(k2::Clock));
+        ensureCapacity(8);
+        cudaFuncAttributes attr{};
+        check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
+        registers_ = attr.numRegs;
+    }
+    ~TypedEngine3D() override {
+        dropGraphs();
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+    bool faulted() const override { return faulted_; }
+    void step(double dt, double frequency, int step) override {
+        DeviceScope scope(device_);
+        dt_ = dt;
+        ensureCapacity(1);
+        hostClock_.step = hostClock_.first = step;
+        hostClock_.faulted = 0;
+        hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_;
+        pushClock();
+        fillForcing(step, 1, dt, frequency);
+        enqueueStep(step, false);
+        previous_ = true;
+        check(cudaStreamSynchronize(stream_), "3D step completion");
+    }
+    int advance(int first, int count, double dt, double frequency, double growthAfter) override {
+        DeviceScope scope(device_);
+        if (count <= 0) return 0;
+        if (dt != dt_) dropGraphs(), dt_ = dt;
+        ensureCapacity(count);
+        hostClock_.step = hostClock_.first = first;
+        hostClock_.faulted = 0;
+        hostClock_.fault_step = -1;
+        hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_;
+        hostClock_.dt = dt;
+        hostClock_.growth_after = growthAfter;
+        pushClock();
+        fillForcing(first, count, dt, frequency);
+        const int u0 = u_;
+        int done = 0;
+        while (count - done >= 8) {
+            const int key = ((first + done) % 8) * 2 + (u_ == 0 ? 0 : 1);
+            auto it = graphs_.find(key);
+            if (it == graphs_.end()) {
+                cudaGraph_t graph;
+                const int su = u_, sa = a_;
+                check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin graph capture");
+                for (int j = 0; j < 8; ++j) enqueueStep(first + done + j, true);
+                check(cudaStreamEndCapture(stream_, &graph), "end graph capture");
+                u_ = su, a_ = sa;
+                cudaGraphExec_t exec;
+                check(cudaGraphInstantiate(&exec, graph, 0), "instantiate step graph");
+                cudaGraphDestroy(graph);
+                it = graphs_.emplace(key, exec).first;
+            }
+            check(cudaGraphLaunch(it->second, stream_), "launch step graph");
+            done += 8;
+        }
+        for (; done < count; ++done) enqueueStep(first + done, true);
+        pullClock();
+        const int accepted = hostClock_.accepted;
+        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+        return accepted;
+    }
+    void rollback() override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "3D rollback");
+        if (previous_) std::swap(u_, a_), previous_ = false;
+    }
+    void reset() override {
+        DeviceScope scope(device_);
+        check(cudaMemsetAsync(sets_.ptr, 0, sets_.bytes, stream_), "3D reset");
+        if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "3D trace reset");
+        check(cudaMemsetAsync(surfRate_.ptr, 0, surfRate_.bytes, stream_), "3D surface reset");
+        hostClock_ = k2::Clock{};
+        pushClock();
+        check(cudaStreamSynchronize(stream_), "3D clear completion");
+        u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
+    }
+    void diagnostics(swl_diag3d &d) override {
+        DeviceScope scope(device_);
+        k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, set_[u_], surfRate_.as<double>(), nullptr, partials_.as<k3::Partial>());
+        check(cudaGetLastError(), "3D diagnostics");
+        std::vector<k3::Partial> parts(nparts_);
+        check(cudaMemcpyAsync(parts.data(), partials_.ptr, parts.size() * sizeof(k3::Partial), cudaMemcpyDeviceToHost, stream_),
+              "3D diagnostics readback");
+        check(cudaStreamSynchronize(stream_), "3D diagnostics completion");
+        double norm = 0, traction = 0;
+        d = swl_diag3d{};
+        d.finite = 1;
+        for (const auto &p : parts) {
+            d.energy += p.energy;
+            d.max_velocity = std::max(d.max_velocity, p.velocity);
+            for (int c = 0; c < 5; ++c) d.peaks[c] = std::max(d.peaks[c], p.peak[c]);
+            norm = std::max(norm, p.rateNorm);
+            traction = std::max(traction, p.rateTraction);
+            d.finite &= !p.bad;
+        }
+        d.traction_rate_relative = traction / std::max(norm, 1e-30);
+        d.peak_energy = hostClock_.peak_energy;
+        d.rhs_registers = registers_;
+        d.resident_bytes = residentBytes();
+    }
+    void sample(double *vx, double *vy, double *vz) override {
+        DeviceScope scope(device_);
+        if (!nrec_) return;
+        std::vector<long long> idx(nrec_);
+        check(cudaMemcpy(idx.data(), recIdx_.ptr, nrec_ * sizeof(long long), cudaMemcpyDeviceToHost), "receiver index readback");
+        DeviceBuffer out(std::size_t(nrec_) * 3 * sizeof(double));
+        k2::gather2d<Real><<<(nrec_ + 127) / 128, 128, 0, stream_>>>(set_[u_], count_, recIdx_.as<long long>(), nrec_, 3,
+                                                                     out.as<double>());
+        check(cudaGetLastError(), "3D receiver launch");
+        std::vector<double> v(std::size_t(nrec_) * 3);
+        check(cudaMemcpyAsync(v.data(), out.ptr, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_), "3D receiver readback");
+        check(cudaStreamSynchronize(stream_), "3D receiver completion");
+        for (int r = 0; r < nrec_; ++r) vx[r] = v[3 * r], vy[r] = v[3 * r + 1], vz[r] = v[3 * r + 2];
+    }
+    void traces(int first, int count, double *vx, double *vy, double *vz) override {
+        DeviceScope scope(device_);
+        const int row0 = first - hostClock_.first;
+        if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
+            throw Error(SWL_ERR_INVALID, "requested trace rows were not recorded by the last advance");
+        std::vector<double> buf(std::size_t(count) * nrec_ * 3);
+        if (!buf.empty())
+            check(cudaMemcpy(buf.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 3, buf.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost),
+                  "trace readback");
+        for (int r = 0; r < nrec_; ++r)
+            for (int j = 0; j < count; ++j) {
+                const std::size_t at = (std::size_t(j) * nrec_ + r) * 3, to = std::size_t(r) * count + j;
+                vx[to] = buf[at], vy[to] = buf[at + 1], vz[to] = buf[at + 2];
+            }
+    }
+    void snapshot(int field, double *out) override {
+        DeviceScope scope(device_);
+        if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "snapshot field out of range");
+        check(cudaStreamSynchronize(stream_), "snapshot ordering");
+        std::vector<Real> tmp(count_);
+        check(cudaMemcpy(tmp.data(), set_[u_] + std::size_t(field) * count_, count_ * sizeof(Real), cudaMemcpyDeviceToHost),
+              "snapshot download");
+        for (long long i = 0; i < count_; ++i) out[i] = double(tmp[i]);
+    }
+    void load(int field, const double *in) override {
+        DeviceScope scope(device_);
+        if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
+        check(cudaStreamSynchronize(stream_), "load ordering");
+        std::vector<Real> tmp(in, in + count_);
+        check(cudaMemcpy(set_[u_] + std::size_t(field) * count_, tmp.data(), count_ * sizeof(Real), cudaMemcpyHostToDevice),
+              "field upload");
+        previous_ = false;
+    }
+    int64_t residentBytes() const override {
+        int64_t b = 0;
+        for (const auto &x : model_) b += x.bytes;
+        for (const auto *x : {&sets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_, &surfRate_}) b += x->bytes;
+        return b;
+    }
+};
+
+} // namespace swl

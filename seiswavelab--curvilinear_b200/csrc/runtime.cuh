@@ -1,0 +1,112 @@
+// Runtime helpers shared by the engines: the CUDA error convention (a failure throws
+// std::runtime_error("CUDA <action>: <message>") inside the library; the C ABI turns it
+// into a status, cf. src/common/CudaSupport.cuh:5-8), device selection scope and RAII
+// device/pinned buffers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace swl {
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(cudaError_t e, const char *action) {
+    if (e != cudaSuccess) throw Error(-2, std::string("CUDA ") + action + ": " + cudaGetErrorString(e));
+}
+
+// Makes `device` current for the scope and restores the caller's device afterwards.
+struct DeviceScope {
+    int previous{-1};
+    explicit DeviceScope(int device) {
+        check(cudaGetDevice(&previous), "query current device");
+        if (previous != device) check(cudaSetDevice(device), "select device");
+    }
+    ~DeviceScope() {
+        if (previous >= 0) cudaSetDevice(previous);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
+// Owning device allocation (zeroed on allocation).
+struct DeviceBuffer {
+    void *ptr{};
+    std::size_t bytes{};
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(std::size_t n) { allocate(n); }
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(std::exchange(o.ptr, nullptr)), bytes(std::exchange(o.bytes, 0)) {}
+    DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = std::exchange(o.ptr, nullptr);
+            bytes = std::exchange(o.bytes, 0);
+        }
+        return *this;
+    }
+    ~DeviceBuffer() { release(); }
+    void allocate(std::size_t n) {
+        release();
+        if (!n) return;
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            cudaGetLastError();
+            throw Error(-3, std::string("CUDA allocate ") + std::to_string(n) + " bytes: " + cudaGetErrorString(e));
+        }
+        bytes = n;
+        check(cudaMemset(ptr, 0, n), "clear allocation");
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Owning pinned host allocation for asynchronous copies.
+struct PinnedBuffer {
+    void *ptr{};
+    std::size_t bytes{};
+    PinnedBuffer() = default;
+    PinnedBuffer(const PinnedBuffer &) = delete;
+    PinnedBuffer &operator=(const PinnedBuffer &) = delete;
+    ~PinnedBuffer() { release(); }
+    void reserve(std::size_t n) {
+        if (n <= bytes) return;
+        release();
+        check(cudaMallocHost(&ptr, n), "allocate pinned host buffer");
+        bytes = n;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Device with the most global memory among sm_100 devices, or -1.
+int selectDevice(int requested);
+
+// The 8-step MacCormack direction table of include/SeisCommon/FiniteDifference.hpp:9-13
+// (axis 0 = x, 1 = y, 2 = z), flipped at each RK stage.
+inline int direction(int step, int stage, int axis) {
+    static const int table[8][3] = {{0, 0, 0}, {1, 1, 0}, {1, 1, 1}, {0, 0, 1},
+                                    {0, 1, 0}, {1, 0, 0}, {1, 0, 1}, {0, 1, 1}};
+    return (table[step % 8][axis] + stage) % 2;
+}
+
+// Ricker wavelet of src/two_d/CurvilinearSolver2D.cpp:31-34.
+double ricker(double t, double f);
+
+} // namespace swl

@@ -1,0 +1,374 @@
+// 3D nine-field elastic device code: one fused kernel per classic-RK4 stage.
+//
+// Each thread owns one physical node: 27 MacCormack-DRP derivatives of the stage input, the
+// metric transform to physical gradients, the nine rates of src/three_d/PointKernels3D.hpp:92-112
+// (traction-image momentum near the surface, traction-free surface derivative on the top
+// row, sponge damping, force or moment source), then its part of the RK combine and the
+// tangential-stress projection.  The 3D reference sums the RK stages as
+// (((base + dt/6 k1) + dt/3 k2) + dt/3 k3) + dt/6 k4 (src/three_d/CurvilinearSolver.cpp:91-101),
+// so the accumulator here carries the partial state sum: A = U + dt/6 k1, A += dt/3 k2,
+// A += dt/3 k3, new state = A + dt/6 k4 written over A.
+//
+// Metrics are stored as nine separate arrays (structure of arrays) so that every load of a
+// warp is coalesced; the surface normals and the traction-rate diagnostics only exist for
+// the top row.
+#pragma once
+#include "runtime.cuh"
+#include "stage2d.cuh"
+#include <cstdint>
+
+namespace swl::k3 {
+
+template <class Real> struct Mesh {
+    int nx, ny, nz;
+    long long count, plane;
+    Real h, lambda, mu, density;    // uniform material (used when the material arrays are null)
+    const Real *metric[9];          // d(xi,eta,zeta)/d(x,y,z), row-major 3x3 per node
+    const Real *jac, *damping, *source, *sg[3];
+    const Real *mlambda, *mmu, *mdensity;
+    const Real *normals;            // 3 per surface node (i + nx*j)
+    Real sdir[3];
+    int src_i0, src_i1, src_j0, src_j1, src_k0, src_k1;
+    int dmp_i0, dmp_i1, dmp_j0, dmp_j1, dmp_k1; // damping is zero inside this box
+};
+
+using k2::Clock;
+
+template <class Real> struct StageArgs {
+    Mesh<Real> m;
+    const Real *in;
+    Real *out;
+    const Real *base;
+    Real *acc;
+    const Real *forcing; // 3 per step: source at t, t+dt/2, t+dt
+    const Clock *clock;
+    Real weight;         // stage combine weight: dt/2, dt/2, dt
+    Real w6, w3;         // dt/6, dt/3
+    double *surfRate;    // stage 3: |traction rate| and rate norm per surface node (2 x nx*ny)
+};
+
+using k2::ld;
+
+template <class Real, int DIR>
+__device__ __forceinline__ Real drp5(const Real *__restrict__ v, long long q, long long s, Real h) {
+    return k2::drp5<Real, DIR>(v, q, s, h);
+}
+
+template <class Real>
+__device__ __forceinline__ Real tractionFlux(const Mesh<Real> &m, const Real *__restrict__ w, long long qq, int axis, int comp) {
+    const int F[3][3] = {{3, 6, 7}, {6, 4, 8}, {7, 8, 5}};
+    Real v = Real(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v += ld(m.metric[3 * axis + a] + qq) * ld(w + F[comp][a] * m.count + qq);
+    return ld(m.jac + qq) * v;
+}
+
+// src/three_d/PointKernels3D.hpp:73-91
+template <class Real, int DX, int DY, int DZ>
+__device__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, Real rho) {
+    const Real C[5] = {Real(-.30874), Real(-.6326), Real(1.233), Real(-.3334), Real(.04168)};
+    Real sum = Real(0);
+    for (int axis = 0; axis < 3; ++axis) {
+        const int dir = axis == 0 ? DX : axis == 1 ? DY : DZ;
+        const long long s = axis == 0 ? 1 : axis == 1 ? m.nx : m.plane;
+        for (int l = 0; l < 5; ++l) {
+            const int pos = l - 1;
+            int off = dir ? -pos : pos;
+            const Real c = dir ? -C[l] : C[l];
+            Real sign = Real(1);
+            if (axis == 2) {
+                const int z = depth + off;
+                if (z == 0) continue;
+                if (z < 0) {
+                    off = -z - depth;
+                    sign = Real(-1);
+                }
+            }
+            sum += sign * c * tractionFlux(m, w, q + off * s, axis, comp);
+        }
+    }
+    return sum / (m.h * ld(m.jac + q) * rho);
+}
+
+template <class Real, int DX, int DY, int DZ, int STAGE>
+__global__ void __launch_bounds__(256) stage3d(const StageArgs<Real> p) {
+    const Mesh<Real> &m = p.m;
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    if (i >= m.nx - 3 || j >= m.ny - 3) return;
+    const Clock *clk = p.clock;
+    if (clk->faulted) return;
+    const long long n = m.count, nx = m.nx, plane = m.plane;
+    const long long q = i + nx * j + plane * k;
+    const int depth = k - 3;
+    const Real *__restrict__ w = p.in;
+    const Real h = m.h;
+    const Real lam = m.mlambda ? ld(m.mlambda + q) : m.lambda;
+    const Real mu = m.mmu ? ld(m.mmu + q) : m.mu;
+    const Real rho = m.mdensity ? ld(m.mdensity + q) : m.density;
+    Real M[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) M[c] = ld(m.metric[c] + q);
+
+    // raw xi / eta derivatives of the velocities (also used by the surface solve)
+    Real dv[3][2];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        dv[v][0] = drp5<Real, DX>(w + v * n, q, 1, h);
+        dv[v][1] = drp5<Real, DY>(w + v * n, q, nx, h);
+    }
+    Real dzs[3] = {0, 0, 0};
+    if (depth == 0) { // src/three_d/PointKernels3D.hpp:52-66
+        const Real c[3] = {M[6], M[7], M[8]};
+        const Real c2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2], len = sqrt(c2);
+        const Real nn[3] = {c[0] / len, c[1] / len, c[2] / len};
+        Real g[9], t[3] = {0, 0, 0};
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) g[3 * v + a] = M[a] * dv[v][0] + M[3 + a] * dv[v][1];
+        const Real trace = g[0] + g[4] + g[8];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) t[a] += ((a == b ? lam * trace : Real(0)) + mu * (g[3 * a + b] + g[3 * b + a])) * c[b];
+        const Real normal = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) dzs[a] = -(t[a] - nn[a] * normal) / (mu * c2) - nn[a] * normal / ((lam + 2 * mu) * c2);
+    }
+    Real gr[9][3];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) {
+        Real d0, d1, d2;
+        if (f < 3) {
+            d0 = dv[f][0];
+            d1 = dv[f][1];
+            if (depth == 0) d2 = dzs[f];
+            else if (depth == 1) d2 = k2::near2<Real, DZ>(w + f * n, q, plane, h);
+            else if (depth == 2) d2 = k2::near3<Real, DZ>(w + f * n, q, plane, h);
+            else d2 = drp5<Real, DZ>(w + f * n, q, plane, h);
+        } else {
+            d0 = drp5<Real, DX>(w + f * n, q, 1, h);
+            d1 = drp5<Real, DY>(w + f * n, q, nx, h);
+            d2 = drp5<Real, DZ>(w + f * n, q, plane, h);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gr[f][a] = M[a] * d0 + M[3 + a] * d1 + M[6 + a] * d2;
+    }
+    Real r[9];
+    if (depth <= (DZ ? 3 : 1)) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, a, depth, rho);
+    } else {
+        r[0] = (gr[3][0] + gr[6][1] + gr[7][2]) / rho;
+        r[1] = (gr[6][0] + gr[4][1] + gr[8][2]) / rho;
+        r[2] = (gr[7][0] + gr[8][1] + gr[5][2]) / rho;
+    }
+    if (i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
+        const Real s = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
+        const Real ratio = m.density / rho;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] += s * (m.sg[a] ? ld(m.sg[a] + q) : ld(m.source + q) * m.sdir[a]) * ratio;
+    }
+    const Real div = gr[0][0] + gr[1][1] + gr[2][2];
+    r[3] = lam * div + 2 * mu * gr[0][0];
+    r[4] = lam * div + 2 * mu * gr[1][1];
+    r[5] = lam * div + 2 * mu * gr[2][2];
+    r[6] = mu * (gr[0][1] + gr[1][0]);
+    r[7] = mu * (gr[0][2] + gr[2][0]);
+    r[8] = mu * (gr[1][2] + gr[2][1]);
+    if (!(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
+        const Real d = ld(m.damping + q);
+#pragma unroll
+        for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
+    }
+    const long long sq = i + nx * j; // surface index
+    if (STAGE == 3 && depth == 0 && p.surfRate) {
+        // traction-rate residual of k4 (src/three_d/CurvilinearSolver.cpp:231-239)
+        const double n0 = ld(m.normals + 3 * sq), n1 = ld(m.normals + 3 * sq + 1), n2 = ld(m.normals + 3 * sq + 2);
+        const double t0 = double(r[3]) * n0 + double(r[6]) * n1 + double(r[7]) * n2;
+        const double t1 = double(r[6]) * n0 + double(r[4]) * n1 + double(r[8]) * n2;
+        const double t2 = double(r[7]) * n0 + double(r[8]) * n1 + double(r[5]) * n2;
+        double norm2 = 0;
+#pragma unroll
+        for (int f = 3; f < 9; ++f) norm2 += (f >= 6 ? 2.0 : 1.0) * double(r[f]) * double(r[f]);
+        p.surfRate[sq] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+        p.surfRate[plane + sq] = sqrt(norm2);
+    }
+    Real o[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) {
+        if (STAGE == 0) {
+            const Real u = ld(p.base + f * n + q);
+            p.acc[f * n + q] = u + p.w6 * r[f];
+            o[f] = u + p.weight * r[f];
+        } else if (STAGE < 3) {
+            const Real u = ld(p.base + f * n + q);
+            p.acc[f * n + q] = p.acc[f * n + q] + p.w3 * r[f];
+            o[f] = u + p.weight * r[f];
+        } else {
+            o[f] = p.acc[f * n + q] + p.w6 * r[f];
+        }
+    }
+    if (depth == 0) { // tangential stress projection (PointKernels3D.hpp:36-51)
+        const Real nn[3] = {ld(m.normals + 3 * sq), ld(m.normals + 3 * sq + 1), ld(m.normals + 3 * sq + 2)};
+        const Real s[9] = {o[3], o[6], o[7], o[6], o[4], o[8], o[7], o[8], o[5]};
+        Real t[3] = {0, 0, 0}, x[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) t[a] += s[3 * a + b] * nn[b];
+        const Real nnn = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) x[3 * a + b] = s[3 * a + b] - nn[a] * t[b] - t[a] * nn[b] + nnn * nn[a] * nn[b];
+        o[3] = x[0];
+        o[4] = x[4];
+        o[5] = x[8];
+        o[6] = Real(0.5) * (x[1] + x[3]);
+        o[7] = Real(0.5) * (x[2] + x[6]);
+        o[8] = Real(0.5) * (x[5] + x[7]);
+    }
+    Real *dst = STAGE == 3 ? p.acc : p.out;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) dst[f * n + q] = o[f];
+}
+
+struct Partial {
+    double energy, velocity, rateTraction, rateNorm;
+    double peak[5];
+    int bad, pad;
+};
+
+// Energy, peaks, finiteness and the traction-rate residual of a state
+// (src/three_d/CurvilinearSolver.cpp:214-250, CudaEngine3D.cu:36-55).
+template <class Real>
+__global__ void __launch_bounds__(256) stats3d(const Mesh<Real> m, const Real *__restrict__ w, const double *__restrict__ surfRate,
+                                               const Clock *clk, Partial *out) {
+    __shared__ Partial sh[256];
+    const int t = threadIdx.x + blockDim.x * threadIdx.y;
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    Partial s{};
+    if (i < m.nx - 3 && j < m.ny - 3 && !(clk && clk->faulted)) {
+        const long long n = m.count, q = i + (long long)m.nx * j + m.plane * k;
+        double f[9];
+        for (int c = 0; c < 9; ++c) {
+            f[c] = double(ld(w + c * n + q));
+            if (!isfinite(f[c])) s.bad = 1;
+        }
+        const double lam = m.mlambda ? double(ld(m.mlambda + q)) : double(m.lambda);
+        const double mu = m.mmu ? double(ld(m.mmu + q)) : double(m.mu);
+        const double rho = m.mdensity ? double(ld(m.mdensity + q)) : double(m.density);
+        const double v2 = f[0] * f[0] + f[1] * f[1] + f[2] * f[2];
+        s.velocity = sqrt(v2);
+        s.peak[0] = fabs(f[2]), s.peak[1] = fabs(f[0]), s.peak[2] = fabs(f[1]), s.peak[3] = sqrt(v2);
+        s.peak[4] = fabs((f[3] + f[4] + f[5]) / 3.0);
+        const double mean = (f[3] + f[4] + f[5]) / 3;
+        double dev = 0;
+        for (int c = 0; c < 3; ++c) dev += (f[c + 3] - mean) * (f[c + 3] - mean);
+        for (int c = 6; c < 9; ++c) dev += 2 * f[c] * f[c];
+        const double hh = double(m.h);
+        s.energy = (0.5 * rho * v2 + dev / (4 * mu) + mean * mean / (2 * (lam + 2 * mu / 3))) * double(ld(m.jac + q)) * hh * hh * hh;
+        if (!isfinite(s.energy)) s.bad = 1;
+        if (k == 3 && surfRate) {
+            const long long sq = i + (long long)m.nx * j;
+            s.rateTraction = surfRate[sq];
+            s.rateNorm = surfRate[m.plane + sq];
+        }
+    }
+    sh[t] = s;
+    __syncthreads();
+    for (int stride = 128; stride > 0; stride >>= 1) {
+        if (t < stride) {
+            Partial &x = sh[t];
+            const Partial y = sh[t + stride];
+            x.energy += y.energy;
+            x.velocity = fmax(x.velocity, y.velocity);
+            x.rateTraction = fmax(x.rateTraction, y.rateTraction);
+            x.rateNorm = fmax(x.rateNorm, y.rateNorm);
+            for (int c = 0; c < 5; ++c) x.peak[c] = fmax(x.peak[c], y.peak[c]);
+            x.bad |= y.bad;
+        }
+        __syncthreads();
+    }
+    if (t == 0) out[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = sh[0];
+}
+
+struct Clock3 {
+    double sourcePeak;
+};
+
+// Acceptance rule of CpuSimulation3D::advance (src/three_d/CurvilinearSolver.cpp:475-488):
+// non-finite fields, or energy above 1e4 x the peak of the source window (t <= 3/f).
+template <class Real>
+__global__ void __launch_bounds__(512) verdict3d(const Partial *__restrict__ parts, int nparts, const Real *__restrict__ w,
+                                                  long long count, const long long *__restrict__ receivers, int nrec,
+                                                  double *__restrict__ traces, Clock *clk) {
+    __shared__ Partial sh[512];
+    __shared__ int accept;
+    const int t = threadIdx.x;
+    if (clk->faulted) return;
+    Partial s{};
+    for (int b = t; b < nparts; b += blockDim.x) {
+        const Partial y = parts[b];
+        s.energy += y.energy;
+        s.velocity = fmax(s.velocity, y.velocity);
+        s.rateTraction = fmax(s.rateTraction, y.rateTraction);
+        s.rateNorm = fmax(s.rateNorm, y.rateNorm);
+        for (int c = 0; c < 5; ++c) s.peak[c] = fmax(s.peak[c], y.peak[c]);
+        s.bad |= y.bad;
+    }
+    sh[t] = s;
+    __syncthreads();
+    for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if (t < stride) {
+            Partial &x = sh[t];
+            const Partial y = sh[t + stride];
+            x.energy += y.energy;
+            x.velocity = fmax(x.velocity, y.velocity);
+            x.rateTraction = fmax(x.rateTraction, y.rateTraction);
+            x.rateNorm = fmax(x.rateNorm, y.rateNorm);
+            for (int c = 0; c < 5; ++c) x.peak[c] = fmax(x.peak[c], y.peak[c]);
+            x.bad |= y.bad;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const Partial tot = sh[0];
+        const double ratio = tot.rateTraction / fmax(tot.rateNorm, 1.0e-30);
+        const bool finite = !tot.bad && isfinite(tot.energy) && isfinite(ratio);
+        const double tnext = (clk->step + 1) * clk->dt;
+        // the source-window peak lives in peak_energy
+        double peak = clk->peak_energy;
+        if (tnext <= clk->growth_after) peak = fmax(peak, tot.energy);
+        const bool growth = tnext > clk->growth_after && peak > 0 && tot.energy > 1e4 * peak;
+        const int ok = finite && !growth;
+        clk->finite = finite;
+        if (ok) {
+            clk->peak_energy = peak;
+            clk->energy = tot.energy;
+            clk->max_velocity = tot.velocity;
+            clk->traction = ratio;
+        }
+        accept = ok;
+    }
+    __syncthreads();
+    if (!accept) {
+        if (t == 0) clk->faulted = 1, clk->fault_step = clk->step;
+        return;
+    }
+    const int row = clk->step - clk->first;
+    if (row < clk->trace_steps)
+        for (int r = t; r < nrec; r += blockDim.x) {
+            const long long qq = receivers[r];
+            for (int c = 0; c < 3; ++c) traces[((long long)row * nrec + r) * 3 + c] = double(w[c * count + qq]);
+        }
+    __syncthreads();
+    if (t == 0) clk->step += 1, clk->accepted += 1;
+}
+
+} // namespace swl::k3
