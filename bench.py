@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the curvilinear velocity-stress RK4 step on B200.
+
+One "step" is one accepted classic-RK4 time step of a whole shot (four fused stage kernels, the
+device-side diagnostics/acceptance verdict and the receiver recording).  Default workload: the
+5001x2001 2D elastic curvilinear shot (seeded terrain and layers, 30-cell CFS-PML, explosive
+source), plain FP64.  Metric: grid-point RK4 updates per second (Mpt-updates/s), computational
+nodes (absorber strips included, ghosts excluded) x steps / time.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl swl|reference] [--workload NAME]
+
+* value      : device time (CUDA events on the engine's stream) of K steps, state resident in HBM
+* e2e        : the same K steps through the public session API (Simulation2D.advance): forcing
+               uploads from pinned host memory and receiver traces downloaded every step, wall time
+* roofline   : algorithmic HBM bytes of the stage kernels / their event-timed duration
+* cpu_baseline: the reference's own CPU solver (oracle/_ref, built from its sources) on a bounded
+               sample of the same shot, all host threads
+* N > 1      : one independent shot per GPU (shots never exchange data); weak scaling
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "seiswavelab--curvilinear_b200"
+METRIC = "Mpt-updates/s & shots/hr: batched FP32 vs plain FP64 on B200 at <=1e-4 trace L2"
+UNIT = "Mpt-updates/s"
+
+
+def load_package():
+    if "swl_b200" in sys.modules:
+        return sys.modules["swl_b200"]
+    spec = importlib.util.spec_from_file_location("swl_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["swl_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(name: str, precision: int) -> tuple[dict, str]:
+    import importlib
+    W = importlib.import_module("swl_b200.workloads")
+    if name == "curvilinear_large":
+        return W.curvilinear_large(precision=precision), "2D elastic curvilinear 5001x2001 h=2 m, seeded terrain (60 m relief), 5 layers, explosive source 10 m deep, 30-cell CFS-PML, 1000 receivers"
+    if name == "small":
+        return W.curvilinear_large(precision=precision, nx=2001, nz=801), "2D elastic curvilinear 2001x801 (profiling size of curvilinear_large)"
+    if name == "plain_small":
+        return W.plain_small(precision=precision), "2D elastic 500x200 flat, 3 layers, surface force, 20-cell CFS-PML"
+    if name == "gsls_medium":
+        return W.gsls_medium(precision=precision), "2D GSLS (3 mechanisms) 2001x801, 40 m sinusoidal terrain, 30-cell CFS-PML"
+    if name == "elastic_3d":
+        return W.elastic_3d(precision=precision), "3D nine-field elastic 400x288x200 h=10 m, DEM terrain, 3 layers, 20-cell sponge"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def source_scale_2d(p: dict) -> float:
+    # src/two_d/CurvilinearSolver2D.cpp:558-561: (moment or force per length) / h^2
+    amp = p.get("momentPerLength", 2e6) if int(p.get("sourceKind", 0)) == 1 else p.get("forcePerLength", 2e5)
+    return amp / (p["spacing"] ** 2)
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.lines, self.proc, self.thread = gpu, [], None, None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=lambda: [self.lines.append(l) for l in self.proc.stdout], daemon=True)
+        self.thread.start()
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_baseline(params: dict, dim: int, steps: int, warmup: int) -> dict | None:
+    """The reference's own CPU solver on a bounded sample of the same shot, all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    threads = min(64, os.cpu_count() or 1)
+    run = O.run_reference_2d if dim == 2 else O.run_reference_3d
+    ref = O.REF2D if dim == 2 else O.REF3D
+    if not ref.exists():
+        return None
+    p = dict(params)
+    p["maxSteps"] = warmup + steps
+    p["precision"] = 0
+    r = run(p, steps=steps, threads=threads, dump_mesh=False, warmup=warmup)
+    pts = float(np.prod([int(r[k]) - 6 for k in (("nx", "nz") if dim == 2 else ("nx", "ny", "nz"))]))
+    sec = float(r["runMs"]) / 1e3
+    return {"value": pts * steps / sec / 1e6, "unit": UNIT, "cores": int(r["threads"]), "kind": "reference",
+            "sample": f"{steps} timed steps after {warmup} warm-up of the same shot (reference CPU solver, FP64, "
+                      f"{int(r['threads'])} OpenMP threads); {float(r['msPerStep']):.1f} ms/step, init {float(r['initMs'])/1e3:.1f} s"}
+
+
+def traffic_from_profiles(workload_name: str, dtype: str):
+    path = ROOT / "profiles" / "traffic.json"
+    try:
+        t = json.loads(path.read_text())
+        return t.get(f"{workload_name}:{dtype}")
+    except Exception:
+        return None
+
+
+def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
+    """Device time of `steps` engine steps on torch's current stream; returns (ms, profile)."""
+    L = swl.library()
+    eng = C.c_void_p(sim.engine_handle())
+    info = sim.info()
+    dt, f = info["dt"], float(params["frequency"])
+    stream = torch.cuda.Stream()  # a real stream: handle 0 would mean "the engine's own stream"
+    acc = C.c_int32()
+    set_stream = L.swl2d_set_stream if dim == 2 else L.swl3d_set_stream
+    swl._check(set_stream(eng, C.c_void_p(stream.cuda_stream)))
+
+    def run(first, n):
+        if dim == 2:
+            st = L.swl2d_advance(eng, first, n, dt, f, source_scale_2d(params), 3.0 / f, C.byref(acc))
+        else:
+            st = L.swl3d_advance(eng, first, n, dt, f, 3.0 / f, C.byref(acc))
+        swl._check(st)
+
+    step = info["step"]
+    run(step, warmup)
+    step += warmup
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    run(step, steps)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    step += steps
+    prof = swl.Profile()
+    if dim == 2:
+        swl._check(L.swl2d_profile(eng, step, 8, dt, f, source_scale_2d(params), C.byref(prof)))
+    else:
+        swl._check(L.swl3d_profile(eng, step, 8, dt, f, C.byref(prof)))
+    swl._check(set_stream(eng, None))
+    return ms, prof.as_dict()
+
+
+def gpu_arm(args):
+    import torch
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as D
+        torch.cuda.set_device(local)
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = D
+    torch.cuda.set_device(local)
+    swl = load_package()
+    import importlib
+    S = importlib.import_module("swl_b200.session")
+    dim = 3 if args.workload == "elastic_3d" else 2
+    Sim = S.Simulation2D if dim == 2 else S.Simulation3D
+    peak, peak_src = measured_hbm_peak()
+
+    def measure(precision):
+        params, desc = workload(args.workload, precision)
+        t0 = time.perf_counter()
+        sim = Sim(params, device=local)
+        init_s = time.perf_counter() - t0
+        info = sim.info()
+        pts = (info["nx"] - 6) * (info["nz"] - 6) if dim == 2 else (info["nx"] - 6) * (info["ny"] - 6) * (info["nz"] - 6)
+        sampler = ClockSampler(local) if precision == 0 and rank == 0 else None
+        if sampler:
+            sampler.start()
+        ms, prof = time_engine(swl, sim, dim, params, args.steps, args.warmup, torch, dist, rank)
+        clocks = sampler.stop() if sampler else None
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        stage_ms = sum(prof["stage_ms"])
+        achieved = prof["bytes_per_step"] / (stage_ms * 1e-3) / 1e9
+        res = {"value": world * pts * args.steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / args.steps, "points": pts,
+               "init_s": init_s, "profile": prof, "desc": desc, "params": params, "clocks": clocks,
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                            "traffic": traffic_from_profiles(args.workload, "f64" if precision == 0 else "f32"),
+                            "kernel": "fused RK stage kernels (4 per step)", "peak_source": peak_src,
+                            "bytes_per_step": prof["bytes_per_step"], "stage_ms_per_step": stage_ms}}
+        return sim, res
+
+    sim64, r64 = measure(0)
+    # e2e: the same K steps through the public session API (host forcing upload and trace
+    # download inside the timed region), from a reset shot.
+    sim64.reset()
+    sim64.advance(max(1, args.warmup))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    sim64.advance(args.steps)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    info = sim64.info()
+    nrec = info["receivers"]
+    e2e = {"value": world * r64["points"] * args.steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": 3 * 8, "d2h_bytes_per_step": (2 if dim == 2 else 3) * 8 * nrec,
+           "api": "Simulation.advance (session C ABI), wall time"}
+    del sim64
+    r32 = None
+    if not args.no_fp32:
+        sim32, r32 = measure(1)
+        del sim32
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        base = cpu_baseline(r64["params"], dim, args.cpu_steps, 1)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r64["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded terrain/layers/sources, PCG64)",
+            "config": {"workload": args.workload, "description": r64["desc"], "points": r64["points"],
+                       "precision": "fp64 plain", "l2": "inputs larger than L2 (resident state and model > 2 GB)",
+                       "parallelism": "one independent shot per GPU" if world > 1 else "single shot",
+                       "init_s": round(r64["init_s"], 3)},
+            "roofline": r64["roofline"], "e2e": e2e, "gpu_launches": int(args.steps * r64["profile"]["launches_per_step"]),
+            "clocks": r64["clocks"], "cpu_baseline": base,
+        }
+        if r32:
+            line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],
+                            "roofline": r32["roofline"], "speedup_vs_fp64": r32["value"] / r64["value"]}
+        line["profile_fp64"] = r64["profile"]
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    load_package()
+    dim = 3 if args.workload == "elastic_3d" else 2
+    params, desc = workload(args.workload, 0)
+    steps = min(args.steps, args.cpu_steps)
+    base = cpu_baseline(params, dim, steps, min(args.warmup, 2))
+    if base is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver binaries (oracle/_ref) are not built"}))
+        return
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
+        "warmup": min(args.warmup, 2), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded terrain/layers/sources, PCG64)",
+        "config": {"workload": args.workload, "description": desc, "precision": "fp64 plain"},
+        "cpu_baseline": base, "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", choices=["swl", "reference"], default="swl")
+    ap.add_argument("--workload", default="curvilinear_large",
+                    choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d"])
+    ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

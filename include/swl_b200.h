@@ -120,6 +120,21 @@ swl_status swl2d_load_field(swl2d_engine *engine, int32_t field, const double *v
 swl_status swl2d_probes(swl2d_engine *engine, const int64_t *nodes, int32_t n, double *out5);
 int64_t swl2d_resident_bytes(const swl2d_engine *engine);
 
+/* Kernel timing of `count` steps run one launch at a time with CUDA events around every
+ * kernel (the steps are real, accepted steps of the simulation).  No counterpart in the
+ * reference (its own timing is host wall time per advance, CurvilinearSolver2D.cpp:553-596). */
+typedef struct swl_profile {
+    double stage_ms[4]; /* mean duration of each RK-stage kernel */
+    double stats_ms, verdict_ms, step_ms;
+    int64_t steps, launches_per_step;
+    double bytes_per_step; /* algorithmic HBM bytes of the four stage kernels per step */
+} swl_profile;
+swl_status swl2d_profile(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency, double scale,
+                         swl_profile *out);
+/* Run the engine's work on a caller-provided cudaStream_t (NULL restores its own stream).
+ * No counterpart in the reference (its engines launch on the legacy default stream). */
+swl_status swl2d_set_stream(swl2d_engine *engine, void *cuda_stream);
+
 /* ---------------------------------------------------------------- engine, 3D ---- */
 
 /* POD mirror of Seis3D::Curvilinear::Point::Mesh (src/three_d/PointKernels3D.hpp:13-21),
@@ -163,6 +178,10 @@ swl_status swl3d_traces(swl3d_engine *engine, int32_t first, int32_t count, doub
 swl_status swl3d_snapshot(swl3d_engine *engine, int32_t field, double *out);
 swl_status swl3d_load_field(swl3d_engine *engine, int32_t field, const double *values);
 int64_t swl3d_resident_bytes(const swl3d_engine *engine);
+/* As swl2d_profile / swl2d_set_stream (no counterpart in the reference). */
+swl_status swl3d_profile(swl3d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
+                         swl_profile *out);
+swl_status swl3d_set_stream(swl3d_engine *engine, void *cuda_stream);
 
 #ifdef __cplusplus
 }

@@ -266,7 +266,7 @@ def _load_dir(d: Path) -> dict:
 
 
 def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_mesh: bool = True,
-                  workdir: Path | None = None, timeout: float | None = None) -> dict:
+                  workdir: Path | None = None, timeout: float | None = None, warmup: int = 0) -> dict:
     exe = REF2D if dim == 2 else REF3D
     if not exe.exists():
         raise FileNotFoundError(f"{exe} is not built (make -C oracle ref)")
@@ -279,7 +279,8 @@ def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_
     write_case(case, workdir / "case.txt")
     out = workdir / "out"
     proc = subprocess.run([str(exe), str(workdir / "case.txt"), str(out), str(steps), str(threads),
-                           "1" if dump_mesh else "0"], capture_output=True, text=True, timeout=timeout)
+                           "1" if dump_mesh else "0", str(int(warmup))], capture_output=True, text=True,
+                          timeout=timeout)
     if proc.returncode != 0:
         raise RuntimeError(f"reference {dim}D run failed ({proc.returncode}): {proc.stderr.strip()}")
     res = _load_dir(out)

@@ -4,7 +4,7 @@
 // float64 files.  Nothing in the product links or runs this program; tests use it as
 // the parity truth and bench.py times it as the reference CPU arm.
 //
-// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1]
+// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps]
 //   steps  : accepted RK4 steps to run (default: the session's total)
 //   threads: ComputeSettings3D::cpuThreads (0 = reference default)
 //
@@ -150,7 +150,7 @@ template <class A> std::vector<double> doubles(const A &a) { return a.toDouble()
 int main(int argc, char **argv) {
     try {
         if (argc < 3) {
-            std::cerr << "usage: ref2d case.txt outdir [steps] [threads] [dump_mesh]\n";
+            std::cerr << "usage: ref2d case.txt outdir [steps] [threads] [dump_mesh] [warmup]\n";
             return 2;
         }
         const Case c{readCase(argv[1])};
@@ -199,6 +199,9 @@ int main(int argc, char **argv) {
                 write(out, s1.c_str(), doubles(s.deltaS[l]));
             }
         }
+        // Optional untimed warm-up (benchmarks/ComputeBenchmark.cpp:71-75 times after warm-up).
+        const int warmup = argc > 6 ? std::max(0, std::atoi(argv[6])) : 0;
+        if (warmup > 0 && !sim.advance(warmup, error)) std::cerr << "warm-up failed: " << error << '\n';
         const auto t1 = std::chrono::steady_clock::now();
         if (steps > 0 && !sim.advance(steps, error)) {
             std::ofstream(out / "error.txt") << error << '\n';

@@ -3,7 +3,7 @@
 // file and dumps the FP64 model arrays, receiver traces and final wavefields as
 // little-endian float64 files.  The product never links or runs this program.
 //
-// Usage: ref3d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1]
+// Usage: ref3d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps]
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -140,7 +140,7 @@ void write(const std::filesystem::path &dir, const std::string &name, const std:
 int main(int argc, char **argv) {
     try {
         if (argc < 3) {
-            std::cerr << "usage: ref3d case.txt outdir [steps] [threads] [dump_mesh]\n";
+            std::cerr << "usage: ref3d case.txt outdir [steps] [threads] [dump_mesh] [warmup]\n";
             return 2;
         }
         const auto c = readCase(argv[1]);
@@ -177,6 +177,8 @@ int main(int argc, char **argv) {
                 write(out, "materialDensity.bin", s.materialDensity);
             }
         }
+        const int warmup = argc > 6 ? std::max(0, std::atoi(argv[6])) : 0;
+        if (warmup > 0 && !sim.advance(warmup, error)) std::cerr << "warm-up failed: " << error << '\n';
         const auto t1 = std::chrono::steady_clock::now();
         if (steps > 0 && !sim.advance(steps, error)) {
             std::ofstream(out / "error.txt") << error << '\n';

@@ -73,6 +73,17 @@ class Diag3D(C.Structure):
                 ("rhs_registers", C.c_int32), ("resident_bytes", C.c_int64)]
 
 
+class Profile(C.Structure):
+    _fields_ = [("stage_ms", C.c_double * 4), ("stats_ms", C.c_double), ("verdict_ms", C.c_double),
+                ("step_ms", C.c_double), ("steps", C.c_int64), ("launches_per_step", C.c_int64),
+                ("bytes_per_step", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"stage_ms": list(self.stage_ms), "stats_ms": self.stats_ms, "verdict_ms": self.verdict_ms,
+                "step_ms": self.step_ms, "steps": self.steps, "launches_per_step": self.launches_per_step,
+                "bytes_per_step": self.bytes_per_step}
+
+
 _lib = None
 
 
@@ -120,6 +131,11 @@ def library() -> C.CDLL:
     L.swl3d_load_field.argtypes = [C.c_void_p, C.c_int32, _dp]
     L.swl3d_resident_bytes.argtypes = [C.c_void_p]
     L.swl3d_resident_bytes.restype = C.c_int64
+    L.swl2d_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                C.POINTER(Profile)]
+    L.swl3d_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(Profile)]
+    L.swl2d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.swl3d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
@@ -247,6 +263,14 @@ class Engine2D:
     def resident_bytes(self) -> int:
         return int(library().swl2d_resident_bytes(self._h))
 
+    def profile(self, first, count, dt, frequency, scale) -> dict:
+        p = Profile()
+        _check(library().swl2d_profile(self._h, first, count, dt, frequency, scale, C.byref(p)))
+        return p.as_dict()
+
+    def set_stream(self, stream_handle: int | None):
+        _check(library().swl2d_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
 
 class Engine3D:
     """GPU engine for one 3D shot.  Mesh keys: nx, ny, nz (padded), h, lambda, mu, density,
@@ -334,3 +358,11 @@ class Engine3D:
 
     def resident_bytes(self) -> int:
         return int(library().swl3d_resident_bytes(self._h))
+
+    def profile(self, first, count, dt, frequency) -> dict:
+        p = Profile()
+        _check(library().swl3d_profile(self._h, first, count, dt, frequency, C.byref(p)))
+        return p.as_dict()
+
+    def set_stream(self, stream_handle: int | None):
+        _check(library().swl3d_set_stream(self._h, C.c_void_p(stream_handle or 0)))

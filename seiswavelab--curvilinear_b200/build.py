@@ -29,6 +29,11 @@ UNITS = {
     "engine3d_f64.cu": ["--fmad=false"],
     "engine3d_f32.cu": [],
     "abi.cpp": ["-x", "cu"],
+    # C++20 host: model construction and sessions (no FMA on the host either, as in the reference)
+    "host/gsls.cpp": [],
+    "host/model2d.cpp": [],
+    "host/model3d.cpp": [],
+    "host/session.cpp": [],
 }
 
 
@@ -41,13 +46,13 @@ def nvcc() -> str:
 
 def _deps() -> float:
     """Newest modification time among headers (any header change rebuilds everything)."""
-    stamps = [p.stat().st_mtime for p in list(SRC.glob("*.cuh")) + list(SRC.glob("*.h")) + list(INCLUDE.glob("*.h"))]
+    stamps = [p.stat().st_mtime for p in list(SRC.rglob("*.cuh")) + list(SRC.rglob("*.hpp")) + list(INCLUDE.glob("*.h"))]
     return max(stamps) if stamps else 0.0
 
 
 def _compile(unit: str, flags: list[str], verbose: bool, newest: float) -> Path:
     src = SRC / unit
-    obj = OUT / (unit + ".o")
+    obj = OUT / (unit.replace("/", "_") + ".o")
     if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest):
         return obj
     cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]

@@ -6,8 +6,15 @@
 #include <cstring>
 #include <string>
 
+namespace swl {
+std::string &lastErrorRef() {
+    thread_local std::string message;
+    return message;
+}
+} // namespace swl
+
 namespace {
-thread_local std::string lastError;
+#define lastError (swl::lastErrorRef())
 
 template <class F> swl_status guarded(F &&f) {
     try {
@@ -159,6 +166,20 @@ swl_status swl2d_probes(swl2d_engine *e, const int64_t *nodes, int32_t n, double
     });
 }
 int64_t swl2d_resident_bytes(const swl2d_engine *e) { return e && e->impl ? e->impl->residentBytes() : 0; }
+swl_status swl2d_profile(swl2d_engine *e, int32_t first, int32_t count, double dt, double frequency, double scale,
+                         swl_profile *out) {
+    return guarded([&] {
+        ENGINE(e);
+        need(out, "out");
+        if (E.faulted()) throw swl::Error(SWL_ERR_STATE, "2D engine holds a rejected step; reset or rebuild it");
+        if (!(dt > 0) || first < 0 || count <= 0 || count > 4096)
+            throw swl::Error(SWL_ERR_INVALID, "profile needs dt > 0, first >= 0 and 1..4096 steps");
+        E.profile(first, count, dt, frequency, scale, *out);
+    });
+}
+swl_status swl2d_set_stream(swl2d_engine *e, void *stream) {
+    return guarded([&] { ENGINE(e); E.setStream(static_cast<cudaStream_t>(stream)); });
+}
 
 // ----------------------------------------------------------------------------- 3D
 swl_status swl3d_create(const swl_mesh3d *mesh, const int64_t *receivers, int32_t n, int32_t dev, swl3d_engine **out) {
@@ -236,5 +257,18 @@ swl_status swl3d_load_field(swl3d_engine *e, int32_t field, const double *values
     });
 }
 int64_t swl3d_resident_bytes(const swl3d_engine *e) { return e && e->impl ? e->impl->residentBytes() : 0; }
+swl_status swl3d_profile(swl3d_engine *e, int32_t first, int32_t count, double dt, double frequency, swl_profile *out) {
+    return guarded([&] {
+        ENGINE(e);
+        need(out, "out");
+        if (E.faulted()) throw swl::Error(SWL_ERR_STATE, "3D engine holds a rejected step; reset or rebuild it");
+        if (!(dt > 0) || first < 0 || count <= 0 || count > 4096)
+            throw swl::Error(SWL_ERR_INVALID, "profile needs dt > 0, first >= 0 and 1..4096 steps");
+        E.profile(first, count, dt, frequency, *out);
+    });
+}
+swl_status swl3d_set_stream(swl3d_engine *e, void *stream) {
+    return guarded([&] { ENGINE(e); E.setStream(static_cast<cudaStream_t>(stream)); });
+}
 
 } // extern "C"

@@ -38,6 +38,8 @@ class Engine2D {
     virtual void probes(const int64_t *nodes, int n, double *out5) = 0;
     virtual int64_t residentBytes() const = 0;
     virtual bool faulted() const = 0;
+    virtual void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) = 0;
+    virtual void setStream(cudaStream_t stream) = 0;
 };
 
 std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &, const int64_t *, int, int);
@@ -94,7 +96,7 @@ template <class Real> std::vector<Real> convert(const void *src, std::size_t n, 
 
 template <class Real> class TypedEngine2D final : public Engine2D {
     int device_{};
-    cudaStream_t stream_{};
+    cudaStream_t stream_{}, ownStream_{};
     k2::Mesh<Real> m_{};
     int mech_{}, fc_{};
     long long count_{}, pcount_{};
@@ -146,18 +148,32 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     }
     double dt_{};
     // Enqueue one step: 4 stages (+ diagnostics and verdict when `verdict`).  Swaps roles.
-    void enqueueStep(int step, bool verdict) {
-        for (int s = 0; s < 4; ++s)
+    // `ev`, when given, receives 7 events: before stage 0, after each stage, after stats, after verdict.
+    void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
+        if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
+        for (int s = 0; s < 4; ++s) {
             detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, grid_, block_, stream_, args(s));
+            if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
+        }
         check(cudaGetLastError(), "2D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
             k2::stats2d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, pset_[a_], clock_.as<k2::Clock>(), partials_.as<k2::Partial>());
+            if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
             k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), nparts_, fresh, count_, recIdx_.as<long long>(),
                                                          nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
+            if (ev) check(cudaEventRecord(ev[6], stream_), "record event");
             check(cudaGetLastError(), "2D verdict launch");
         }
         std::swap(u_, a_);
+    }
+    // Algorithmic HBM bytes of the four stage kernels of one step: 17 F + 4 M per physical
+    // node (stage reads/writes of U, A, S and the per-node model arrays a, b, rho, lambda, mu
+    // and the GSLS strengths) plus 17 values per CFS-PML memory.
+    double bytesPerStep() const {
+        const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.nz - 6);
+        const double F = fc_ * s, M = (5 + 2 * mech_) * s;
+        return points * (17 * F + 4 * M) + double(pcount_) * 17 * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -202,7 +218,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         if (g.mechanisms < 0 || g.mechanisms > 3 || g.field_count != (g.mechanisms ? 6 + 4 * g.mechanisms : 5))
             throw Error(SWL_ERR_INVALID, "2D mesh field_count must be 5 (elastic) or 6 + 4*mechanisms (GSLS)");
         if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
-        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
+        check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "create stream");
+        stream_ = ownStream_;
         const std::size_t n = std::size_t(g.count);
         count_ = g.count;
         mech_ = g.mechanisms;
@@ -305,10 +322,50 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         localBytes_ = attr.localSizeBytes;
     }
     ~TypedEngine2D() override {
+        if (stream_) cudaStreamSynchronize(stream_);
         dropGraphs();
-        if (stream_) cudaStreamDestroy(stream_);
+        if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
+    void setStream(cudaStream_t s) override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "drain stream");
+        stream_ = s ? s : ownStream_;
+    }
+    void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) override {
+        DeviceScope scope(device_);
+        if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
+        if (dt != dt_) dropGraphs(), dt_ = dt;
+        ensureCapacity(count);
+        hostClock_.step = hostClock_.first = first;
+        hostClock_.faulted = 0, hostClock_.fault_step = -1, hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_, hostClock_.dt = dt, hostClock_.growth_after = 3 / frequency;
+        pushClock();
+        fillForcing(first, count, dt, frequency, scale);
+        std::vector<cudaEvent_t> ev(7 * std::size_t(count));
+        for (auto &e : ev) check(cudaEventCreate(&e), "create event");
+        const int u0 = u_;
+        for (int j = 0; j < count; ++j) enqueueStep(first + j, true, ev.data() + 7 * j);
+        pullClock();
+        out = swl_profile{};
+        for (int j = 0; j < count; ++j) {
+            float ms;
+            const cudaEvent_t *e = ev.data() + 7 * j;
+            for (int s = 0; s < 4; ++s) check(cudaEventElapsedTime(&ms, e[s], e[s + 1]), "event time"), out.stage_ms[s] += ms / count;
+            check(cudaEventElapsedTime(&ms, e[4], e[5]), "event time"), out.stats_ms += ms / count;
+            check(cudaEventElapsedTime(&ms, e[5], e[6]), "event time"), out.verdict_ms += ms / count;
+            check(cudaEventElapsedTime(&ms, e[0], e[6]), "event time"), out.step_ms += ms / count;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        out.steps = hostClock_.accepted;
+        out.launches_per_step = 6;
+        out.bytes_per_step = bytesPerStep();
+        const int accepted = hostClock_.accepted;
+        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+    }
 
     void step(double dt, double frequency, double scale, int step) override {
         DeviceScope scope(device_);

@@ -27,6 +27,8 @@ class Engine3D {
     virtual void load(int field, const double *in) = 0;
     virtual int64_t residentBytes() const = 0;
     virtual bool faulted() const = 0;
+    virtual void profile(int first, int count, double dt, double frequency, swl_profile &out) = 0;
+    virtual void setStream(cudaStream_t stream) = 0;
 };
 
 std::unique_ptr<Engine3D> makeEngine3D64(const swl_mesh3d &, const int64_t *, int, int);
@@ -60,7 +62,7 @@ template <class Real> struct Launch {
 
 template <class Real> class TypedEngine3D final : public Engine3D {
     int device_{};
-    cudaStream_t stream_{};
+    cudaStream_t stream_{}, ownStream_{};
     k3::Mesh<Real> m_{};
     long long count_{};
     std::vector<DeviceBuffer> model_;
@@ -118,20 +120,33 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         p.surfRate = surfRate_.as<double>();
         return p;
     }
-    void enqueueStep(int step, bool verdict) {
-        for (int s = 0; s < 4; ++s)
+    void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
+        if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
+        for (int s = 0; s < 4; ++s) {
             detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, grid_, block_,
                                          stream_, args(s));
+            if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
+        }
         check(cudaGetLastError(), "3D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
             k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, surfRate_.as<double>(), clock_.as<k2::Clock>(),
                                                              partials_.as<k3::Partial>());
+            if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
             k3::verdict3d<Real><<<1, 512, 0, stream_>>>(partials_.as<k3::Partial>(), nparts_, fresh, count_,
                                                          recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>());
+            if (ev) check(cudaEventRecord(ev[6], stream_), "record event");
             check(cudaGetLastError(), "3D verdict launch");
         }
         std::swap(u_, a_);
+    }
+    // Algorithmic HBM bytes of the four stage kernels of one step: 16 F + 4 M per physical node
+    // (the accumulator carries the partial state sum, so the last stage does not read U); M =
+    // nine metrics plus lambda, mu, rho when the material varies.
+    double bytesPerStep() const {
+        const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
+        const double F = 9 * s, M = (m_.mlambda ? 12 : 9) * s;
+        return points * (16 * F + 4 * M);
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -181,7 +196,8 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         if (!g.metrics || !g.jacobian || !g.source || !g.damping || !g.normals)
             throw Error(SWL_ERR_INVALID, "3D mesh arrays (metrics, jacobian, source, damping, normals) are required");
         if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
-        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
+        check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "create stream");
+        stream_ = ownStream_;
         const std::size_t n = std::size_t(g.count);
         count_ = g.count;
         nrec_ = nrec;
@@ -274,10 +290,50 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         registers_ = attr.numRegs;
     }
     ~TypedEngine3D() override {
+        if (stream_) cudaStreamSynchronize(stream_);
         dropGraphs();
-        if (stream_) cudaStreamDestroy(stream_);
+        if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
+    void setStream(cudaStream_t s) override {
+        DeviceScope scope(device_);
+        check(cudaStreamSynchronize(stream_), "drain stream");
+        stream_ = s ? s : ownStream_;
+    }
+    void profile(int first, int count, double dt, double frequency, swl_profile &out) override {
+        DeviceScope scope(device_);
+        if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
+        if (dt != dt_) dropGraphs(), dt_ = dt;
+        ensureCapacity(count);
+        hostClock_.step = hostClock_.first = first;
+        hostClock_.faulted = 0, hostClock_.fault_step = -1, hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_, hostClock_.dt = dt, hostClock_.growth_after = 3 / frequency;
+        pushClock();
+        fillForcing(first, count, dt, frequency);
+        std::vector<cudaEvent_t> ev(7 * std::size_t(count));
+        for (auto &e : ev) check(cudaEventCreate(&e), "create event");
+        const int u0 = u_;
+        for (int j = 0; j < count; ++j) enqueueStep(first + j, true, ev.data() + 7 * j);
+        pullClock();
+        out = swl_profile{};
+        for (int j = 0; j < count; ++j) {
+            float ms;
+            const cudaEvent_t *e = ev.data() + 7 * j;
+            for (int s = 0; s < 4; ++s) check(cudaEventElapsedTime(&ms, e[s], e[s + 1]), "event time"), out.stage_ms[s] += ms / count;
+            check(cudaEventElapsedTime(&ms, e[4], e[5]), "event time"), out.stats_ms += ms / count;
+            check(cudaEventElapsedTime(&ms, e[5], e[6]), "event time"), out.verdict_ms += ms / count;
+            check(cudaEventElapsedTime(&ms, e[0], e[6]), "event time"), out.step_ms += ms / count;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        out.steps = hostClock_.accepted;
+        out.launches_per_step = 6;
+        out.bytes_per_step = bytesPerStep();
+        const int accepted = hostClock_.accepted;
+        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+    }
     void step(double dt, double frequency, int step) override {
         DeviceScope scope(device_);
         dt_ = dt;

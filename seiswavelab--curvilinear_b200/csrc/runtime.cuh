@@ -98,6 +98,9 @@ struct PinnedBuffer {
 // Device with the most global memory among sm_100 devices, or -1.
 int selectDevice(int requested);
 
+// The calling thread's last failure message, reported by swl_last_error().
+std::string &lastErrorRef();
+
 // The 8-step MacCormack direction table of include/SeisCommon/FiniteDifference.hpp:9-13
 // (axis 0 = x, 1 = y, 2 = z), flipped at each RK stage.
 inline int direction(int step, int stage, int axis) {
