@@ -103,6 +103,17 @@ swl_status swl2d_step(swl2d_engine *engine, double time, double dt, double frequ
 swl_status swl2d_advance(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
                          double scale, double check_growth_after, int32_t *accepted);
 
+/* Asynchronous form of swl2d_advance for callers that overlap many shots on one device: the
+ * batch is enqueued on the engine's stream and the call returns; swl2d_query reports completion
+ * without blocking (*done = 0/1), swl2d_wait blocks.  Both return SWL_ERR_FAULT once a rejected
+ * step has ended the batch.  Any other call on the engine first waits for the batch.  No
+ * counterpart in the reference, whose AsyncSimulation moves whole advance calls onto a worker
+ * thread (src/two_d/AsyncSimulation2D.cpp:30-58). */
+swl_status swl2d_launch(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency, double scale,
+                        double check_growth_after);
+swl_status swl2d_query(swl2d_engine *engine, int32_t *done, int32_t *accepted);
+swl_status swl2d_wait(swl2d_engine *engine, int32_t *accepted);
+
 swl_status swl2d_rollback(swl2d_engine *engine);    /* CudaEngine::rollback */
 swl_status swl2d_reset(swl2d_engine *engine);       /* CudaEngine::reset: zero fields, memories, traces */
 swl_status swl2d_diagnostics(swl2d_engine *engine, swl_diag2d *out); /* CudaEngine::diagnostics */
@@ -170,6 +181,11 @@ void swl3d_destroy(swl3d_engine *engine);
 swl_status swl3d_step(swl3d_engine *engine, double time, double dt, double frequency, int32_t step);
 swl_status swl3d_advance(swl3d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
                          double check_growth_after, int32_t *accepted);
+/* As swl2d_launch / swl2d_query / swl2d_wait (no counterpart in the reference). */
+swl_status swl3d_launch(swl3d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
+                        double check_growth_after);
+swl_status swl3d_query(swl3d_engine *engine, int32_t *done, int32_t *accepted);
+swl_status swl3d_wait(swl3d_engine *engine, int32_t *accepted);
 swl_status swl3d_rollback(swl3d_engine *engine);
 swl_status swl3d_reset(swl3d_engine *engine);
 swl_status swl3d_diagnostics(swl3d_engine *engine, swl_diag3d *out);

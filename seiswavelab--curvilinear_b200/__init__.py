@@ -14,12 +14,13 @@ Session level (model build + engine), mirroring Simulation / ISimulationBackend3
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libswl_b200.so"
+LIB_PATH = Path(os.environ.get("SWL_B200_LIBRARY", PKG / "libswl_b200.so"))  # override: an alternative build
 
 SWL_FP64, SWL_FP32 = 0, 1
 OK, ERR_INVALID, ERR_CUDA, ERR_MEMORY, ERR_FAULT, ERR_UNAVAILABLE, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
@@ -136,6 +137,12 @@ def library() -> C.CDLL:
     L.swl3d_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(Profile)]
     L.swl2d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.swl3d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.swl2d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
+    L.swl2d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.swl2d_wait.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+    L.swl3d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double]
+    L.swl3d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.swl3d_wait.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
     _lib = L
     return L
 
@@ -217,6 +224,25 @@ class Engine2D:
     def advance(self, first, count, dt, frequency, scale, growth_after=np.inf):
         acc = C.c_int32()
         st = library().swl2d_advance(self._h, first, count, dt, frequency, scale, growth_after, C.byref(acc))
+        if st not in (OK, ERR_FAULT):
+            _check(st)
+        return acc.value, st == ERR_FAULT
+
+    def launch(self, first, count, dt, frequency, scale, growth_after=np.inf):
+        """Enqueue a batch and return at once (see swl2d_launch)."""
+        _check(library().swl2d_launch(self._h, first, count, dt, frequency, scale, growth_after))
+
+    def query(self):
+        """(done, accepted, faulted) of the batch in flight, without blocking."""
+        done, acc = C.c_int32(), C.c_int32()
+        st = library().swl2d_query(self._h, C.byref(done), C.byref(acc))
+        if st not in (OK, ERR_FAULT):
+            _check(st)
+        return bool(done.value), acc.value, st == ERR_FAULT
+
+    def wait(self):
+        acc = C.c_int32()
+        st = library().swl2d_wait(self._h, C.byref(acc))
         if st not in (OK, ERR_FAULT):
             _check(st)
         return acc.value, st == ERR_FAULT

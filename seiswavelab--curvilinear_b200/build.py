@@ -34,6 +34,7 @@ UNITS = {
     "host/model2d.cpp": [],
     "host/model3d.cpp": [],
     "host/session.cpp": [],
+    "host/server.cpp": [],
 }
 
 

@@ -118,6 +118,35 @@ swl_status swl2d_advance(swl2d_engine *e, int32_t first, int32_t count, double d
     if (accepted) *accepted = done;
     return s;
 }
+swl_status swl2d_launch(swl2d_engine *e, int32_t first, int32_t count, double dt, double frequency, double scale,
+                        double growthAfter) {
+    return guarded([&] {
+        ENGINE(e);
+        if (E.faulted()) throw swl::Error(SWL_ERR_STATE, "2D engine holds a rejected step; reset or rebuild it");
+        if (!(dt > 0) || first < 0 || count < 0) throw swl::Error(SWL_ERR_INVALID, "launch needs dt > 0, first >= 0, count >= 0");
+        E.launch(first, count, dt, frequency, scale, growthAfter);
+    });
+}
+swl_status swl2d_query(swl2d_engine *e, int32_t *done, int32_t *accepted) {
+    return guarded([&] {
+        ENGINE(e);
+        need(done, "done");
+        int acc = 0;
+        *done = E.query(acc) ? 1 : 0;
+        if (accepted) *accepted = acc;
+        if (*done && E.faulted())
+            throw swl::Error(SWL_ERR_FAULT, "2D step rejected: nonfinite fields or excessive late energy growth. Rebuild the session.");
+    });
+}
+swl_status swl2d_wait(swl2d_engine *e, int32_t *accepted) {
+    return guarded([&] {
+        ENGINE(e);
+        const int acc = E.finish();
+        if (accepted) *accepted = acc;
+        if (E.faulted())
+            throw swl::Error(SWL_ERR_FAULT, "2D step rejected: nonfinite fields or excessive late energy growth. Rebuild the session.");
+    });
+}
 swl_status swl2d_rollback(swl2d_engine *e) { return guarded([&] { ENGINE(e); E.rollback(); }); }
 swl_status swl2d_reset(swl2d_engine *e) { return guarded([&] { ENGINE(e); E.reset(); }); }
 swl_status swl2d_diagnostics(swl2d_engine *e, swl_diag2d *out) {
@@ -218,6 +247,32 @@ swl_status swl3d_advance(swl3d_engine *e, int32_t first, int32_t count, double d
     });
     if (accepted) *accepted = done;
     return s;
+}
+swl_status swl3d_launch(swl3d_engine *e, int32_t first, int32_t count, double dt, double frequency, double growthAfter) {
+    return guarded([&] {
+        ENGINE(e);
+        if (E.faulted()) throw swl::Error(SWL_ERR_STATE, "3D engine holds a rejected step; reset or rebuild it");
+        if (!(dt > 0) || first < 0 || count < 0) throw swl::Error(SWL_ERR_INVALID, "launch needs dt > 0, first >= 0, count >= 0");
+        E.launch(first, count, dt, frequency, growthAfter);
+    });
+}
+swl_status swl3d_query(swl3d_engine *e, int32_t *done, int32_t *accepted) {
+    return guarded([&] {
+        ENGINE(e);
+        need(done, "done");
+        int acc = 0;
+        *done = E.query(acc) ? 1 : 0;
+        if (accepted) *accepted = acc;
+        if (*done && E.faulted()) throw swl::Error(SWL_ERR_FAULT, "Non-finite RK4 step or energy growth rejected.");
+    });
+}
+swl_status swl3d_wait(swl3d_engine *e, int32_t *accepted) {
+    return guarded([&] {
+        ENGINE(e);
+        const int acc = E.finish();
+        if (accepted) *accepted = acc;
+        if (E.faulted()) throw swl::Error(SWL_ERR_FAULT, "Non-finite RK4 step or energy growth rejected.");
+    });
 }
 swl_status swl3d_rollback(swl3d_engine *e) { return guarded([&] { ENGINE(e); E.rollback(); }); }
 swl_status swl3d_reset(swl3d_engine *e) { return guarded([&] { ENGINE(e); E.reset(); }); }

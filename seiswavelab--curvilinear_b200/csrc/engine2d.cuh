@@ -40,6 +40,11 @@ class Engine2D {
     virtual bool faulted() const = 0;
     virtual void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) = 0;
     virtual void setStream(cudaStream_t stream) = 0;
+    // Asynchronous batches: launch returns once the batch is enqueued; query polls and finish
+    // waits; both return the accepted step count of the batch.
+    virtual void launch(int first, int count, double dt, double frequency, double scale, double growthAfter) = 0;
+    virtual bool query(int &accepted) = 0;
+    virtual int finish() = 0;
 };
 
 std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &, const int64_t *, int, int);
@@ -49,7 +54,30 @@ namespace detail2 {
 
 template <class Real> struct Launch {
     template <int DX, int DZ, int MECH, int ST> static void go(dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-        k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, 0, s>>>(a);
+        k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, k2::tileBytes<Real>(), s>>>(a);
+    }
+    // Opt every instantiation into the tile's dynamic shared memory (above the 48 KB default).
+    template <int DX, int DZ, int MECH, int ST> static void allow() {
+        check(cudaFuncSetAttribute(k2::stage2d<Real, DX, DZ, MECH, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(k2::tileBytes<Real>())),
+              "2D stage shared memory");
+        check(cudaFuncSetAttribute(k2::stage2d<Real, DX, DZ, MECH, ST>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   int(cudaSharedmemCarveoutMaxShared)),
+              "2D stage shared-memory carveout");
+    }
+    template <int DX, int DZ, int MECH> static void allowStages() {
+        allow<DX, DZ, MECH, 0>(), allow<DX, DZ, MECH, 1>(), allow<DX, DZ, MECH, 2>(), allow<DX, DZ, MECH, 3>();
+    }
+    template <int DX, int DZ> static void allowMech(int mech) {
+        switch (mech) {
+        case 0: allowStages<DX, DZ, 0>(); break;
+        case 1: allowStages<DX, DZ, 1>(); break;
+        case 2: allowStages<DX, DZ, 2>(); break;
+        default: allowStages<DX, DZ, 3>(); break;
+        }
+    }
+    static void prepare(int mech) {
+        allowMech<0, 0>(mech), allowMech<0, 1>(mech), allowMech<1, 0>(mech), allowMech<1, 1>(mech);
     }
     template <int DX, int DZ, int MECH> static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
         switch (stage) {
@@ -107,7 +135,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     int u_{0}, a_{1};       // state / accumulator roles among set 0 and 1
     bool previous_{false};  // set a_ holds the state before the last step
     int nrec_{}, traceCap_{}, forcingCap_{};
-    dim3 grid_, block_{32, 8};
+    dim3 grid_, block_{32, 8};                               // one node per thread (diagnostics kernel)
+    dim3 tileGrid_, tileBlock_{k2::TX, k2::TILE_THREADS / k2::TX}; // 32x32-node tiles (stage kernels)
     int nparts_{};
     k2::Clock hostClock_{};
     PinnedBuffer pinnedForcing_, pinnedClock_;
@@ -115,6 +144,12 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     bool faulted_{false};
     int registers_{};
     int64_t localBytes_{};
+    cudaEvent_t done_{};    // completion of the in-flight batch
+    bool inflight_{false};
+    int batchU0_{0};
+    void settle() {
+        if (inflight_) finish();
+    }
 
     Real *upload(const std::vector<Real> &v) {
         model_.emplace_back(v.size() * sizeof(Real));
@@ -144,6 +179,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         p.clock = clock_.as<k2::Clock>();
         p.weight = stage == 2 ? static_cast<Real>(dt_) : static_cast<Real>(dt_ / 2);
         p.delta = static_cast<Real>(dt_);
+        p.partials = nullptr;
         return p;
     }
     double dt_{};
@@ -152,16 +188,17 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
         if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
         for (int s = 0; s < 4; ++s) {
-            detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, grid_, block_, stream_, args(s));
+            auto a = args(s);
+            if (s == 3 && verdict) a.partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
+            detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, tileGrid_, tileBlock_, stream_, a);
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
         check(cudaGetLastError(), "2D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
-            k2::stats2d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, pset_[a_], clock_.as<k2::Clock>(), partials_.as<k2::Partial>());
             if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
-            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), nparts_, fresh, count_, recIdx_.as<long long>(),
-                                                         nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
+            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), int(tileGrid_.x * tileGrid_.y), fresh, count_,
+                                                         recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
             if (ev) check(cudaEventRecord(ev[6], stream_), "record event");
             check(cudaGetLastError(), "2D verdict launch");
         }
@@ -233,6 +270,14 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         m_.nz = g.nz;
         m_.count = g.count;
         m_.h = static_cast<Real>(g.h);
+        {
+            // x/h equals x*(1/h) bit for bit when h is a power of two; the FP32 form always
+            // multiplies by the reciprocal.
+            int e2 = 0;
+            const bool pow2 = g.h > 0 && std::frexp(g.h, &e2) == 0.5;
+            m_.hinv = static_cast<Real>(1.0 / g.h);
+            m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
+        }
         m_.a = arr(g.a, n, "a");
         m_.b = arr(g.b, n, "b");
         m_.jac = arr(g.jac, n, "jac");
@@ -311,10 +356,13 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.nz - 6 + block_.y - 1) / block_.y);
+        tileGrid_ = dim3((g.nx - 6 + k2::TX - 1) / k2::TX, (g.nz - 6 + k2::TZ - 1) / k2::TZ);
         nparts_ = grid_.x * grid_.y;
-        partials_.allocate(nparts_ * sizeof(k2::Partial));
+        partials_.allocate(std::max<std::size_t>(nparts_, tileGrid_.x * tileGrid_.y) * sizeof(k2::Partial));
+        detail2::Launch<Real>::prepare(mech_);
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
+        check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
         cudaFuncAttributes attr{};
         check(cudaFuncGetAttributes(&attr, k2::stage2d<Real, 0, 0, 0, 1>), "2D kernel compatibility");
@@ -322,17 +370,20 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         localBytes_ = attr.localSizeBytes;
     }
     ~TypedEngine2D() override {
+        if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
         if (stream_) cudaStreamSynchronize(stream_);
         dropGraphs();
         if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
     void setStream(cudaStream_t s) override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "drain stream");
         stream_ = s ? s : ownStream_;
     }
     void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) override {
+        settle();
         DeviceScope scope(device_);
         if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
         if (dt != dt_) dropGraphs(), dt_ = dt;
@@ -358,7 +409,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         }
         for (auto &e : ev) cudaEventDestroy(e);
         out.steps = hostClock_.accepted;
-        out.launches_per_step = 6;
+        out.launches_per_step = 5;
         out.bytes_per_step = bytesPerStep();
         const int accepted = hostClock_.accepted;
         u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
@@ -368,6 +419,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     }
 
     void step(double dt, double frequency, double scale, int step) override {
+        settle();
         DeviceScope scope(device_);
         dt_ = dt;
         ensureCapacity(1);
@@ -384,8 +436,46 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     }
 
     int advance(int first, int count, double dt, double frequency, double scale, double growthAfter) override {
+        launch(first, count, dt, frequency, scale, growthAfter);
+        return finish();
+    }
+    // Completion of an in-flight batch: roles after `accepted` steps (a rejected step leaves its
+    // starting state current).
+    void finalize() {
+        hostClock_ = *pinnedClock_.as<k2::Clock>();
+        const int accepted = hostClock_.accepted;
+        u_ = (accepted % 2 == 0) ? batchU0_ : 1 - batchU0_;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+        inflight_ = false;
+    }
+    int finish() override {
+        if (!inflight_) return hostClock_.accepted;
         DeviceScope scope(device_);
-        if (count <= 0) return 0;
+        check(cudaEventSynchronize(done_), "2D batch completion");
+        finalize();
+        return hostClock_.accepted;
+    }
+    bool query(int &accepted) override {
+        if (inflight_) {
+            DeviceScope scope(device_);
+            const cudaError_t e = cudaEventQuery(done_);
+            if (e == cudaErrorNotReady) return false;
+            check(e, "2D batch query");
+            finalize();
+        }
+        accepted = hostClock_.accepted;
+        return true;
+    }
+    // Enqueue a batch of steps on the engine's stream and return immediately.
+    void launch(int first, int count, double dt, double frequency, double scale, double growthAfter) override {
+        DeviceScope scope(device_);
+        if (inflight_) throw Error(SWL_ERR_STATE, "a batch is already in flight on this engine");
+        if (count <= 0) {
+            hostClock_.accepted = 0;
+            return;
+        }
         if (dt != dt_) dropGraphs(), dt_ = dt;
         ensureCapacity(count);
         hostClock_.step = first;
@@ -419,21 +509,20 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             done += 8; // eight role swaps: roles are back where they started
         }
         for (; done < count; ++done) enqueueStep(first + done, true);
-        pullClock();
-        const int accepted = hostClock_.accepted;
-        // Roles after `accepted` steps; a rejected step leaves its starting state current.
-        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
-        a_ = 1 - u_;
-        previous_ = accepted > 0;
-        faulted_ = hostClock_.faulted != 0;
-        return accepted;
+        check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
+        check(cudaEventRecord(done_, stream_), "record batch completion");
+        batchU0_ = u0;
+        u_ = u0, a_ = 1 - u0; // the host view of the roles is settled by finalize()
+        inflight_ = true;
     }
     void rollback() override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "2D rollback");
         if (previous_) std::swap(u_, a_), previous_ = false;
     }
     void reset() override {
+        settle();
         DeviceScope scope(device_);
         check(cudaMemsetAsync(sets_.ptr, 0, sets_.bytes, stream_), "2D reset");
         check(cudaMemsetAsync(psets_.ptr, 0, psets_.bytes, stream_), "2D PML reset");
@@ -444,6 +533,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
     }
     void diagnostics(swl_diag2d &d) override {
+        settle();
         DeviceScope scope(device_);
         k2::stats2d<Real><<<grid_, block_, 0, stream_>>>(m_, set_[u_], pset_[u_], nullptr, partials_.as<k2::Partial>());
         check(cudaGetLastError(), "2D diagnostics");
@@ -478,6 +568,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         check(cudaStreamSynchronize(stream_), "probe completion");
     }
     void sample(double *vx, double *vz) override {
+        settle();
         DeviceScope scope(device_);
         if (!nrec_) return;
         std::vector<int64_t> idx(nrec_);
@@ -487,6 +578,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         for (int r = 0; r < nrec_; ++r) vx[r] = v[2 * r], vz[r] = v[2 * r + 1];
     }
     void traces(int first, int count, double *vx, double *vz) override {
+        settle();
         DeviceScope scope(device_);
         const int row0 = first - hostClock_.first;
         if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
@@ -503,6 +595,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             }
     }
     void snapshot(int field, double *out) override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "snapshot ordering");
         const Real *src;
@@ -515,6 +608,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         for (std::size_t i = 0; i < len; ++i) out[i] = double(tmp[i]);
     }
     void load(int field, const double *in) override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "load ordering");
         Real *dst;
@@ -527,6 +621,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         previous_ = false;
     }
     void probes(const int64_t *nodes, int n, double *out5) override {
+        settle();
         DeviceScope scope(device_);
         gather(nodes, n, 5, out5);
     }

@@ -29,6 +29,9 @@ class Engine3D {
     virtual bool faulted() const = 0;
     virtual void profile(int first, int count, double dt, double frequency, swl_profile &out) = 0;
     virtual void setStream(cudaStream_t stream) = 0;
+    virtual void launch(int first, int count, double dt, double frequency, double growthAfter) = 0;
+    virtual bool query(int &accepted) = 0;
+    virtual int finish() = 0;
 };
 
 std::unique_ptr<Engine3D> makeEngine3D64(const swl_mesh3d &, const int64_t *, int, int);
@@ -80,6 +83,12 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     int registers_{};
     double dt_{}, amplitudeScale_{};
     double hostDensity_{}, hostH_{}, amplitude_{};
+    cudaEvent_t done_{}; // completion of the in-flight batch
+    bool inflight_{false};
+    int batchU0_{0};
+    void settle() {
+        if (inflight_) finish();
+    }
 
     Real *upload(const std::vector<Real> &v) {
         model_.emplace_back(std::max<std::size_t>(1, v.size()) * sizeof(Real));
@@ -284,23 +293,27 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
+        check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
         cudaFuncAttributes attr{};
         check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
         registers_ = attr.numRegs;
     }
     ~TypedEngine3D() override {
+        if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
         if (stream_) cudaStreamSynchronize(stream_);
         dropGraphs();
         if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
     void setStream(cudaStream_t s) override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "drain stream");
         stream_ = s ? s : ownStream_;
     }
     void profile(int first, int count, double dt, double frequency, swl_profile &out) override {
+        settle();
         DeviceScope scope(device_);
         if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
         if (dt != dt_) dropGraphs(), dt_ = dt;
@@ -335,6 +348,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         faulted_ = hostClock_.faulted != 0;
     }
     void step(double dt, double frequency, int step) override {
+        settle();
         DeviceScope scope(device_);
         dt_ = dt;
         ensureCapacity(1);
@@ -349,8 +363,43 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         check(cudaStreamSynchronize(stream_), "3D step completion");
     }
     int advance(int first, int count, double dt, double frequency, double growthAfter) override {
+        launch(first, count, dt, frequency, growthAfter);
+        return finish();
+    }
+    void finalize() {
+        hostClock_ = *pinnedClock_.as<k2::Clock>();
+        const int accepted = hostClock_.accepted;
+        u_ = (accepted % 2 == 0) ? batchU0_ : 1 - batchU0_;
+        a_ = 1 - u_;
+        previous_ = accepted > 0;
+        faulted_ = hostClock_.faulted != 0;
+        inflight_ = false;
+    }
+    int finish() override {
+        if (!inflight_) return hostClock_.accepted;
         DeviceScope scope(device_);
-        if (count <= 0) return 0;
+        check(cudaEventSynchronize(done_), "3D batch completion");
+        finalize();
+        return hostClock_.accepted;
+    }
+    bool query(int &accepted) override {
+        if (inflight_) {
+            DeviceScope scope(device_);
+            const cudaError_t e = cudaEventQuery(done_);
+            if (e == cudaErrorNotReady) return false;
+            check(e, "3D batch query");
+            finalize();
+        }
+        accepted = hostClock_.accepted;
+        return true;
+    }
+    void launch(int first, int count, double dt, double frequency, double growthAfter) override {
+        DeviceScope scope(device_);
+        if (inflight_) throw Error(SWL_ERR_STATE, "a batch is already in flight on this engine");
+        if (count <= 0) {
+            hostClock_.accepted = 0;
+            return;
+        }
         if (dt != dt_) dropGraphs(), dt_ = dt;
         ensureCapacity(count);
         hostClock_.step = hostClock_.first = first;
@@ -383,20 +432,20 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             done += 8;
         }
         for (; done < count; ++done) enqueueStep(first + done, true);
-        pullClock();
-        const int accepted = hostClock_.accepted;
-        u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
-        a_ = 1 - u_;
-        previous_ = accepted > 0;
-        faulted_ = hostClock_.faulted != 0;
-        return accepted;
+        check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
+        check(cudaEventRecord(done_, stream_), "record batch completion");
+        batchU0_ = u0;
+        u_ = u0, a_ = 1 - u0;
+        inflight_ = true;
     }
     void rollback() override {
+        settle();
         DeviceScope scope(device_);
         check(cudaStreamSynchronize(stream_), "3D rollback");
         if (previous_) std::swap(u_, a_), previous_ = false;
     }
     void reset() override {
+        settle();
         DeviceScope scope(device_);
         check(cudaMemsetAsync(sets_.ptr, 0, sets_.bytes, stream_), "3D reset");
         if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "3D trace reset");
@@ -407,6 +456,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
     }
     void diagnostics(swl_diag3d &d) override {
+        settle();
         DeviceScope scope(device_);
         k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, set_[u_], surfRate_.as<double>(), nullptr, partials_.as<k3::Partial>());
         check(cudaGetLastError(), "3D diagnostics");
@@ -431,6 +481,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         d.resident_bytes = residentBytes();
     }
     void sample(double *vx, double *vy, double *vz) override {
+        settle();
         DeviceScope scope(device_);
         if (!nrec_) return;
         std::vector<long long> idx(nrec_);
@@ -445,6 +496,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         for (int r = 0; r < nrec_; ++r) vx[r] = v[3 * r], vy[r] = v[3 * r + 1], vz[r] = v[3 * r + 2];
     }
     void traces(int first, int count, double *vx, double *vy, double *vz) override {
+        settle();
         DeviceScope scope(device_);
         const int row0 = first - hostClock_.first;
         if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
@@ -461,6 +513,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             }
     }
     void snapshot(int field, double *out) override {
+        settle();
         DeviceScope scope(device_);
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "snapshot field out of range");
         check(cudaStreamSynchronize(stream_), "snapshot ordering");
@@ -470,6 +523,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         for (long long i = 0; i < count_; ++i) out[i] = double(tmp[i]);
     }
     void load(int field, const double *in) override {
+        settle();
         DeviceScope scope(device_);
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
         check(cudaStreamSynchronize(stream_), "load ordering");

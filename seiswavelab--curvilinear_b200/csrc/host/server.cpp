@@ -1,0 +1,381 @@
+// Serving request loop (include/swl_server.h): admission by device-memory budget, model builds
+// on a host thread pool, and one scheduler thread that keeps a batch in flight on every running
+// shot.  Each shot owns its engine and CUDA stream, so batches of different shots overlap on
+// the GPU.  Finished shots release their device memory at once, which admits the next request.
+#include "../../../include/swl_server.h"
+#include "sessions.hpp"
+#include <atomic>
+#include <condition_variable>
+#include <cstdio>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+
+namespace swl::host {
+
+struct Shot {
+    int64_t id{};
+    int dim{2};
+    int state{SWL_SHOT_QUEUED};
+    Params2D p2;
+    Params3D p3;
+    std::unique_ptr<Session2D> s2;
+    std::unique_ptr<Session3D> s3;
+    double submit{}, start{}, finish{};
+    std::string error;
+    int64_t bytes{}; // device bytes charged against the budget
+    int steps() const { return dim == 2 ? (s2 ? s2->step : 0) : (s3 ? s3->step : 0); }
+    int total() const { return dim == 2 ? (s2 ? s2->model.total : 0) : (s3 ? s3->model.total : 0); }
+};
+
+// Device bytes of a request before its model exists (src/two_d/MemoryBudget2D.hpp:12-38 style:
+// four state sets, the model arrays, ADE memories, plus a fixed allowance).
+int64_t estimate(const Shot &s) {
+    if (s.dim == 2) {
+        const auto &p = s.p2;
+        const int wx = std::clamp(p.spongeX, 1, std::max(1, p.nx / 3)), wz = std::clamp(p.spongeZ, 1, std::max(1, p.nz / 3));
+        const bool ext = p.absorbing && p.externalAbsorption;
+        const double n = double(p.nx + 6 + (ext ? 2 * wx : 0)) * (p.nz + 6 + (ext ? wz : 0));
+        const int L = p.attenuation.enabled ? p.attenuation.mechanisms : 0, fc = L ? 6 + 4 * L : 5;
+        const double s = p.precision == SWL_FP32 ? 4 : 8;
+        return int64_t(n * s * (4 * fc + 14 + 2 * L)) + (64ll << 20);
+    }
+    const auto &p = s.p3;
+    const double n = double(p.nx + 6) * (p.ny + 6) * (p.nz + 6), bytes = p.precision == SWL_FP32 ? 4 : 8;
+    return int64_t(n * bytes * (36 + 9 + 5 + (p.layered ? 3 : 0) + (p.sourceKind == 1 ? 3 : 0))) + (64ll << 20);
+}
+
+class Server {
+  public:
+    explicit Server(const swl_server_config &c) : cfg_(c), t0_(std::chrono::steady_clock::now()) {
+        device_ = selectDevice(c.device);
+        if (device_ < 0) throw Failure(SWL_ERR_UNAVAILABLE, "no usable sm_100 CUDA device for the server");
+        if (cfg_.batch_steps <= 0) cfg_.batch_steps = 64;
+        if (cfg_.build_threads <= 0) cfg_.build_threads = 4;
+        budget_ = cfg_.memory_budget;
+        if (budget_ <= 0) {
+            DeviceScope scope(device_);
+            std::size_t freeB = 0, totalB = 0;
+            check(cudaMemGetInfo(&freeB, &totalB), "query device memory");
+            budget_ = int64_t(0.85 * double(freeB));
+        }
+        for (int t = 0; t < cfg_.build_threads; ++t) builders_.emplace_back([this] { buildLoop(); });
+        loop_ = std::thread([this] { schedule(); });
+    }
+    ~Server() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cvBuild_.notify_all();
+        cvWork_.notify_all();
+        cvDone_.notify_all();
+        for (auto &t : builders_) t.join();
+        loop_.join();
+    }
+    int64_t submit(std::shared_ptr<Shot> s) {
+        std::lock_guard<std::mutex> g(mu_);
+        s->id = nextId_++;
+        s->submit = now();
+        shots_[s->id] = s;
+        queue_.push_back(s->id);
+        cvWork_.notify_all();
+        return s->id;
+    }
+    swl_shot_status status(int64_t id) {
+        std::lock_guard<std::mutex> g(mu_);
+        const auto s = find(id);
+        swl_shot_status o{};
+        o.id = id, o.dim = s->dim, o.state = s->state, o.submit_s = s->submit, o.start_s = s->start, o.finish_s = s->finish;
+        o.resident_bytes = s->bytes;
+        if (s->state >= SWL_SHOT_RUNNING || s->state == SWL_SHOT_FAILED) {
+            o.steps_done = s->steps(), o.total_steps = s->total();
+            if (s->dim == 2 && s->s2) o.receivers = int32_t(s->s2->vx.size()), o.samples = s->s2->vx.empty() ? 0 : int64_t(s->s2->vx.front().size());
+            if (s->dim == 3 && s->s3) o.receivers = int32_t(s->s3->rec[0].size()), o.samples = int64_t(s->s3->step) + 1;
+        }
+        std::snprintf(o.error, sizeof(o.error), "%s", s->error.c_str());
+        return o;
+    }
+    int64_t nextFinished(int timeoutMs) {
+        std::unique_lock<std::mutex> g(mu_);
+        cvDone_.wait_for(g, std::chrono::milliseconds(std::max(0, timeoutMs)), [&] { return !unreported_.empty() || stop_; });
+        if (unreported_.empty()) return -1;
+        const int64_t id = unreported_.front();
+        unreported_.pop_front();
+        return id;
+    }
+    void records(int64_t id, double *vx, double *vy, double *vz) {
+        std::lock_guard<std::mutex> g(mu_);
+        const auto s = find(id);
+        if (s->state != SWL_SHOT_DONE && s->state != SWL_SHOT_FAILED) throw Failure(SWL_ERR_STATE, "shot has not finished");
+        const auto copy = [](const std::vector<std::vector<double>> &src, double *dst) {
+            if (!dst) return;
+            std::size_t at = 0;
+            for (const auto &v : src) std::copy(v.begin(), v.end(), dst + at), at += v.size();
+        };
+        if (s->dim == 2 && s->s2) copy(s->s2->vx, vx), copy(s->s2->vz, vz);
+        if (s->dim == 3 && s->s3) copy(s->s3->rec[0], vx), copy(s->s3->rec[1], vy), copy(s->s3->rec[2], vz);
+    }
+    void release(int64_t id) {
+        std::lock_guard<std::mutex> g(mu_);
+        const auto s = find(id);
+        if (s->state != SWL_SHOT_DONE && s->state != SWL_SHOT_FAILED) throw Failure(SWL_ERR_STATE, "shot has not finished");
+        shots_.erase(id);
+    }
+    void drain() {
+        std::unique_lock<std::mutex> g(mu_);
+        cvDone_.wait(g, [&] { return stop_ || finished_ == submittedCount(); });
+    }
+    swl_server_stats stats() {
+        std::lock_guard<std::mutex> g(mu_);
+        swl_server_stats o{};
+        for (const auto &kv : shots_) {
+            const int st = kv.second->state;
+            o.queued += st == SWL_SHOT_QUEUED, o.building += st == SWL_SHOT_BUILDING, o.running += st == SWL_SHOT_RUNNING;
+            o.done += st == SWL_SHOT_DONE, o.failed += st == SWL_SHOT_FAILED;
+        }
+        o.peak_running = peakRunning_, o.resident_bytes = used_, o.peak_resident_bytes = peakUsed_, o.memory_budget = budget_;
+        return o;
+    }
+
+  private:
+    swl_server_config cfg_;
+    int device_{};
+    int64_t budget_{}, used_{}, peakUsed_{};
+    std::chrono::steady_clock::time_point t0_;
+    std::mutex mu_;
+    std::condition_variable cvWork_, cvDone_, cvBuild_;
+    std::deque<int64_t> queue_, unreported_;
+    std::deque<std::shared_ptr<Shot>> toBuild_, built_;
+    std::map<int64_t, std::shared_ptr<Shot>> shots_;
+    int64_t nextId_{}, finished_{}, building_{};
+    int peakRunning_{};
+    bool stop_{false};
+    std::vector<std::thread> builders_;
+    std::thread loop_;
+
+    double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
+    int64_t submittedCount() const { return nextId_; }
+    std::shared_ptr<Shot> find(int64_t id) {
+        const auto it = shots_.find(id);
+        if (it == shots_.end()) throw Failure(SWL_ERR_INVALID, "unknown shot id");
+        return it->second;
+    }
+    // caller holds mu_
+    void finishShot(const std::shared_ptr<Shot> &s, int state, const std::string &error) {
+        s->state = state;
+        s->error = error;
+        s->finish = now();
+        used_ -= s->bytes;
+        ++finished_;
+        unreported_.push_back(s->id);
+        cvDone_.notify_all();
+        cvWork_.notify_all();
+    }
+    void buildLoop() {
+        for (;;) {
+            std::shared_ptr<Shot> s;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cvBuild_.wait(g, [&] { return stop_ || !toBuild_.empty(); });
+                if (stop_) return;
+                s = toBuild_.front();
+                toBuild_.pop_front();
+            }
+            std::string error;
+            try { // host FP64 model build, then the engine on its own stream
+                if (s->dim == 2) {
+                    auto x = std::make_unique<Session2D>();
+                    x->params = s->p2;
+                    x->create(device_);
+                    s->s2 = std::move(x);
+                } else {
+                    auto x = std::make_unique<Session3D>();
+                    x->params = s->p3;
+                    x->create(device_);
+                    s->s3 = std::move(x);
+                }
+            } catch (const std::exception &e) {
+                error = e.what();
+            }
+            std::lock_guard<std::mutex> g(mu_);
+            --building_;
+            if (!error.empty()) finishShot(s, SWL_SHOT_FAILED, error);
+            else {
+                const int64_t actual = (s->dim == 2 ? swl2d_resident_bytes(s->s2->engine) : swl3d_resident_bytes(s->s3->engine)) + (16ll << 20);
+                used_ += actual - s->bytes;
+                s->bytes = actual;
+                peakUsed_ = std::max(peakUsed_, used_);
+                built_.push_back(s);
+                cvWork_.notify_all();
+            }
+        }
+    }
+    // Admission in arrival order; caller holds mu_.
+    void admit(int running) {
+        while (!queue_.empty()) {
+            const auto s = shots_[queue_.front()];
+            const int64_t need = estimate(*s);
+            const int active = running + int(building_);
+            if (cfg_.max_active > 0 && active >= cfg_.max_active) break;
+            if (used_ + need > budget_) {
+                if (active > 0) break; // wait for memory to free up
+                if (need > budget_) {   // can never fit
+                    queue_.pop_front();
+                    finishShot(s, SWL_SHOT_FAILED, "request exceeds the server's device-memory budget");
+                    continue;
+                }
+            }
+            queue_.pop_front();
+            s->state = SWL_SHOT_BUILDING;
+            s->start = now();
+            s->bytes = need;
+            used_ += need;
+            peakUsed_ = std::max(peakUsed_, used_);
+            ++building_;
+            toBuild_.push_back(s);
+            cvBuild_.notify_one();
+        }
+    }
+    void schedule() {
+        std::vector<std::shared_ptr<Shot>> running;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                if (stop_) break;
+                while (!built_.empty()) {
+                    built_.front()->state = SWL_SHOT_RUNNING;
+                    running.push_back(built_.front());
+                    built_.pop_front();
+                }
+                peakRunning_ = std::max(peakRunning_, int(running.size()));
+                admit(int(running.size()));
+            }
+            bool progressed = false;
+            for (std::size_t i = 0; i < running.size();) {
+                auto &s = running[i];
+                bool finished = false;
+                std::string error;
+                try {
+                    if (s->dim == 2) {
+                        auto &x = *s->s2;
+                        if (x.inflight) {
+                            if (x.pollBatch(false)) progressed = true;
+                        }
+                        if (!x.inflight) {
+                            if (x.completed()) finished = true;
+                            else if (x.launchBatch(cfg_.batch_steps)) progressed = true;
+                        }
+                    } else {
+                        auto &x = *s->s3;
+                        if (x.inflight) {
+                            if (x.pollBatch(false)) progressed = true;
+                        }
+                        if (!x.inflight) {
+                            if (x.completed()) finished = true;
+                            else if (x.launchBatch(cfg_.batch_steps)) progressed = true;
+                        }
+                    }
+                } catch (const std::exception &e) {
+                    error = e.what();
+                    finished = true;
+                }
+                if (finished) {
+                    // free the device memory now; the records stay with the shot
+                    if (s->s2 && s->s2->engine) swl2d_destroy(s->s2->engine), s->s2->engine = nullptr;
+                    if (s->s3 && s->s3->engine) swl3d_destroy(s->s3->engine), s->s3->engine = nullptr;
+                    std::lock_guard<std::mutex> g(mu_);
+                    finishShot(s, error.empty() ? SWL_SHOT_DONE : SWL_SHOT_FAILED, error);
+                    running.erase(running.begin() + i);
+                    progressed = true;
+                    continue;
+                }
+                ++i;
+            }
+            if (!progressed) {
+                std::unique_lock<std::mutex> g(mu_);
+                cvWork_.wait_for(g, std::chrono::microseconds(running.empty() ? 2000 : 100));
+            }
+        }
+        for (auto &s : running) { // abandoned on destruction
+            if (s->s2 && s->s2->engine) swl2d_destroy(s->s2->engine), s->s2->engine = nullptr;
+            if (s->s3 && s->s3->engine) swl3d_destroy(s->s3->engine), s->s3->engine = nullptr;
+        }
+    }
+};
+
+} // namespace swl::host
+
+struct swl_server : swl::host::Server {
+    using Server::Server;
+};
+
+extern "C" {
+void swl_server_config_default(swl_server_config *c) {
+    if (!c) return;
+    *c = swl_server_config{};
+    c->device = -1, c->memory_budget = 0, c->max_active = 0, c->batch_steps = 64, c->build_threads = 4;
+}
+swl_status swl_server_create(const swl_server_config *c, swl_server **out) {
+    return swl::host::guard([&] {
+        if (!c || !out) throw swl::host::Failure(SWL_ERR_INVALID, "config and out are required");
+        *out = new swl_server(*c);
+    });
+}
+void swl_server_destroy(swl_server *s) { delete s; }
+swl_status swl_server_submit2d(swl_server *s, const swl_params2d *p, int64_t *id) {
+    return swl::host::guard([&] {
+        if (!s || !p || !id) throw swl::host::Failure(SWL_ERR_INVALID, "server, params and id are required");
+        auto shot = std::make_shared<swl::host::Shot>();
+        shot->dim = 2;
+        shot->p2 = swl::host::toParams(*p);
+        *id = s->submit(shot);
+    });
+}
+swl_status swl_server_submit3d(swl_server *s, const swl_params3d *p, int64_t *id) {
+    return swl::host::guard([&] {
+        if (!s || !p || !id) throw swl::host::Failure(SWL_ERR_INVALID, "server, params and id are required");
+        auto shot = std::make_shared<swl::host::Shot>();
+        shot->dim = 3;
+        shot->p3 = swl::host::toParams(*p);
+        *id = s->submit(shot);
+    });
+}
+swl_status swl_server_status(swl_server *s, int64_t id, swl_shot_status *out) {
+    return swl::host::guard([&] {
+        if (!s || !out) throw swl::host::Failure(SWL_ERR_INVALID, "server and out are required");
+        *out = s->status(id);
+    });
+}
+swl_status swl_server_next_finished(swl_server *s, int32_t timeoutMs, int64_t *id) {
+    return swl::host::guard([&] {
+        if (!s || !id) throw swl::host::Failure(SWL_ERR_INVALID, "server and id are required");
+        *id = s->nextFinished(timeoutMs);
+    });
+}
+swl_status swl_server_records(swl_server *s, int64_t id, double *vx, double *vy, double *vz) {
+    return swl::host::guard([&] {
+        if (!s) throw swl::host::Failure(SWL_ERR_INVALID, "server is null");
+        s->records(id, vx, vy, vz);
+    });
+}
+swl_status swl_server_release(swl_server *s, int64_t id) {
+    return swl::host::guard([&] {
+        if (!s) throw swl::host::Failure(SWL_ERR_INVALID, "server is null");
+        s->release(id);
+    });
+}
+swl_status swl_server_drain(swl_server *s) {
+    return swl::host::guard([&] {
+        if (!s) throw swl::host::Failure(SWL_ERR_INVALID, "server is null");
+        s->drain();
+    });
+}
+swl_status swl_server_stats_get(swl_server *s, swl_server_stats *out) {
+    return swl::host::guard([&] {
+        if (!s || !out) throw swl::host::Failure(SWL_ERR_INVALID, "server and out are required");
+        *out = s->stats();
+    });
+}
+} // extern "C"

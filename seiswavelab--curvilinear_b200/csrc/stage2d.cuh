@@ -1,15 +1,19 @@
 // 2D P-SV / GSLS device code: one fused kernel per classic-RK4 stage.
 //
-// Each thread owns one physical node.  It evaluates the MacCormack-DRP derivatives of the
-// stage input, the metric-transformed right-hand side (src/two_d/PointKernels2D.hpp:121-172)
-// with the traction-image surface rows, CFS-PML ADE memories and GSLS relaxation, and then
-// immediately performs its part of the RK combine and the free-surface projection -- the
-// rates never touch HBM.  Three state sets stay resident beside the stage outputs:
+// A CTA owns a 32x32 tile of physical nodes.  It first stages the five stencil fields (Vx, Vz,
+// Sxx, Szz, Sxz) of the stage input over the tile plus a 3-node halo into shared memory with
+// asynchronous copies (cp.async; no registers held while the copies are in flight), then each
+// thread evaluates four nodes: the MacCormack-DRP derivatives from shared memory, the
+// metric-transformed right-hand side (src/two_d/PointKernels2D.hpp:121-172) with the
+// traction-image surface rows, CFS-PML ADE memories and GSLS relaxation, and immediately its
+// part of the RK combine and the free-surface projection -- the rates never touch HBM.
+// Three state sets stay resident beside the stage outputs:
 //   U (state at the start of the step), A (running RK accumulator), S (stage state).
 // Stage 0 writes A = k1 and S = U + dt/2 k1; stages 1-2 add 2k to A and write
-// S = U + w k; stage 3 writes U + dt (A + k4) / 6 over A.  The sums are formed in the
-// reference's order (src/two_d/CurvilinearSolver2D.cpp:80-97), so with FMA contraction off
-// the FP64 results equal the reference CPU build's.
+// S = U + w k; stage 3 writes U + dt (A + k4) / 6 over A and (optionally) reduces the
+// diagnostics of the new state per CTA.  Sums are formed in the reference's order
+// (src/two_d/CurvilinearSolver2D.cpp:80-97), so with FMA contraction off the FP64 results equal
+// the reference CPU build's.
 #pragma once
 #include "runtime.cuh"
 #include <cstdint>
@@ -21,7 +25,8 @@ namespace swl::k2 {
 template <class Real> struct Mesh {
     int nx, nz; // padded
     long long count;
-    Real h;
+    Real h, hinv;   // hinv = 1/h, used only when it is exact (h a power of two) or in FP32
+    int hinvExact;
     const Real *a, *b, *jac, *normals, *lambda, *mu, *rho, *damping, *source, *sgx, *sgz;
     Real sdx, sdz;             // unit force direction (x, z)
     int src_i0, src_i1, src_k0, src_k1; // source support box [i0,i1) x [k0,k1), padded indices
@@ -50,6 +55,12 @@ struct Clock {
     double dt, growth_after; // energy-growth rule applies when (step+1)*dt > growth_after
 };
 
+// Per-CTA diagnostics of a state (src/two_d/CudaEngine2D.cu:43-78 semantics).
+struct Partial {
+    double energy, velocity, traction;
+    int bad, pad;
+};
+
 template <class Real> struct StageArgs {
     Mesh<Real> m;
     const Real *in;   // stage input state (stencil reads)
@@ -64,10 +75,12 @@ template <class Real> struct StageArgs {
     const Clock *clock;
     Real weight;         // dt/2, dt/2, dt for stages 0..2
     Real delta;          // dt
+    Partial *partials;   // stage 3: per-CTA diagnostics of the new state (null: none)
 };
 
 template <class Real> __device__ __forceinline__ Real ld(const Real *p) { return __ldg(p); }
 
+// ------------------------------------------------------------- pointer stencils (3D engine)
 // 5-point DRP derivative (include/SeisCommon/FiniteDifference.hpp:14-26, PointKernels2D.hpp:38-47):
 // forward taps at offsets -1..3, backward at +1..-3 with negated coefficients.
 template <class Real, int DIR>
@@ -117,18 +130,77 @@ __device__ __forceinline__ Real near3(const Real *__restrict__ v, long long q, l
     return r / h;
 }
 
-// Traction flux J (x sigma_a + z sigma_b) at node qq (PointKernels2D.hpp:90-93).
+// ------------------------------------------------------------- tiled 2D stage
+constexpr int TX = 32, TZ = 32, HX = TX + 6, HZ = TZ + 6; // tile and halo'd tile
+constexpr int TILE_THREADS = 256, ROWS_PER_THREAD = TZ / (TILE_THREADS / TX);
+template <class Real> constexpr std::size_t tileBytes() { return sizeof(Real) * 5 * HZ * HX; }
+
+// Taps of the five stencil fields around one node in the shared tile.
+template <class Real> struct Tile {
+    const Real *c; // centre element of field 0
+    __device__ __forceinline__ Real at(int f, int dx, int dz) const { return c[f * (HZ * HX) + dz * HX + dx]; }
+};
+
+template <class Real> __device__ __forceinline__ Real scaled(const Mesh<Real> &m, Real r) {
+    // r/h; for h = 2^k the exact reciprocal gives the identical result with a multiply
+    return m.hinvExact ? r * m.hinv : r / m.h;
+}
+template <class Real, int DIR> __device__ __forceinline__ Real tdrp(const Tile<Real> &t, const Mesh<Real> &m, int f, int axis) {
+    const int sx = axis ? 0 : 1, sz = axis ? 1 : 0;
+    Real r = Real(0);
+    if (DIR == 0) {
+        r += Real(-.30874) * t.at(f, -sx, -sz);
+        r += Real(-.6326) * t.at(f, 0, 0);
+        r += Real(1.233) * t.at(f, sx, sz);
+        r += Real(-.3334) * t.at(f, 2 * sx, 2 * sz);
+        r += Real(.04168) * t.at(f, 3 * sx, 3 * sz);
+    } else {
+        r += -Real(-.30874) * t.at(f, sx, sz);
+        r += -Real(-.6326) * t.at(f, 0, 0);
+        r += -Real(1.233) * t.at(f, -sx, -sz);
+        r += -Real(-.3334) * t.at(f, -2 * sx, -2 * sz);
+        r += -Real(.04168) * t.at(f, -3 * sx, -3 * sz);
+    }
+    return scaled(m, r);
+}
+template <class Real, int DIR> __device__ __forceinline__ Real tnear2(const Tile<Real> &t, const Mesh<Real> &m, int f) {
+    Real r = Real(0);
+    if (DIR == 0) {
+        r += Real(-1) * t.at(f, 0, 0);
+        r += Real(1) * t.at(f, 0, 1);
+    } else {
+        r += -Real(-1) * t.at(f, 0, 0);
+        r += -Real(1) * t.at(f, 0, -1);
+    }
+    return scaled(m, r);
+}
+template <class Real, int DIR> __device__ __forceinline__ Real tnear3(const Tile<Real> &t, const Mesh<Real> &m, int f) {
+    const Real c0 = Real(-7) / Real(6), c1 = Real(8) / Real(6), c2 = Real(-1) / Real(6);
+    Real r = Real(0);
+    if (DIR == 0) {
+        r += c0 * t.at(f, 0, 0);
+        r += c1 * t.at(f, 0, 1);
+        r += c2 * t.at(f, 0, 2);
+    } else {
+        r += -c0 * t.at(f, 0, 0);
+        r += -c1 * t.at(f, 0, -1);
+        r += -c2 * t.at(f, 0, -2);
+    }
+    return scaled(m, r);
+}
+
+// Traction flux J (x sigma_a + z sigma_b) at the tap (dx, dz) (PointKernels2D.hpp:90-93).
 template <class Real>
-__device__ __forceinline__ Real flux(const Mesh<Real> &m, const Real *__restrict__ w, long long qq, int axis, int comp) {
-    const long long n = m.count;
+__device__ __forceinline__ Real flux(const Mesh<Real> &m, const Tile<Real> &t, long long q, int dx, int dz, int axis, int comp) {
+    const long long qq = q + dx + (long long)dz * m.nx;
     const Real x = axis ? ld(m.a + qq) : Real(1), z = axis ? ld(m.b + qq) : Real(0);
-    return ld(m.jac + qq) * (x * ld(w + (comp ? 4 : 2) * n + qq) + z * ld(w + (comp ? 3 : 4) * n + qq));
+    return ld(m.jac + qq) * (x * t.at(comp ? 4 : 2, dx, dz) + z * t.at(comp ? 3 : 4, dx, dz));
 }
 
 // Conservative traction-image momentum near the surface (PointKernels2D.hpp:94-120):
 // the surface tap is dropped and taps above it mirror with a sign flip.  only = -1: both axes.
 template <class Real, int DX, int DZ>
-__device__ Real momentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, int only) {
+__device__ Real momentum(const Mesh<Real> &m, const Tile<Real> &t, long long q, int comp, int depth, int only) {
     const Real C[5] = {Real(-.30874), Real(-.6326), Real(1.233), Real(-.3334), Real(.04168)};
     Real r = Real(0);
     for (int axis = 0; axis < 2; ++axis) {
@@ -147,7 +219,7 @@ __device__ Real momentum(const Mesh<Real> &m, const Real *__restrict__ w, long l
                     sign = Real(-1);
                 }
             }
-            r += sign * c * flux(m, w, q + (long long)off * (axis ? m.nx : 1), axis, comp);
+            r += sign * c * flux(m, t, q, axis ? 0 : off, axis ? off : 0, axis, comp);
         }
     }
     return r / (m.h * ld(m.jac + q) * ld(m.rho + q));
@@ -161,28 +233,62 @@ __device__ __forceinline__ Real stretch(const Real *prof, Real psi, Real d, Real
     return d / kappa + psi;
 }
 
-// The fused stage.  DX/DZ: MacCormack directions of this (step, stage); MECH: GSLS
-// mechanisms; STAGE: 0..3.  The CFS-PML branch is uniform across the launch.
+__device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
+// stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
+template <class Real, int STAGE>
+__device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real *acc, Real u, Real r) {
+    if (STAGE == 0) {
+        *acc = r;
+        return u + p.weight * r;
+    } else if (STAGE < 3) {
+        *acc = *acc + 2 * r;
+        return u + p.weight * r;
+    }
+    return u + p.delta * (*acc + r) / Real(6);
+}
+template <class Real, int STAGE> __device__ __forceinline__ void storeField(const StageArgs<Real> &p, long long at, Real v) {
+    (STAGE == 3 ? p.acc : p.out)[at] = v;
+}
+// ADE memory update of one slot value (same scheme as the fields).
+template <class Real, int STAGE>
+__device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long long at, Real rate, Partial &diag, bool withDiag) {
+    const Real u = ld(p.pbase + at);
+    if (STAGE == 0) {
+        p.pacc[at] = rate;
+        p.pout[at] = u + p.weight * rate;
+    } else if (STAGE < 3) {
+        p.pacc[at] = p.pacc[at] + 2 * rate;
+        p.pout[at] = u + p.weight * rate;
+    } else {
+        const Real v = u + p.delta * (p.pacc[at] + rate) / Real(6);
+        p.pacc[at] = v;
+        if (withDiag && !isfinite(v)) diag.bad = 1;
+    }
+}
+
+// One node of one stage, in two phases that keep few values live: (1) velocity derivatives ->
+// stress (and GSLS) rates -> combine/store of the stresses; (2) stress derivatives -> velocity
+// rates -> combine/store of the velocities.  Every expression keeps the reference's operation
+// order (src/two_d/PointKernels2D.hpp:121-172); only independent computations are reordered.
 template <class Real, int DX, int DZ, int MECH, int STAGE>
-__global__ void __launch_bounds__(256) stage2d(const StageArgs<Real> p) {
+__device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<Real> &t, int i, int k, Partial &diag,
+                                          bool withDiag) {
     const Mesh<Real> &m = p.m;
-    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = 3 + blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= m.nx - 3 || k >= m.nz - 3) return;
-    const Clock *clk = p.clock;
-    if (clk->faulted) return;
     const bool CPML = m.wz > 0;
-    constexpr int FC = MECH ? 6 + 4 * MECH : 5;
-    const long long n = m.count, nx = m.nx, q = i + nx * k;
+    const long long n = m.count, q = i + (long long)m.nx * k;
     const int depth = k - 3;
     const Real *__restrict__ w = p.in;
-    const Real h = m.h;
+    const bool damped = !(i >= m.dmp_i0 && i < m.dmp_i1 && k < m.dmp_k1);
+    const Real damp = damped ? ld(m.damping + q) : Real(0);
 
-    // --- derivatives along xi (x) of the five stencil fields
-    Real xi[5], eta[5];
-#pragma unroll
-    for (int f = 0; f < 5; ++f) xi[f] = drp5<Real, DX>(w + f * n, q, 1, h);
-    // --- CFS-PML slots of this node (src/two_d/PointKernels2D.hpp:50-56)
+    // CFS-PML slots of this node (src/two_d/PointKernels2D.hpp:50-56)
     long long slot0 = -1, slot1 = -1;
     const Real *prof0 = nullptr, *prof1 = nullptr;
     if (CPML) {
@@ -192,177 +298,254 @@ __global__ void __launch_bounds__(256) stage2d(const StageArgs<Real> p) {
         if (kc >= nzc - m.wz)
             slot1 = 4 * ((long long)(2 * m.wx) * nzc + (long long)(kc - (nzc - m.wz)) * nxc + ic), prof1 = m.cpz + 3 * kc;
     }
-    Real prate0[4] = {0, 0, 0, 0}, prate1[4] = {0, 0, 0, 0};
-    Real vxs[2] = {xi[0], xi[1]}; // stretched xi of Vx, Vz
-    if (CPML && slot0 >= 0)
-        for (int v = 0; v < 2; ++v) vxs[v] = stretch(prof0, ld(p.pin + slot0 + v), xi[v], prate0[v]);
+    const Real a = ld(m.a + q), b = ld(m.b + q);
 
-    // --- derivatives along eta (z); velocities use the one-sided / traction stencils near the surface
-#pragma unroll
-    for (int f = 2; f < 5; ++f) eta[f] = drp5<Real, DZ>(w + f * n, q, nx, h);
-    if (depth == 0) {
-        // surface eta-derivative from the traction-free condition (PointKernels2D.hpp:79-89)
-        const Real c0 = ld(m.a + q), c1 = ld(m.b + q), c2 = c0 * c0 + c1 * c1, len = sqrt(c2);
+    // ---- phase 1: velocity derivatives -> stress and GSLS rates
+    Real xv[2], vxs[2], ev[2];
+    xv[0] = tdrp<Real, DX>(t, m, 0, 0);
+    xv[1] = tdrp<Real, DX>(t, m, 1, 0);
+    vxs[0] = xv[0], vxs[1] = xv[1];
+    Real prate[4] = {0, 0, 0, 0}; // ADE rates of the velocity-derivative memories: slot0 f0,f1, slot1 f0,f1
+    if (CPML && slot0 >= 0)
+        for (int v = 0; v < 2; ++v) vxs[v] = stretch(prof0, ld(p.pin + slot0 + v), xv[v], prate[v]);
+    const Real lam = ld(m.lambda + q), mu = ld(m.mu + q);
+    if (depth == 0) { // surface eta-derivative from the traction-free condition (PointKernels2D.hpp:79-89)
+        const Real c0 = a, c1 = b, c2 = c0 * c0 + c1 * c1, len = sqrt(c2);
         const Real nn[2] = {c0 / len, c1 / len};
-        const Real dx = vxs[0], dz = vxs[1], lam = ld(m.lambda + q), mu = ld(m.mu + q);
-        Real t[2] = {(lam + 2 * mu) * dx * c0 + mu * dz * c1, mu * dz * c0 + lam * dx * c1};
+        const Real dx = vxs[0], dz = vxs[1];
+        Real tt[2] = {(lam + 2 * mu) * dx * c0 + mu * dz * c1, mu * dz * c0 + lam * dx * c1};
 #pragma unroll
         for (int l = 0; l < MECH; ++l) {
             const int mm = 6 + 4 * l;
-            t[0] -= ld(w + mm * n + q) * c0 + ld(w + (mm + 2) * n + q) * c1;
-            t[1] -= ld(w + (mm + 2) * n + q) * c0 + ld(w + (mm + 1) * n + q) * c1;
+            tt[0] -= ld(w + mm * n + q) * c0 + ld(w + (mm + 2) * n + q) * c1;
+            tt[1] -= ld(w + (mm + 2) * n + q) * c0 + ld(w + (mm + 1) * n + q) * c1;
         }
-        const Real normal = t[0] * nn[0] + t[1] * nn[1];
+        const Real normal = tt[0] * nn[0] + tt[1] * nn[1];
         for (int v = 0; v < 2; ++v)
-            eta[v] = -(t[v] - nn[v] * normal) / (mu * c2) - nn[v] * normal / ((lam + 2 * mu) * c2);
+            ev[v] = -(tt[v] - nn[v] * normal) / (mu * c2) - nn[v] * normal / ((lam + 2 * mu) * c2);
     } else if (depth == 1) {
-        eta[0] = near2<Real, DZ>(w, q, nx, h);
-        eta[1] = near2<Real, DZ>(w + n, q, nx, h);
+        ev[0] = tnear2<Real, DZ>(t, m, 0);
+        ev[1] = tnear2<Real, DZ>(t, m, 1);
     } else if (depth == 2) {
-        eta[0] = near3<Real, DZ>(w, q, nx, h);
-        eta[1] = near3<Real, DZ>(w + n, q, nx, h);
+        ev[0] = tnear3<Real, DZ>(t, m, 0);
+        ev[1] = tnear3<Real, DZ>(t, m, 1);
     } else {
-        eta[0] = drp5<Real, DZ>(w, q, nx, h);
-        eta[1] = drp5<Real, DZ>(w + n, q, nx, h);
+        ev[0] = tdrp<Real, DZ>(t, m, 0, 1);
+        ev[1] = tdrp<Real, DZ>(t, m, 1, 1);
     }
-    const Real a = ld(m.a + q), b = ld(m.b + q), rho = ld(m.rho + q);
-    Real dxv[5], dzv[5];
+    Real dxv[2], dzv[2];
 #pragma unroll
-    for (int f = 0; f < 5; ++f) {
-        Real vx = xi[f], vz = eta[f];
-        if (CPML && f < 2) {
-            vx = vxs[f];
-            if (slot1 >= 0) vz = stretch(prof1, ld(p.pin + slot1 + f), eta[f], prate1[f]);
-        }
-        dxv[f] = vx + a * vz;
+    for (int f = 0; f < 2; ++f) {
+        Real vz = ev[f];
+        if (CPML && slot1 >= 0) vz = stretch(prof1, ld(p.pin + slot1 + f), ev[f], prate[2 + f]);
+        dxv[f] = vxs[f] + a * vz;
         dzv[f] = b * vz;
     }
-
-    // --- velocity rates
-    Real r[FC];
-    const bool near = depth <= (DZ ? 3 : 1);
-    if (!CPML) {
-        if (near) {
-            r[0] = momentum<Real, DX, DZ>(m, w, q, 0, depth, -1);
-            r[1] = momentum<Real, DX, DZ>(m, w, q, 1, depth, -1);
-        } else {
-            r[0] = (dxv[2] + dzv[4]) / rho;
-            r[1] = (dxv[4] + dzv[3]) / rho;
-        }
-    } else {
-#pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            const int f = v ? 4 : 2, o = v ? 3 : 4;
-            Real X, Z;
-            if (near) {
-                X = momentum<Real, DX, DZ>(m, w, q, v, depth, 0);
-                Z = momentum<Real, DX, DZ>(m, w, q, v, depth, 1);
-            } else {
-                X = xi[f] / rho;
-                Z = (a * eta[f] + b * eta[o]) / rho;
-            }
-            if (slot0 >= 0) X = stretch(prof0, ld(p.pin + slot0 + 2 + v), X, prate0[2 + v]);
-            if (slot1 >= 0) Z = stretch(prof1, ld(p.pin + slot1 + 2 + v), Z, prate1[2 + v]);
-            r[v] = X + Z;
-        }
-    }
-    if (i >= m.src_i0 && i < m.src_i1 && k >= m.src_k0 && k < m.src_k1) {
-        const Real forcing = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
-        if (m.sgx) {
-            r[0] += forcing * ld(m.sgx + q) / rho;
-            r[1] += forcing * ld(m.sgz + q) / rho;
-        } else {
-            const Real s = ld(m.source + q);
-            r[0] += forcing * (s * m.sdx) / rho;
-            r[1] += forcing * (s * m.sdz) / rho;
-        }
-    }
-    // --- stress rates (and GSLS memories)
-    const Real lam = ld(m.lambda + q), mu = ld(m.mu + q), div = dxv[0] + dzv[1];
-    r[2] = lam * div + 2 * mu * dxv[0];
-    r[3] = lam * div + 2 * mu * dzv[1];
-    r[4] = mu * (dzv[0] + dxv[1]);
-    Real wc[FC]; // stage input at the node (pointwise fields and damping)
-#pragma unroll
-    for (int f = 0; f < FC; ++f) wc[f] = ld(w + f * n + q);
+    const Real div = dxv[0] + dzv[1];
+    Real r2 = lam * div + 2 * mu * dxv[0];
+    Real r3 = lam * div + 2 * mu * dzv[1];
+    Real r4 = mu * (dzv[0] + dxv[1]);
     if (MECH) {
-        r[5] = lam * div;
+        Real r5 = lam * div;
 #pragma unroll
         for (int l = 0; l < MECH; ++l) {
             const int mm = 6 + 4 * l;
             const Real dp = ld(m.dP[l] + q), ds = ld(m.dS[l] + q), dl = dp - 2 * ds;
             const Real drive[4] = {dl * div + 2 * ds * dxv[0], dl * div + 2 * ds * dzv[1], ds * (dzv[0] + dxv[1]), dl * div};
-            r[2] -= wc[mm];
-            r[3] -= wc[mm + 1];
-            r[4] -= wc[mm + 2];
-            r[5] -= wc[mm + 3];
+            Real wm[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) r[mm + f] = m.rates[l] * (drive[f] - wc[mm + f]);
-        }
-    }
-    if (!(i >= m.dmp_i0 && i < m.dmp_i1 && k < m.dmp_k1)) {
-        const Real d = ld(m.damping + q);
-#pragma unroll
-        for (int f = 0; f < FC; ++f) r[f] -= d * wc[f];
-    }
-
-    // --- RK combine (+ projection of the surface row), fields then ADE memories
-    Real o[FC];
-#pragma unroll
-    for (int f = 0; f < FC; ++f) {
-        const Real u = ld(p.base + f * n + q);
-        if (STAGE == 0) {
-            p.acc[f * n + q] = r[f];
-            o[f] = u + p.weight * r[f];
-        } else if (STAGE < 3) {
-            p.acc[f * n + q] = p.acc[f * n + q] + 2 * r[f];
-            o[f] = u + p.weight * r[f];
-        } else {
-            o[f] = u + p.delta * (p.acc[f * n + q] + r[f]) / Real(6);
-        }
-    }
-    if (depth == 0) { // PointKernels2D.hpp:70-78
-        const Real nx_ = ld(m.normals + 2 * q), nz_ = ld(m.normals + 2 * q + 1);
-        const Real tx = o[2] * nx_ + o[4] * nz_, tz = o[4] * nx_ + o[3] * nz_, nn = nx_ * tx + nz_ * tz;
-        o[2] += -2 * nx_ * tx + nn * nx_ * nx_;
-        o[3] += -2 * nz_ * tz + nn * nz_ * nz_;
-        o[4] += -nx_ * tz - tx * nz_ + nn * nx_ * nz_;
-    }
-    Real *dst = STAGE == 3 ? p.acc : p.out;
-#pragma unroll
-    for (int f = 0; f < FC; ++f) dst[f * n + q] = o[f];
-    if (CPML) {
-#pragma unroll
-        for (int ax = 0; ax < 2; ++ax) {
-            const long long s = ax ? slot1 : slot0;
-            if (s < 0) continue;
-            const Real *pr = ax ? prate1 : prate0;
+            for (int f = 0; f < 4; ++f) wm[f] = ld(w + (mm + f) * n + q);
+            r2 -= wm[0];
+            r3 -= wm[1];
+            r4 -= wm[2];
+            r5 -= wm[3];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const long long at = s + f;
-                const Real u = ld(p.pbase + at);
-                if (STAGE == 0) {
-                    p.pacc[at] = pr[f];
-                    p.pout[at] = u + p.weight * pr[f];
-                } else if (STAGE < 3) {
-                    p.pacc[at] = p.pacc[at] + 2 * pr[f];
-                    p.pout[at] = u + p.weight * pr[f];
-                } else {
-                    p.pacc[at] = u + p.delta * (p.pacc[at] + pr[f]) / Real(6);
-                }
+                Real rm = m.rates[l] * (drive[f] - wm[f]);
+                if (damped) rm -= damp * wm[f];
+                const long long at = (mm + f) * n + q;
+                const Real o = combine<Real, STAGE>(p, p.acc + at, ld(p.base + at), rm);
+                storeField<Real, STAGE>(p, at, o);
+                if (withDiag && !isfinite(o)) diag.bad = 1;
             }
+        }
+        if (damped) r5 -= damp * ld(w + 5 * n + q);
+        const long long at = 5 * n + q;
+        const Real o = combine<Real, STAGE>(p, p.acc + at, ld(p.base + at), r5);
+        storeField<Real, STAGE>(p, at, o);
+        if (withDiag && !isfinite(o)) diag.bad = 1;
+    }
+    if (damped) {
+        r2 -= damp * t.at(2, 0, 0);
+        r3 -= damp * t.at(3, 0, 0);
+        r4 -= damp * t.at(4, 0, 0);
+    }
+    Real o2 = combine<Real, STAGE>(p, p.acc + 2 * n + q, ld(p.base + 2 * n + q), r2);
+    Real o3 = combine<Real, STAGE>(p, p.acc + 3 * n + q, ld(p.base + 3 * n + q), r3);
+    Real o4 = combine<Real, STAGE>(p, p.acc + 4 * n + q, ld(p.base + 4 * n + q), r4);
+    Real nx_ = 0, nz_ = 0;
+    if (depth == 0) { // free-surface projection, PointKernels2D.hpp:70-78
+        nx_ = ld(m.normals + 2 * q), nz_ = ld(m.normals + 2 * q + 1);
+        const Real tx = o2 * nx_ + o4 * nz_, tz = o4 * nx_ + o3 * nz_, nn = nx_ * tx + nz_ * tz;
+        o2 += -2 * nx_ * tx + nn * nx_ * nx_;
+        o3 += -2 * nz_ * tz + nn * nz_ * nz_;
+        o4 += -nx_ * tz - tx * nz_ + nn * nx_ * nz_;
+    }
+    storeField<Real, STAGE>(p, 2 * n + q, o2);
+    storeField<Real, STAGE>(p, 3 * n + q, o3);
+    storeField<Real, STAGE>(p, 4 * n + q, o4);
+    if (CPML) {
+        if (slot0 >= 0)
+            for (int f = 0; f < 2; ++f) combineMemory<Real, STAGE>(p, slot0 + f, prate[f], diag, withDiag);
+        if (slot1 >= 0)
+            for (int f = 0; f < 2; ++f) combineMemory<Real, STAGE>(p, slot1 + f, prate[2 + f], diag, withDiag);
+    }
+
+    // ---- phase 2: stress derivatives -> velocity rates
+    const Real rho = ld(m.rho + q);
+    Real r0, r1;
+    const bool near = depth <= (DZ ? 3 : 1);
+    if (!CPML) {
+        if (near) {
+            r0 = momentum<Real, DX, DZ>(m, t, q, 0, depth, -1);
+            r1 = momentum<Real, DX, DZ>(m, t, q, 1, depth, -1);
+        } else {
+            const Real x2 = tdrp<Real, DX>(t, m, 2, 0), x4 = tdrp<Real, DX>(t, m, 4, 0);
+            const Real e2 = tdrp<Real, DZ>(t, m, 2, 1), e3 = tdrp<Real, DZ>(t, m, 3, 1), e4 = tdrp<Real, DZ>(t, m, 4, 1);
+            r0 = ((x2 + a * e2) + b * e4) / rho;
+            r1 = ((x4 + a * e4) + b * e3) / rho;
+        }
+    } else {
+        Real mrate[4] = {0, 0, 0, 0}; // ADE rates of the momentum memories: slot0 f2,f3, slot1 f2,f3
+        Real rv[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int f = v ? 4 : 2, o = v ? 3 : 4;
+            Real X, Z;
+            if (near) {
+                X = momentum<Real, DX, DZ>(m, t, q, v, depth, 0);
+                Z = momentum<Real, DX, DZ>(m, t, q, v, depth, 1);
+            } else {
+                X = tdrp<Real, DX>(t, m, f, 0) / rho;
+                Z = (a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1)) / rho;
+            }
+            if (slot0 >= 0) X = stretch(prof0, ld(p.pin + slot0 + 2 + v), X, mrate[v]);
+            if (slot1 >= 0) Z = stretch(prof1, ld(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
+            rv[v] = X + Z;
+        }
+        r0 = rv[0], r1 = rv[1];
+        if (slot0 >= 0)
+            for (int v = 0; v < 2; ++v) combineMemory<Real, STAGE>(p, slot0 + 2 + v, mrate[v], diag, withDiag);
+        if (slot1 >= 0)
+            for (int v = 0; v < 2; ++v) combineMemory<Real, STAGE>(p, slot1 + 2 + v, mrate[2 + v], diag, withDiag);
+    }
+    if (i >= m.src_i0 && i < m.src_i1 && k >= m.src_k0 && k < m.src_k1) {
+        const Clock *clk = p.clock;
+        const Real forcing = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
+        if (m.sgx) {
+            r0 += forcing * ld(m.sgx + q) / rho;
+            r1 += forcing * ld(m.sgz + q) / rho;
+        } else {
+            const Real s = ld(m.source + q);
+            r0 += forcing * (s * m.sdx) / rho;
+            r1 += forcing * (s * m.sdz) / rho;
+        }
+    }
+    if (damped) {
+        r0 -= damp * t.at(0, 0, 0);
+        r1 -= damp * t.at(1, 0, 0);
+    }
+    const Real o0 = combine<Real, STAGE>(p, p.acc + q, ld(p.base + q), r0);
+    const Real o1 = combine<Real, STAGE>(p, p.acc + n + q, ld(p.base + n + q), r1);
+    storeField<Real, STAGE>(p, q, o0);
+    storeField<Real, STAGE>(p, n + q, o1);
+
+    if (STAGE == 3 && withDiag) { // energy, |v|^2, surface traction, finiteness (PointKernels2D.hpp:173-184)
+        if (!isfinite(o0) || !isfinite(o1) || !isfinite(o2) || !isfinite(o3) || !isfinite(o4)) diag.bad = 1;
+        const double l = lam, mu_ = mu, xx = o2, zz = o3, xz = o4, vx = o0, vz = o1;
+        // (l+2m)(xx^2+zz^2) - 2 l xx zz over 8m(l+m), plus xz^2/(2m), over one division
+        const double e = (.5 * double(rho) * (vx * vx + vz * vz) +
+                          (((l + 2 * mu_) * (xx * xx + zz * zz) - 2 * l * xx * zz) + 4 * (l + mu_) * xz * xz) / (8 * mu_ * (l + mu_))) *
+                         double(ld(m.jac + q)) * double(m.h) * double(m.h);
+        const double v2 = vx * vx + vz * vz;
+        if (!isfinite(e)) diag.bad = 1;
+        diag.energy += e;
+        diag.velocity = fmax(diag.velocity, v2); // squared; the root is taken once per CTA
+        if (depth == 0) {
+            const double tx = xx * double(nx_) + xz * double(nz_), tz = xz * double(nx_) + zz * double(nz_);
+            const double norm = sqrt(xx * xx + zz * zz + 2 * xz * xz);
+            diag.traction = fmax(diag.traction, sqrt(tx * tx + tz * tz) / fmax(norm, 1e-25));
         }
     }
 }
 
-// ---------------------------------------------------------------- diagnostics ------------
-struct Partial {
-    double energy, velocity, traction;
-    int bad, pad;
-};
+// Block reduction of the per-thread diagnostics into one partial per CTA.
+__device__ __forceinline__ void reducePartial(Partial s, Partial *out, int slot) {
+    for (int o = 16; o > 0; o >>= 1) {
+        s.energy += __shfl_down_sync(0xffffffffu, s.energy, o);
+        s.velocity = fmax(s.velocity, __shfl_down_sync(0xffffffffu, s.velocity, o));
+        s.traction = fmax(s.traction, __shfl_down_sync(0xffffffffu, s.traction, o));
+        s.bad |= __shfl_down_sync(0xffffffffu, s.bad, o);
+    }
+    __shared__ Partial warps[TILE_THREADS / 32];
+    const int t = threadIdx.x + blockDim.x * threadIdx.y, lane = t & 31, wid = t >> 5;
+    if (lane == 0) warps[wid] = s;
+    __syncthreads();
+    if (t == 0) {
+        Partial tot = warps[0];
+        for (int w = 1; w < TILE_THREADS / 32; ++w) {
+            tot.energy += warps[w].energy;
+            tot.velocity = fmax(tot.velocity, warps[w].velocity);
+            tot.traction = fmax(tot.traction, warps[w].traction);
+            tot.bad |= warps[w].bad;
+        }
+        tot.velocity = sqrt(tot.velocity); // the nodes accumulated |v|^2
+        out[slot] = tot;
+    }
+}
 
+// CTAs per SM the register allocation must allow: three FP64 tiles (3 x 57.8 KB of shared
+// memory) or four FP32 tiles.  Fewer resident CTAs leave the memory system idle (measured:
+// one FP64 CTA per SM runs at half the throughput of three).
+// GSLS nodes carry 6 + 4L fields, so they get one CTA fewer instead of spilling.
+template <class Real, int MECH> constexpr int minBlocks() { return (sizeof(Real) == 8 ? 3 : 4) - (MECH ? 1 : 0); }
+
+// The fused stage.  DX/DZ: MacCormack directions of this (step, stage); MECH: GSLS
+// mechanisms; STAGE: 0..3.  Block 32x8, tile 32x32 nodes (4 per thread).
+template <class Real, int DX, int DZ, int MECH, int STAGE>
+__global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage2d(const StageArgs<Real> p) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    Real *tile = reinterpret_cast<Real *>(smemRaw);
+    if (p.clock->faulted) return; // uniform across the grid
+    const Mesh<Real> &m = p.m;
+    const int i0 = 3 + blockIdx.x * TX, k0 = 3 + blockIdx.y * TZ;
+    const int tid = threadIdx.x + TX * threadIdx.y;
+    const long long n = m.count;
+    // stage the halo'd tile of the five stencil fields (rows of HX, x fastest)
+    for (int e = tid; e < 5 * HZ * HX; e += TILE_THREADS) {
+        const int f = e / (HZ * HX), r = e - f * (HZ * HX), zz = r / HX, xx = r - zz * HX;
+        const int gi = i0 - 3 + xx, gk = k0 - 3 + zz;
+        if (gi < m.nx && gk < m.nz) cpAsync(tile + e, p.in + f * n + gi + (long long)m.nx * gk, int(sizeof(Real)));
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    cpAsyncWaitAll();
+    __syncthreads();
+    Partial diag{0, 0, 0, 0, 0};
+    const bool withDiag = STAGE == 3 && p.partials != nullptr;
+#pragma unroll 1
+    for (int j = 0; j < ROWS_PER_THREAD; ++j) {
+        const int lz = threadIdx.y + (TILE_THREADS / TX) * j;
+        const int i = i0 + threadIdx.x, k = k0 + lz;
+        if (i < m.nx - 3 && k < m.nz - 3)
+            stageNode<Real, DX, DZ, MECH, STAGE>(p, Tile<Real>{tile + (lz + 3) * HX + threadIdx.x + 3}, i, k, diag, withDiag);
+    }
+    if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
+}
+
+// ---------------------------------------------------------------- diagnostics ------------
 // Per-block energy / peak velocity / surface traction / finiteness of a state
-// (src/two_d/CudaEngine2D.cu:43-78 semantics, PointKernels2D.hpp:181-184 energy).
+// (src/two_d/CudaEngine2D.cu:43-78 semantics, PointKernels2D.hpp:181-184 energy); used by
+// swl2d_diagnostics outside the step batches.
 template <class Real>
 __global__ void __launch_bounds__(256) stats2d(const Mesh<Real> m, const Real *__restrict__ w, const Real *__restrict__ pml,
                                                const Clock *clk, Partial *out) {

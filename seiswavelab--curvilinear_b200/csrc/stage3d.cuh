@@ -90,8 +90,12 @@ __device__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w,
     return sum / (m.h * ld(m.jac + q) * rho);
 }
 
+// Two CTAs of 256 threads per SM: without the bound the register allocation leaves one CTA per
+// SM and the memory system mostly idle (tighter bounds spill heavily in this kernel).
+template <class Real> constexpr int minBlocks3() { return 2; }
+
 template <class Real, int DX, int DY, int DZ, int STAGE>
-__global__ void __launch_bounds__(256) stage3d(const StageArgs<Real> p) {
+__global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const StageArgs<Real> p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;

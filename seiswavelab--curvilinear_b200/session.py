@@ -153,33 +153,73 @@ def _set(struct, field, value):
     setattr(struct, field, int(value) if t in (C.c_int32, C.c_int64) else float(value))
 
 
+def params2d(params: dict):
+    """swl_params2d from a parameter dictionary; returns (struct, arrays to keep alive)."""
+    L = _bind()
+    p = Params2D()
+    L.swl2d_params_default(C.byref(p))
+    keep = []
+    for k, v in params.items():
+        if k in _MAP2D:
+            _set(p, _MAP2D[k], v)
+    if "sourceDirection" in params:
+        for a in range(3):
+            p.source_direction[a] = float(params["sourceDirection"][a])
+    if "layers" in params:
+        rows = np.asarray(params["layers"], dtype=np.float64).reshape(-1, 6)
+        arr = (Layer2D * len(rows))(*[Layer2D(*r) for r in rows])
+        keep.append(arr)
+        p.layers, p.n_layers = arr, len(rows)
+    if "surface" in params:
+        xz = np.ascontiguousarray(params["surface"], dtype=np.float64).ravel()
+        keep.append(xz)
+        p.surface_xz, p.n_surface = xz.ctypes.data_as(_dp), len(xz) // 2
+    return p, keep
+
+
+def params3d(params: dict):
+    """swl_params3d from a parameter dictionary; returns (struct, arrays to keep alive)."""
+    L = _bind()
+    p = Params3D()
+    L.swl3d_params_default(C.byref(p))
+    keep = []
+    for k, v in params.items():
+        if k in _MAP3D:
+            _set(p, _MAP3D[k], v)
+    if "sourceDirection" in params:
+        for a in range(3):
+            p.source_direction[a] = float(params["sourceDirection"][a])
+    if "layers" in params:
+        rows = np.asarray(params["layers"], dtype=np.float64).reshape(-1, 4)
+        arr = (Layer3D * len(rows))(*[Layer3D(*r) for r in rows])
+        keep.append(arr)
+        p.layers, p.n_layers = arr, len(rows)
+    if "receiverArray" in params:  # kind startX startY z countX countY strideX strideY
+        r = [int(x) for x in params["receiverArray"]]
+        (p.receiver_kind, p.receiver_start_x, p.receiver_start_y, p.receiver_z, p.receiver_count_x,
+         p.receiver_count_y, p.receiver_stride_x, p.receiver_stride_y) = r
+    if "absorbingCells" in params:
+        for a in range(3):
+            p.absorbing_cells[a] = int(params["absorbingCells"][a])
+    if "demShape" in params:  # nx ny spacing originX originY datum
+        d = params["demShape"]
+        p.dem_nx, p.dem_ny = int(d[0]), int(d[1])
+        p.dem_spacing, p.dem_origin_x, p.dem_origin_y, p.dem_datum = map(float, d[2:6])
+        e = np.ascontiguousarray(params["demElevations"], dtype=np.float64)
+        keep.append(e)
+        p.dem_elevations = e.ctypes.data_as(_dp)
+    return p, keep
+
+
 class Simulation2D:
     """Seis2D::Curvilinear::Simulation on the B200 engine."""
 
     def __init__(self, params: dict, device: int = -1):
         L = _bind()
-        p = Params2D()
-        L.swl2d_params_default(C.byref(p))
-        self._keep = []
-        for k, v in params.items():
-            if k in _MAP2D:
-                _set(p, _MAP2D[k], v)
-        if "sourceDirection" in params:
-            for a in range(3):
-                p.source_direction[a] = float(params["sourceDirection"][a])
-        if "layers" in params:
-            rows = np.asarray(params["layers"], dtype=np.float64).reshape(-1, 6)
-            arr = (Layer2D * len(rows))(*[Layer2D(*r) for r in rows])
-            self._keep.append(arr)
-            p.layers, p.n_layers = arr, len(rows)
-        if "surface" in params:
-            xz = np.ascontiguousarray(params["surface"], dtype=np.float64).ravel()
-            self._keep.append(xz)
-            p.surface_xz, p.n_surface = xz.ctypes.data_as(_dp), len(xz) // 2
+        p, keep = params2d(params)
         h = C.c_void_p()
         _check(L.swl2d_session_create(C.byref(p), int(device), C.byref(h)))
         self._h = h
-        self._keep.clear()
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -235,38 +275,10 @@ class Simulation3D:
 
     def __init__(self, params: dict, device: int = -1):
         L = _bind()
-        p = Params3D()
-        L.swl3d_params_default(C.byref(p))
-        self._keep = []
-        for k, v in params.items():
-            if k in _MAP3D:
-                _set(p, _MAP3D[k], v)
-        if "sourceDirection" in params:
-            for a in range(3):
-                p.source_direction[a] = float(params["sourceDirection"][a])
-        if "layers" in params:
-            rows = np.asarray(params["layers"], dtype=np.float64).reshape(-1, 4)
-            arr = (Layer3D * len(rows))(*[Layer3D(*r) for r in rows])
-            self._keep.append(arr)
-            p.layers, p.n_layers = arr, len(rows)
-        if "receiverArray" in params:  # kind startX startY z countX countY strideX strideY
-            r = [int(x) for x in params["receiverArray"]]
-            (p.receiver_kind, p.receiver_start_x, p.receiver_start_y, p.receiver_z, p.receiver_count_x,
-             p.receiver_count_y, p.receiver_stride_x, p.receiver_stride_y) = r
-        if "absorbingCells" in params:
-            for a in range(3):
-                p.absorbing_cells[a] = int(params["absorbingCells"][a])
-        if "demShape" in params:  # nx ny spacing originX originY datum
-            d = params["demShape"]
-            p.dem_nx, p.dem_ny = int(d[0]), int(d[1])
-            p.dem_spacing, p.dem_origin_x, p.dem_origin_y, p.dem_datum = map(float, d[2:6])
-            e = np.ascontiguousarray(params["demElevations"], dtype=np.float64)
-            self._keep.append(e)
-            p.dem_elevations = e.ctypes.data_as(_dp)
+        p, keep = params3d(params)
         h = C.c_void_p()
         _check(L.swl3d_session_create(C.byref(p), int(device), C.byref(h)))
         self._h = h
-        self._keep.clear()
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

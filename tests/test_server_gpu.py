@@ -1,0 +1,118 @@
+"""Serving on the GPU: many shots run concurrently through the request loop.
+
+Each shot's records must be the same when it runs alone (session API) and when it runs in a mix
+with other shots of different sizes, physics and precisions (here they are identical bit for
+bit: every shot owns its state and the kernels are deterministic).  Admission respects the
+device-memory budget; an invalid request fails alone without disturbing the others.
+"""
+import importlib
+import time
+
+import numpy as np
+import pytest
+
+from cases import CASES_2D, CASES_3D
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mods(swl):
+    return importlib.import_module("swl_b200.session"), importlib.import_module("swl_b200.server")
+
+
+def mix():
+    long2 = dict(duration=1.0, maxSteps=300)
+    long3 = dict(duration=1.0, maxSteps=60)
+    shots = [
+        (2, dict(CASES_2D["cpml_external_moment_layers"], precision=1, **long2)),
+        (2, dict(CASES_2D["gsls3_cpml_surface_force"], precision=1, **long2)),
+        (2, dict(CASES_2D["sponge_force"], precision=0, **long2)),
+        (2, dict(CASES_2D["cpml_internal_steep"], precision=1, **long2)),
+        (3, dict(CASES_3D["moment_layered"], precision=1, **long3)),
+        (3, dict(CASES_3D["force"], precision=0, **long3)),
+        (2, dict(CASES_2D["gsls1_layers_sponge"], precision=1, **long2)),
+    ]
+    return shots
+
+
+def alone(S, dim, params):
+    sim = (S.Simulation2D if dim == 2 else S.Simulation3D)(params, device=0)
+    sim.advance(sim.info()["total_steps"])
+    return sim.records()
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(mods):
+    S, V = mods
+    shots = mix()
+    srv = V.Server(device=0, batch_steps=7)
+    ids = [srv.submit(p, dim) for dim, p in shots]
+    srv.drain()
+    st = srv.stats()
+    assert st["done"] == len(shots) and st["failed"] == 0
+    assert st["peak_running"] >= 2  # shots really overlapped
+    for (dim, p), sid in zip(shots, ids):
+        got = srv.records(sid)
+        want = alone(S, dim, p)
+        assert len(got) == len(want)
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g, w)
+        s = srv.status(sid)
+        assert s["state"] == "done" and s["steps_done"] == s["total_steps"] > 0
+        assert s["finish_s"] >= s["start_s"] >= s["submit_s"]
+
+
+def test_admission_respects_memory_budget(mods):
+    S, V = mods
+    p = dict(CASES_2D["cpml_external_moment_layers"], precision=1)
+    one = S.Simulation2D(p, device=0).info()["resident_bytes"]
+    budget = int(2.5 * (one + (64 << 20) + (16 << 20)))
+    srv = V.Server(device=0, memory_budget=budget, batch_steps=5)
+    ids = [srv.submit(p, 2) for _ in range(6)]
+    srv.drain()
+    st = srv.stats()
+    assert st["done"] == 6 and st["peak_resident_bytes"] <= budget
+    assert st["peak_running"] <= 3  # the budget, not the queue, limited concurrency
+    ref = srv.records(ids[0])
+    for sid in ids[1:]:
+        np.testing.assert_array_equal(srv.records(sid)[1], ref[1])
+
+
+def test_invalid_request_fails_alone(mods):
+    S, V = mods
+    srv = V.Server(device=0)
+    bad = srv.submit({"nx": 4, "nz": 40}, 2)
+    good = srv.submit(dict(CASES_2D["sponge_force"], precision=1), 2)
+    too_big = V.Server(device=0, memory_budget=1 << 20)
+    huge = too_big.submit(dict(CASES_2D["sponge_force"], precision=1), 2)
+    srv.drain()
+    too_big.drain()
+    assert srv.status(bad)["state"] == "failed" and "2D dimensions" in srv.status(bad)["error"]
+    assert srv.status(good)["state"] == "done"
+    assert too_big.status(huge)["state"] == "failed" and "budget" in too_big.status(huge)["error"]
+
+
+def test_next_finished_streams_completions(mods):
+    S, V = mods
+    srv = V.Server(device=0, batch_steps=4)
+    ids = {srv.submit(dict(CASES_2D["flat_surface_force"], precision=1), 2) for _ in range(3)}
+    seen = set()
+    t0 = time.time()
+    while len(seen) < 3 and time.time() - t0 < 60:
+        sid = srv.next_finished(2000)
+        if sid is not None:
+            seen.add(sid)
+    assert seen == ids
+
+
+def test_engine_async_batches_match_blocking_advance(swl):
+    from helpers import load_2d, receivers_2d
+    case, res, mesh = load_2d("gsls3_cpml_surface_force")
+    dt = float(res["dt"])
+    a = swl.Engine2D(mesh, receivers_2d(res))
+    a.advance(0, 20, dt, mesh["frequency"], mesh["scale"])
+    b = swl.Engine2D(mesh, receivers_2d(res))
+    b.launch(0, 20, dt, mesh["frequency"], mesh["scale"])
+    while not b.query()[0]:
+        time.sleep(0.001)
+    np.testing.assert_array_equal(a.fields(), b.fields())
