@@ -200,6 +200,68 @@ def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
     return ms, prof.as_dict()
 
 
+def serving_leg(args, device: int) -> dict:
+    """Shots/hour and latency of a seeded request stream: batched FP32 through the request loop
+    (requests submitted at their Poisson arrival times, concurrent shots on one GPU) versus the
+    plain FP64 path running the same requests one after another."""
+    import importlib
+    W = importlib.import_module("swl_b200.workloads")
+    S = importlib.import_module("swl_b200.session")
+    V = importlib.import_module("swl_b200.server")
+    reqs = W.serving_mix(n=args.serving_requests, rate=20.0, seed=5, scale=args.serving_scale,
+                         steps_scale=args.serving_steps)
+    a0 = reqs[0]["arrival"]
+    # batched FP32
+    srv = V.Server(device=device, batch_steps=64)
+    t0 = time.perf_counter()
+    ids = []
+    for r in reqs:
+        delay = (r["arrival"] - a0) - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(dict(r["params"], precision=1), r["dim"]))
+    srv.drain()
+    st = [srv.status(i) for i in ids]
+    failed = [s["error"] for s in st if s["state"] != "done"]
+    lat32 = np.array([s["finish_s"] - s["submit_s"] for s in st])
+    span32 = max(s["finish_s"] for s in st) - min(s["submit_s"] for s in st)
+    rec32 = [srv.records(i) for i in ids]
+    stats = srv.stats()
+    srv.close()
+    # sequential plain FP64 (same requests, arrival order, one at a time)
+    service, rec64 = [], []
+    for r in reqs:
+        t = time.perf_counter()
+        sim = (S.Simulation2D if r["dim"] == 2 else S.Simulation3D)(dict(r["params"], precision=0), device=device)
+        sim.advance(sim.info()["total_steps"])
+        rec64.append(sim.records())
+        del sim
+        service.append(time.perf_counter() - t)
+    finish, lat64, clock = [], [], 0.0
+    for r, s in zip(reqs, service):
+        start = max(clock, r["arrival"] - a0)
+        clock = start + s
+        lat64.append(clock - (r["arrival"] - a0))
+    span64 = clock
+    errs = []
+    for a, b in zip(rec32, rec64):
+        num = sum(float(np.sum((x - y) ** 2)) for x, y in zip(a, b))
+        den = sum(float(np.sum(y ** 2)) for y in b)
+        errs.append((num / den) ** 0.5 if den > 0 else 0.0)
+    shots = len(reqs)
+    return {
+        "requests": shots, "mix": f"seeded (seed 5) Poisson 20/s; 80% 2D elastic/GSLS, 20% 3D; grid edges x{args.serving_scale}, "
+                                  f"steps x{args.serving_steps} of the full mix",
+        "batched_fp32": {"shots_per_hour": shots / span32 * 3600, "p50_s": float(np.percentile(lat32, 50)),
+                         "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32,
+                         "peak_running": stats["peak_running"], "failed": failed},
+        "sequential_fp64": {"shots_per_hour": shots / span64 * 3600, "p50_s": float(np.percentile(lat64, 50)),
+                            "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64},
+        "shots_per_hour_ratio": (shots / span32) / (shots / span64),
+        "max_trace_rel_l2_fp32_vs_fp64": max(errs), "median_trace_rel_l2_fp32_vs_fp64": float(np.median(errs)),
+    }
+
+
 def gpu_arm(args):
     import torch
     rank = int(os.environ.get("RANK", 0))
@@ -275,6 +337,9 @@ def gpu_arm(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu:
         base = cpu_baseline(r64["params"], dim, args.cpu_steps, 1)
+    serving = None
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        serving = serving_leg(args, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -290,6 +355,8 @@ def gpu_arm(args):
         if r32:
             line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],
                             "roofline": r32["roofline"], "speedup_vs_fp64": r32["value"] / r64["value"]}
+        if serving:
+            line["serving"] = serving
         line["profile_fp64"] = r64["profile"]
         print(json.dumps(line), flush=True)
     if dist:
@@ -329,6 +396,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=48, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")
+    ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
