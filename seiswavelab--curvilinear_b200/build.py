@@ -54,14 +54,17 @@ def _deps() -> float:
 def _compile(unit: str, flags: list[str], verbose: bool, newest: float) -> Path:
     src = SRC / unit
     obj = OUT / (unit.replace("/", "_") + ".o")
-    if obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, newest):
-        return obj
     cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
+    stamp = obj.with_suffix(".cmd")  # the command an object was built with; a change rebuilds it
+    if (obj.exists() and stamp.exists() and stamp.read_text() == " ".join(cmd)
+            and obj.stat().st_mtime >= max(src.stat().st_mtime, newest)):
+        return obj
     if verbose:
         print(" ".join(cmd), flush=True)
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError(f"nvcc failed for {unit}:\n{proc.stdout}\n{proc.stderr}")
+    stamp.write_text(" ".join(cmd))
     if verbose and proc.stderr.strip():
         print(proc.stderr, flush=True)
     return obj

@@ -64,15 +64,17 @@ def test_each_result_is_the_same_alone_and_in_the_mix(mods):
 
 def test_admission_respects_memory_budget(mods):
     S, V = mods
-    p = dict(CASES_2D["cpml_external_moment_layers"], precision=1)
+    # large enough that the device bytes, not the fixed per-shot allowance, dominate
+    p = dict(CASES_2D["cpml_external_moment_layers"], precision=1, nx=1000, nz=400, maxSteps=60, duration=1.0)
     one = S.Simulation2D(p, device=0).info()["resident_bytes"]
-    budget = int(2.5 * (one + (64 << 20) + (16 << 20)))
+    charge = one + (16 << 20)  # a built shot is charged its resident bytes plus a margin
+    budget = int(2.5 * (one + (80 << 20)))
     srv = V.Server(device=0, memory_budget=budget, batch_steps=5)
     ids = [srv.submit(p, 2) for _ in range(6)]
     srv.drain()
     st = srv.stats()
     assert st["done"] == 6 and st["peak_resident_bytes"] <= budget
-    assert st["peak_running"] <= 3  # the budget, not the queue, limited concurrency
+    assert st["peak_running"] <= budget // charge < 6  # the budget, not the queue, limited concurrency
     ref = srv.records(ids[0])
     for sid in ids[1:]:
         np.testing.assert_array_equal(srv.records(sid)[1], ref[1])
