@@ -146,6 +146,33 @@ swl_status swl2d_profile(swl2d_engine *engine, int32_t first, int32_t count, dou
  * No counterpart in the reference (its engines launch on the legacy default stream). */
 swl_status swl2d_set_stream(swl2d_engine *engine, void *cuda_stream);
 
+/* A 2D FP64 state held in caller-owned device memory (padded nx x nz grid, x fastest). */
+typedef struct swl_state2d_view {
+    int32_t nx, nz;                             /* padded node counts */
+    double h;
+    const double *vx, *vz, *sxx, *szz, *sxz;   /* device pointers, nx*nz values each */
+    const double *lambda, *mu, *rho, *jac;     /* device pointers, nx*nz values each */
+    const double *normals;                     /* device pointer, 2 values per node */
+    const double *pml;                         /* device pointer to the CFS-PML memories, or null */
+    int32_t cpml_width_x, cpml_width_z;        /* strip widths when pml is given */
+} swl_state2d_view;
+
+/* Diagnostics of a 2D state without allocating any memory: the energy, peak |v|, peak surface
+ * traction ratio and finiteness that swl2d_diagnostics reports, computed from the caller's device
+ * arrays and written to out[0..3] in device memory (out[3] = 1 when every value is finite, else 0),
+ * enqueued on cuda_stream (null: the default stream).  It is meant for callers that cannot call
+ * cudaMalloc: processes whose device memory is owned entirely by their own allocator or pre-sized
+ * arena (a serving process that reserves the GPU up front, a framework's caching allocator), and
+ * latency-critical loops where an allocation could synchronise the device.  Its per-block partial
+ * sums live in one fixed device array inside this library, sized for at most 65,536 blocks of
+ * 32x8 nodes (about 16.7 million physical nodes); larger states are rejected with SWL_ERR_INVALID.
+ * Every GPU that loads the library holds that array (2 MiB) until the process exits.  The first
+ * call on a device looks up the array's device address, so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (on different streams, or on
+ * the same device from several threads) race and must be serialised by the caller.
+ * No counterpart in the reference. */
+swl_status swl2d_stats_noalloc(const swl_state2d_view *state, double *out, void *cuda_stream);
+
 /* ---------------------------------------------------------------- engine, 3D ---- */
 
 /* POD mirror of Seis3D::Curvilinear::Point::Mesh (src/three_d/PointKernels3D.hpp:13-21),

@@ -29,6 +29,7 @@ UNITS = {
     "engine3d_f64.cu": ["--fmad=false"],
     "engine3d_f32.cu": [],
     "abi.cpp": ["-x", "cu"],
+    "noalloc.cu": ["--fmad=false"],
     # C++20 host: model construction and sessions (no FMA on the host either, as in the reference)
     "host/gsls.cpp": [],
     "host/model2d.cpp": [],
