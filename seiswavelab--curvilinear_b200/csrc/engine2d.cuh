@@ -53,17 +53,20 @@ std::unique_ptr<Engine2D> makeEngine2D32(const swl_mesh2d &, const int64_t *, in
 namespace detail2 {
 
 template <class Real> struct Launch {
+    // Elastic stages run the streaming kernel, GSLS stages the tiled one.
     template <int DX, int DZ, int MECH, int ST> static void go(dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-        k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, k2::tileBytes<Real>(), s>>>(a);
+        if constexpr (MECH == 0) k2::stream2d<Real, DX, DZ, ST><<<g, b, k2::streamBytes<Real>(), s>>>(a);
+        else k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, k2::tileBytes<Real>(), s>>>(a);
     }
-    // Opt every instantiation into the tile's dynamic shared memory (above the 48 KB default).
-    template <int DX, int DZ, int MECH, int ST> static void allow() {
-        check(cudaFuncSetAttribute(k2::stage2d<Real, DX, DZ, MECH, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   int(k2::tileBytes<Real>())),
-              "2D stage shared memory");
-        check(cudaFuncSetAttribute(k2::stage2d<Real, DX, DZ, MECH, ST>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   int(cudaSharedmemCarveoutMaxShared)),
+    template <class K> static void allowKernel(K kernel, std::size_t bytes) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "2D stage shared memory");
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)),
               "2D stage shared-memory carveout");
+    }
+    // Opt every instantiation into its dynamic shared memory (above the 48 KB default).
+    template <int DX, int DZ, int MECH, int ST> static void allow() {
+        if constexpr (MECH == 0) allowKernel(k2::stream2d<Real, DX, DZ, ST>, k2::streamBytes<Real>());
+        else allowKernel(k2::stage2d<Real, DX, DZ, MECH, ST>, k2::tileBytes<Real>());
     }
     template <int DX, int DZ, int MECH> static void allowStages() {
         allow<DX, DZ, MECH, 0>(), allow<DX, DZ, MECH, 1>(), allow<DX, DZ, MECH, 2>(), allow<DX, DZ, MECH, 3>();
@@ -136,7 +139,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     bool previous_{false};  // set a_ holds the state before the last step
     int nrec_{}, traceCap_{}, forcingCap_{};
     dim3 grid_, block_{32, 8};                               // one node per thread (diagnostics kernel)
-    dim3 tileGrid_, tileBlock_{k2::TX, k2::TILE_THREADS / k2::TX}; // 32x32-node tiles (stage kernels)
+    dim3 stageGrid_, stageBlock_{32, 8}; // strips x segments (elastic) or 32x32-node tiles (GSLS)
     int nparts_{};
     k2::Clock hostClock_{};
     PinnedBuffer pinnedForcing_, pinnedClock_;
@@ -190,14 +193,14 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         for (int s = 0; s < 4; ++s) {
             auto a = args(s);
             if (s == 3 && verdict) a.partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
-            detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, tileGrid_, tileBlock_, stream_, a);
+            detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, stageGrid_, stageBlock_, stream_, a);
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
         check(cudaGetLastError(), "2D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
             if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
-            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), int(tileGrid_.x * tileGrid_.y), fresh, count_,
+            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), int(stageGrid_.x * stageGrid_.y), fresh, count_,
                                                          recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
             if (ev) check(cudaEventRecord(ev[6], stream_), "record event");
             check(cudaGetLastError(), "2D verdict launch");
@@ -356,16 +359,20 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.nz - 6 + block_.y - 1) / block_.y);
-        tileGrid_ = dim3((g.nx - 6 + k2::TX - 1) / k2::TX, (g.nz - 6 + k2::TZ - 1) / k2::TZ);
+        if (mech_ == 0)
+            stageGrid_ = dim3((g.nx - 6 + k2::SW - 1) / k2::SW, (g.nz - 6 + k2::SB * k2::SEG_BLOCKS - 1) / (k2::SB * k2::SEG_BLOCKS));
+        else
+            stageGrid_ = dim3((g.nx - 6 + k2::TX - 1) / k2::TX, (g.nz - 6 + k2::TZ - 1) / k2::TZ);
         nparts_ = grid_.x * grid_.y;
-        partials_.allocate(std::max<std::size_t>(nparts_, tileGrid_.x * tileGrid_.y) * sizeof(k2::Partial));
+        partials_.allocate(std::max<std::size_t>(nparts_, stageGrid_.x * stageGrid_.y) * sizeof(k2::Partial));
         detail2::Launch<Real>::prepare(mech_);
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
         cudaFuncAttributes attr{};
-        check(cudaFuncGetAttributes(&attr, k2::stage2d<Real, 0, 0, 0, 1>), "2D kernel compatibility");
+        if (mech_ == 0) check(cudaFuncGetAttributes(&attr, k2::stream2d<Real, 0, 0, 1>), "2D kernel compatibility");
+        else check(cudaFuncGetAttributes(&attr, k2::stage2d<Real, 0, 0, 1, 1>), "2D kernel compatibility");
         registers_ = attr.numRegs;
         localBytes_ = attr.localSizeBytes;
     }

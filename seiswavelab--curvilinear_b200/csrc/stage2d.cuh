@@ -1,12 +1,15 @@
 // 2D P-SV / GSLS device code: one fused kernel per classic-RK4 stage.
 //
-// A CTA owns a 32x32 tile of physical nodes.  It first stages the five stencil fields (Vx, Vz,
-// Sxx, Szz, Sxz) of the stage input over the tile plus a 3-node halo into shared memory with
-// asynchronous copies (cp.async; no registers held while the copies are in flight), then each
-// thread evaluates four nodes: the MacCormack-DRP derivatives from shared memory, the
-// metric-transformed right-hand side (src/two_d/PointKernels2D.hpp:121-172) with the
-// traction-image surface rows, CFS-PML ADE memories and GSLS relaxation, and immediately its
-// part of the RK combine and the free-surface projection -- the rates never touch HBM.
+// Each stage kernel evaluates, per node, the MacCormack-DRP derivatives of the five stencil
+// fields (Vx, Vz, Sxx, Szz, Sxz), the metric-transformed right-hand side
+// (src/two_d/PointKernels2D.hpp:121-172) with the traction-image surface rows, CFS-PML ADE
+// memories and GSLS relaxation, and immediately its part of the RK combine and the
+// free-surface projection -- the rates never touch HBM.  Two kernel shapes share that node code:
+//   stream2d (elastic): a CTA walks a 32-column strip down 64 rows, 8 rows at a time, with
+//     every operand (a ring of stencil rows, U, A and the model words) staged in shared memory
+//     by asynchronous copies one row block ahead of the arithmetic;
+//   stage2d (GSLS): a CTA stages a 32x32 tile plus a 3-node halo of the stencil fields and
+//     reads the per-node words (6 + 4L fields) from global memory.
 // Three state sets stay resident beside the stage outputs:
 //   U (state at the start of the step), A (running RK accumulator), S (stage state).
 // Stage 0 writes A = k1 and S = U + dt/2 k1; stages 1-2 add 2k to A and write
@@ -130,82 +133,134 @@ __device__ __forceinline__ Real near3(const Real *__restrict__ v, long long q, l
     return r / h;
 }
 
-// ------------------------------------------------------------- tiled 2D stage
+// ------------------------------------------------------------- node sources
+// The node arithmetic reads its operands through a source: the five stencil fields of the
+// stage input at (dx, dz) from the node, the start-of-step state U and the RK accumulator A of
+// the node, and its model words.  TileNode serves the tiled kernel (taps staged in shared
+// memory, the other words read from global memory); StreamNode serves the streaming kernel
+// (every word staged in shared memory one row block ahead of use).  `exact`: h is a power of
+// two, so x/h is formed as x*(1/h) -- the same value -- and no division is compiled in.
 constexpr int TX = 32, TZ = 32, HX = TX + 6, HZ = TZ + 6; // tile and halo'd tile
 constexpr int TILE_THREADS = 256, ROWS_PER_THREAD = TZ / (TILE_THREADS / TX);
 template <class Real> constexpr std::size_t tileBytes() { return sizeof(Real) * 5 * HZ * HX; }
 
-// Taps of the five stencil fields around one node in the shared tile.
-template <class Real> struct Tile {
-    const Real *c; // centre element of field 0
+template <class Real, bool EXACT> struct TileNode {
+    static constexpr bool exact = EXACT;
+    const Real *c; // centre element of field 0 in the tile
+    long long q, n;
+    int stage0;    // stage 0 reads U from the tile (U is the stage input)
     __device__ __forceinline__ Real at(int f, int dx, int dz) const { return c[f * (HZ * HX) + dz * HX + dx]; }
+    __device__ __forceinline__ Real u(const StageArgs<Real> &p, int f) const { return stage0 ? at(f, 0, 0) : ld(p.base + f * n + q); }
+    __device__ __forceinline__ Real acc(const StageArgs<Real> &p, int f) const { return p.acc[f * n + q]; }
+    __device__ __forceinline__ Real a(const Mesh<Real> &m) const { return ld(m.a + q); }
+    __device__ __forceinline__ Real b(const Mesh<Real> &m) const { return ld(m.b + q); }
+    __device__ __forceinline__ Real lam(const Mesh<Real> &m) const { return ld(m.lambda + q); }
+    __device__ __forceinline__ Real mu(const Mesh<Real> &m) const { return ld(m.mu + q); }
+    __device__ __forceinline__ Real rho(const Mesh<Real> &m) const { return ld(m.rho + q); }
+    __device__ __forceinline__ Real jac(const Mesh<Real> &m) const { return ld(m.jac + q); }
 };
 
-template <class Real> __device__ __forceinline__ Real scaled(const Mesh<Real> &m, Real r) {
-    // r/h; for h = 2^k the exact reciprocal gives the identical result with a multiply
-    return m.hinvExact ? r * m.hinv : r / m.h;
+// Streaming geometry: a CTA owns a strip of SW node columns and a segment of SB*SEG_BLOCKS
+// node rows, and walks down the segment one block of SB rows (one row per warp) at a time.
+// Shared memory holds a ring of RING stencil rows (five fields, SW + 6 columns each) and two
+// buffers of the per-node words of a row block.
+constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, RING = 3 * SB, RC = 40, RS = 5 * RC, PW = 16;
+constexpr int STREAM_THREADS = SW * SB;
+enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15 };
+template <class Real> constexpr std::size_t streamBytes() { return sizeof(Real) * (RING * RS + 2 * PW * STREAM_THREADS); }
+
+template <class Real, bool EXACT, int STAGE> struct StreamNode {
+    static constexpr bool exact = EXACT;
+    const Real *col; // ring slot 0, field 0, this node's column
+    const Real *pw;  // this node's per-node words (stride STREAM_THREADS)
+    long long q;
+    int centre;      // ring slot of this node's row
+    __device__ __forceinline__ Real at(int f, int dx, int dz) const {
+        int s = centre + dz;
+        s = s < 0 ? s + RING : s >= RING ? s - RING : s;
+        return col[s * RS + f * RC + dx];
+    }
+    __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
+    __device__ __forceinline__ Real u(const StageArgs<Real> &, int f) const { return STAGE == 0 ? at(f, 0, 0) : word(PW_U + f); }
+    __device__ __forceinline__ Real acc(const StageArgs<Real> &, int f) const { return word(PW_A + f); }
+    __device__ __forceinline__ Real a(const Mesh<Real> &) const { return word(PW_a); }
+    __device__ __forceinline__ Real b(const Mesh<Real> &) const { return word(PW_b); }
+    __device__ __forceinline__ Real lam(const Mesh<Real> &) const { return word(PW_lam); }
+    __device__ __forceinline__ Real mu(const Mesh<Real> &) const { return word(PW_mu); }
+    __device__ __forceinline__ Real rho(const Mesh<Real> &) const { return word(PW_rho); }
+    __device__ __forceinline__ Real jac(const Mesh<Real> &m) const { return STAGE == 3 ? word(PW_jac) : ld(m.jac + q); }
+};
+
+// ------------------------------------------------------------- stencils on a node source
+// The reference accumulates each derivative from zero (PointKernels2D.hpp:38-47); starting
+// from the first product gives the same value (0 + x == x, up to the sign of a zero result).
+template <class Real, class S> __device__ __forceinline__ Real scaled(const Mesh<Real> &m, Real r) {
+    if constexpr (S::exact) return r * m.hinv;
+    else return r / m.h;
 }
-template <class Real, int DIR> __device__ __forceinline__ Real tdrp(const Tile<Real> &t, const Mesh<Real> &m, int f, int axis) {
+template <class Real, int DIR, class S> __device__ __forceinline__ Real tdrp(const S &t, const Mesh<Real> &m, int f, int axis) {
     const int sx = axis ? 0 : 1, sz = axis ? 1 : 0;
-    Real r = Real(0);
+    Real r;
     if (DIR == 0) {
-        r += Real(-.30874) * t.at(f, -sx, -sz);
+        r = Real(-.30874) * t.at(f, -sx, -sz);
         r += Real(-.6326) * t.at(f, 0, 0);
         r += Real(1.233) * t.at(f, sx, sz);
         r += Real(-.3334) * t.at(f, 2 * sx, 2 * sz);
         r += Real(.04168) * t.at(f, 3 * sx, 3 * sz);
     } else {
-        r += -Real(-.30874) * t.at(f, sx, sz);
+        r = -Real(-.30874) * t.at(f, sx, sz);
         r += -Real(-.6326) * t.at(f, 0, 0);
         r += -Real(1.233) * t.at(f, -sx, -sz);
         r += -Real(-.3334) * t.at(f, -2 * sx, -2 * sz);
         r += -Real(.04168) * t.at(f, -3 * sx, -3 * sz);
     }
-    return scaled(m, r);
+    return scaled<Real, S>(m, r);
 }
-template <class Real, int DIR> __device__ __forceinline__ Real tnear2(const Tile<Real> &t, const Mesh<Real> &m, int f) {
-    Real r = Real(0);
+template <class Real, int DIR, class S> __device__ __forceinline__ Real tnear2(const S &t, const Mesh<Real> &m, int f) {
+    Real r;
     if (DIR == 0) {
-        r += Real(-1) * t.at(f, 0, 0);
+        r = Real(-1) * t.at(f, 0, 0);
         r += Real(1) * t.at(f, 0, 1);
     } else {
-        r += -Real(-1) * t.at(f, 0, 0);
+        r = -Real(-1) * t.at(f, 0, 0);
         r += -Real(1) * t.at(f, 0, -1);
     }
-    return scaled(m, r);
+    return scaled<Real, S>(m, r);
 }
-template <class Real, int DIR> __device__ __forceinline__ Real tnear3(const Tile<Real> &t, const Mesh<Real> &m, int f) {
+template <class Real, int DIR, class S> __device__ __forceinline__ Real tnear3(const S &t, const Mesh<Real> &m, int f) {
     const Real c0 = Real(-7) / Real(6), c1 = Real(8) / Real(6), c2 = Real(-1) / Real(6);
-    Real r = Real(0);
+    Real r;
     if (DIR == 0) {
-        r += c0 * t.at(f, 0, 0);
+        r = c0 * t.at(f, 0, 0);
         r += c1 * t.at(f, 0, 1);
         r += c2 * t.at(f, 0, 2);
     } else {
-        r += -c0 * t.at(f, 0, 0);
+        r = -c0 * t.at(f, 0, 0);
         r += -c1 * t.at(f, 0, -1);
         r += -c2 * t.at(f, 0, -2);
     }
-    return scaled(m, r);
+    return scaled<Real, S>(m, r);
 }
 
 // Traction flux J (x sigma_a + z sigma_b) at the tap (dx, dz) (PointKernels2D.hpp:90-93).
-template <class Real>
-__device__ __forceinline__ Real flux(const Mesh<Real> &m, const Tile<Real> &t, long long q, int dx, int dz, int axis, int comp) {
-    const long long qq = q + dx + (long long)dz * m.nx;
+template <class Real, class S>
+__device__ __forceinline__ Real flux(const Mesh<Real> &m, const S &t, int dx, int dz, int axis, int comp) {
+    const long long qq = t.q + dx + (long long)dz * m.nx;
     const Real x = axis ? ld(m.a + qq) : Real(1), z = axis ? ld(m.b + qq) : Real(0);
     return ld(m.jac + qq) * (x * t.at(comp ? 4 : 2, dx, dz) + z * t.at(comp ? 3 : 4, dx, dz));
 }
 
 // Conservative traction-image momentum near the surface (PointKernels2D.hpp:94-120):
 // the surface tap is dropped and taps above it mirror with a sign flip.  only = -1: both axes.
-template <class Real, int DX, int DZ>
-__device__ Real momentum(const Mesh<Real> &m, const Tile<Real> &t, long long q, int comp, int depth, int only) {
+template <class Real, int DX, int DZ, class S>
+__device__ __forceinline__ Real momentum(const Mesh<Real> &m, const S &t, Real jac, Real rho, int comp, int depth, int only) {
     const Real C[5] = {Real(-.30874), Real(-.6326), Real(1.233), Real(-.3334), Real(.04168)};
     Real r = Real(0);
+#pragma unroll
     for (int axis = 0; axis < 2; ++axis) {
         if (only >= 0 && axis != only) continue;
         const int dir = axis ? DZ : DX;
+#pragma unroll
         for (int l = 0; l < 5; ++l) {
             const int pos = l - 1;
             int off = dir ? -pos : pos;
@@ -219,10 +274,10 @@ __device__ Real momentum(const Mesh<Real> &m, const Tile<Real> &t, long long q, 
                     sign = Real(-1);
                 }
             }
-            r += sign * c * flux(m, t, q, axis ? 0 : off, axis ? off : 0, axis, comp);
+            r += sign * c * flux(m, t, axis ? 0 : off, axis ? off : 0, axis, comp);
         }
     }
-    return r / (m.h * ld(m.jac + q) * ld(m.rho + q));
+    return r / (m.h * jac * rho);
 }
 
 // CFS-PML ADE (PointKernels2D.hpp:57-64): returns d/kappa + psi, rate -(d/k+a) psi - d/k^2 d.
@@ -238,23 +293,34 @@ __device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes)
     if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitPrior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
+// `acc` is the node's A (unused in stage 0); `accOut` receives the new A (stages 0-2).
 template <class Real, int STAGE>
-__device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real *acc, Real u, Real r) {
+__device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real acc, Real u, Real r, Real &accOut) {
     if (STAGE == 0) {
-        *acc = r;
+        accOut = r;
         return u + p.weight * r;
     } else if (STAGE < 3) {
-        *acc = *acc + 2 * r;
+        accOut = acc + 2 * r;
         return u + p.weight * r;
     }
-    return u + p.delta * (*acc + r) / Real(6);
+    accOut = Real(0);
+    return u + p.delta * (acc + r) / Real(6);
 }
-template <class Real, int STAGE> __device__ __forceinline__ void storeField(const StageArgs<Real> &p, long long at, Real v) {
-    (STAGE == 3 ? p.acc : p.out)[at] = v;
+// Stages 0-2 write A and the stage output; stage 3 writes the new state over A.
+template <class Real, int STAGE>
+__device__ __forceinline__ void store(const StageArgs<Real> &p, long long at, Real out, Real accOut) {
+    if (STAGE < 3) {
+        p.acc[at] = accOut;
+        p.out[at] = out;
+    } else {
+        p.acc[at] = out;
+    }
 }
 // ADE memory update of one slot value (same scheme as the fields).
 template <class Real, int STAGE>
@@ -277,12 +343,12 @@ __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long lon
 // stress (and GSLS) rates -> combine/store of the stresses; (2) stress derivatives -> velocity
 // rates -> combine/store of the velocities.  Every expression keeps the reference's operation
 // order (src/two_d/PointKernels2D.hpp:121-172); only independent computations are reordered.
-template <class Real, int DX, int DZ, int MECH, int STAGE>
-__device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<Real> &t, int i, int k, Partial &diag,
-                                          bool withDiag) {
+// GSLS memory fields (index >= 5) are read and written in global memory directly.
+template <class Real, int DX, int DZ, int MECH, int STAGE, class S>
+__device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, int i, int k, Partial &diag, bool withDiag) {
     const Mesh<Real> &m = p.m;
     const bool CPML = m.wz > 0;
-    const long long n = m.count, q = i + (long long)m.nx * k;
+    const long long n = m.count, q = t.q;
     const int depth = k - 3;
     const Real *__restrict__ w = p.in;
     const bool damped = !(i >= m.dmp_i0 && i < m.dmp_i1 && k < m.dmp_k1);
@@ -298,7 +364,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
         if (kc >= nzc - m.wz)
             slot1 = 4 * ((long long)(2 * m.wx) * nzc + (long long)(kc - (nzc - m.wz)) * nxc + ic), prof1 = m.cpz + 3 * kc;
     }
-    const Real a = ld(m.a + q), b = ld(m.b + q);
+    const Real a = t.a(m), b = t.b(m);
 
     // ---- phase 1: velocity derivatives -> stress and GSLS rates
     Real xv[2], vxs[2], ev[2];
@@ -308,7 +374,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
     Real prate[4] = {0, 0, 0, 0}; // ADE rates of the velocity-derivative memories: slot0 f0,f1, slot1 f0,f1
     if (CPML && slot0 >= 0)
         for (int v = 0; v < 2; ++v) vxs[v] = stretch(prof0, ld(p.pin + slot0 + v), xv[v], prate[v]);
-    const Real lam = ld(m.lambda + q), mu = ld(m.mu + q);
+    const Real lam = t.lam(m), mu = t.mu(m);
     if (depth == 0) { // surface eta-derivative from the traction-free condition (PointKernels2D.hpp:79-89)
         const Real c0 = a, c1 = b, c2 = c0 * c0 + c1 * c1, len = sqrt(c2);
         const Real nn[2] = {c0 / len, c1 / len};
@@ -364,15 +430,17 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
                 Real rm = m.rates[l] * (drive[f] - wm[f]);
                 if (damped) rm -= damp * wm[f];
                 const long long at = (mm + f) * n + q;
-                const Real o = combine<Real, STAGE>(p, p.acc + at, ld(p.base + at), rm);
-                storeField<Real, STAGE>(p, at, o);
+                Real an;
+                const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), rm, an);
+                store<Real, STAGE>(p, at, o, an);
                 if (withDiag && !isfinite(o)) diag.bad = 1;
             }
         }
         if (damped) r5 -= damp * ld(w + 5 * n + q);
         const long long at = 5 * n + q;
-        const Real o = combine<Real, STAGE>(p, p.acc + at, ld(p.base + at), r5);
-        storeField<Real, STAGE>(p, at, o);
+        Real an;
+        const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), r5, an);
+        store<Real, STAGE>(p, at, o, an);
         if (withDiag && !isfinite(o)) diag.bad = 1;
     }
     if (damped) {
@@ -380,9 +448,10 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
         r3 -= damp * t.at(3, 0, 0);
         r4 -= damp * t.at(4, 0, 0);
     }
-    Real o2 = combine<Real, STAGE>(p, p.acc + 2 * n + q, ld(p.base + 2 * n + q), r2);
-    Real o3 = combine<Real, STAGE>(p, p.acc + 3 * n + q, ld(p.base + 3 * n + q), r3);
-    Real o4 = combine<Real, STAGE>(p, p.acc + 4 * n + q, ld(p.base + 4 * n + q), r4);
+    Real a2, a3, a4;
+    Real o2 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 2) : Real(0), t.u(p, 2), r2, a2);
+    Real o3 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 3) : Real(0), t.u(p, 3), r3, a3);
+    Real o4 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 4) : Real(0), t.u(p, 4), r4, a4);
     Real nx_ = 0, nz_ = 0;
     if (depth == 0) { // free-surface projection, PointKernels2D.hpp:70-78
         nx_ = ld(m.normals + 2 * q), nz_ = ld(m.normals + 2 * q + 1);
@@ -391,9 +460,9 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
         o3 += -2 * nz_ * tz + nn * nz_ * nz_;
         o4 += -nx_ * tz - tx * nz_ + nn * nx_ * nz_;
     }
-    storeField<Real, STAGE>(p, 2 * n + q, o2);
-    storeField<Real, STAGE>(p, 3 * n + q, o3);
-    storeField<Real, STAGE>(p, 4 * n + q, o4);
+    store<Real, STAGE>(p, 2 * n + q, o2, a2);
+    store<Real, STAGE>(p, 3 * n + q, o3, a3);
+    store<Real, STAGE>(p, 4 * n + q, o4, a4);
     if (CPML) {
         if (slot0 >= 0)
             for (int f = 0; f < 2; ++f) combineMemory<Real, STAGE>(p, slot0 + f, prate[f], diag, withDiag);
@@ -402,13 +471,14 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
     }
 
     // ---- phase 2: stress derivatives -> velocity rates
-    const Real rho = ld(m.rho + q);
+    const Real rho = t.rho(m);
     Real r0, r1;
     const bool near = depth <= (DZ ? 3 : 1);
     if (!CPML) {
         if (near) {
-            r0 = momentum<Real, DX, DZ>(m, t, q, 0, depth, -1);
-            r1 = momentum<Real, DX, DZ>(m, t, q, 1, depth, -1);
+            const Real jac = t.jac(m);
+            r0 = momentum<Real, DX, DZ>(m, t, jac, rho, 0, depth, -1);
+            r1 = momentum<Real, DX, DZ>(m, t, jac, rho, 1, depth, -1);
         } else {
             const Real x2 = tdrp<Real, DX>(t, m, 2, 0), x4 = tdrp<Real, DX>(t, m, 4, 0);
             const Real e2 = tdrp<Real, DZ>(t, m, 2, 1), e3 = tdrp<Real, DZ>(t, m, 3, 1), e4 = tdrp<Real, DZ>(t, m, 4, 1);
@@ -423,8 +493,9 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
             const int f = v ? 4 : 2, o = v ? 3 : 4;
             Real X, Z;
             if (near) {
-                X = momentum<Real, DX, DZ>(m, t, q, v, depth, 0);
-                Z = momentum<Real, DX, DZ>(m, t, q, v, depth, 1);
+                const Real jac = t.jac(m);
+                X = momentum<Real, DX, DZ>(m, t, jac, rho, v, depth, 0);
+                Z = momentum<Real, DX, DZ>(m, t, jac, rho, v, depth, 1);
             } else {
                 X = tdrp<Real, DX>(t, m, f, 0) / rho;
                 Z = (a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1)) / rho;
@@ -455,10 +526,11 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
         r0 -= damp * t.at(0, 0, 0);
         r1 -= damp * t.at(1, 0, 0);
     }
-    const Real o0 = combine<Real, STAGE>(p, p.acc + q, ld(p.base + q), r0);
-    const Real o1 = combine<Real, STAGE>(p, p.acc + n + q, ld(p.base + n + q), r1);
-    storeField<Real, STAGE>(p, q, o0);
-    storeField<Real, STAGE>(p, n + q, o1);
+    Real a0, a1;
+    const Real o0 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 0) : Real(0), t.u(p, 0), r0, a0);
+    const Real o1 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 1) : Real(0), t.u(p, 1), r1, a1);
+    store<Real, STAGE>(p, q, o0, a0);
+    store<Real, STAGE>(p, n + q, o1, a1);
 
     if (STAGE == 3 && withDiag) { // energy, |v|^2, surface traction, finiteness (PointKernels2D.hpp:173-184)
         if (!isfinite(o0) || !isfinite(o1) || !isfinite(o2) || !isfinite(o3) || !isfinite(o4)) diag.bad = 1;
@@ -466,7 +538,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
         // (l+2m)(xx^2+zz^2) - 2 l xx zz over 8m(l+m), plus xz^2/(2m), over one division
         const double e = (.5 * double(rho) * (vx * vx + vz * vz) +
                           (((l + 2 * mu_) * (xx * xx + zz * zz) - 2 * l * xx * zz) + 4 * (l + mu_) * xz * xz) / (8 * mu_ * (l + mu_))) *
-                         double(ld(m.jac + q)) * double(m.h) * double(m.h);
+                         double(t.jac(m)) * double(m.h) * double(m.h);
         const double v2 = vx * vx + vz * vz;
         if (!isfinite(e)) diag.bad = 1;
         diag.energy += e;
@@ -479,7 +551,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const Tile<R
     }
 }
 
-// Block reduction of the per-thread diagnostics into one partial per CTA.
+// Block reduction of the per-thread diagnostics into one partial per CTA (256 threads).
 __device__ __forceinline__ void reducePartial(Partial s, Partial *out, int slot) {
     for (int o = 16; o > 0; o >>= 1) {
         s.energy += __shfl_down_sync(0xffffffffu, s.energy, o);
@@ -504,19 +576,15 @@ __device__ __forceinline__ void reducePartial(Partial s, Partial *out, int slot)
     }
 }
 
+// ------------------------------------------------------------- tiled stage (GSLS)
 // CTAs per SM the register allocation must allow: three FP64 tiles (3 x 57.8 KB of shared
 // memory) or four FP32 tiles.  Fewer resident CTAs leave the memory system idle (measured:
 // one FP64 CTA per SM runs at half the throughput of three).
 // GSLS nodes carry 6 + 4L fields, so they get one CTA fewer instead of spilling.
 template <class Real, int MECH> constexpr int minBlocks() { return (sizeof(Real) == 8 ? 3 : 4) - (MECH ? 1 : 0); }
 
-// The fused stage.  DX/DZ: MacCormack directions of this (step, stage); MECH: GSLS
-// mechanisms; STAGE: 0..3.  Block 32x8, tile 32x32 nodes (4 per thread).
-template <class Real, int DX, int DZ, int MECH, int STAGE>
-__global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage2d(const StageArgs<Real> p) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    Real *tile = reinterpret_cast<Real *>(smemRaw);
-    if (p.clock->faulted) return; // uniform across the grid
+template <class Real, int DX, int DZ, int MECH, int STAGE, bool EXACT>
+__device__ __forceinline__ void tileBody(const StageArgs<Real> &p, Real *tile) {
     const Mesh<Real> &m = p.m;
     const int i0 = 3 + blockIdx.x * TX, k0 = 3 + blockIdx.y * TZ;
     const int tid = threadIdx.x + TX * threadIdx.y;
@@ -527,7 +595,7 @@ __global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage
         const int gi = i0 - 3 + xx, gk = k0 - 3 + zz;
         if (gi < m.nx && gk < m.nz) cpAsync(tile + e, p.in + f * n + gi + (long long)m.nx * gk, int(sizeof(Real)));
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    cpAsyncCommit();
     cpAsyncWaitAll();
     __syncthreads();
     Partial diag{0, 0, 0, 0, 0};
@@ -536,10 +604,118 @@ __global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage
     for (int j = 0; j < ROWS_PER_THREAD; ++j) {
         const int lz = threadIdx.y + (TILE_THREADS / TX) * j;
         const int i = i0 + threadIdx.x, k = k0 + lz;
-        if (i < m.nx - 3 && k < m.nz - 3)
-            stageNode<Real, DX, DZ, MECH, STAGE>(p, Tile<Real>{tile + (lz + 3) * HX + threadIdx.x + 3}, i, k, diag, withDiag);
+        if (i < m.nx - 3 && k < m.nz - 3) {
+            const TileNode<Real, EXACT> t{tile + (lz + 3) * HX + threadIdx.x + 3, i + (long long)m.nx * k, n, STAGE == 0};
+            stageNode<Real, DX, DZ, MECH, STAGE>(p, t, i, k, diag, withDiag);
+        }
     }
     if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
+}
+
+// The fused tiled stage.  DX/DZ: MacCormack directions of this (step, stage); MECH: GSLS
+// mechanisms; STAGE: 0..3.  Block 32x8, tile 32x32 nodes (4 per thread).
+template <class Real, int DX, int DZ, int MECH, int STAGE>
+__global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage2d(const __grid_constant__ StageArgs<Real> p) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    if (p.clock->faulted) return; // uniform across the grid
+    Real *tile = reinterpret_cast<Real *>(smemRaw);
+    if constexpr (sizeof(Real) == 4) tileBody<Real, DX, DZ, MECH, STAGE, true>(p, tile);
+    else if (p.m.hinvExact) tileBody<Real, DX, DZ, MECH, STAGE, true>(p, tile);
+    else tileBody<Real, DX, DZ, MECH, STAGE, false>(p, tile);
+}
+
+// ------------------------------------------------------------- streaming stage (elastic)
+// A CTA walks its strip down one block of 8 rows at a time.  While it evaluates block b, the
+// copies of block b+1 (its 8 new stencil rows and the U, A and model words of its 256 nodes)
+// are in flight; after block b it issues those of block b+2.  The evaluation therefore reads
+// shared memory only, and each thread keeps one block of copies in flight.
+template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 4; }
+
+template <class Real, int DX, int DZ, int STAGE, bool EXACT>
+__device__ __forceinline__ void streamBody(const StageArgs<Real> &p, Real *ring, Real *pw) {
+    constexpr int T = STREAM_THREADS;
+    constexpr int bytes = int(sizeof(Real));
+    const Mesh<Real> &m = p.m;
+    const int lane = threadIdx.x, wy = threadIdx.y, tid = lane + SW * wy;
+    const int i0 = 3 + blockIdx.x * SW, z0 = 3 + blockIdx.y * (SB * SEG_BLOCKS), zb = z0 - 3;
+    const int iEnd = m.nx - 3, kEnd = m.nz - 3;
+    const long long n = m.count, nx = m.nx;
+    const int blocks = min(SEG_BLOCKS, (kEnd - z0 + SB - 1) / SB);
+    const int gx = i0 - 3 + lane; // first staged column of this lane (and gx + 32 for lanes 0-5)
+    const bool colA = gx < m.nx, colB = lane < 6 && gx + 32 < m.nx;
+    // ring rows [rel0, rel0 + rows) relative to row zb; warp wy stages every SB-th row
+    auto stageRows = [&](int rel0, int rows) {
+        for (int r = wy; r < rows; r += SB) {
+            const int rel = rel0 + r, gk = zb + rel;
+            if (gk >= m.nz) break;
+            Real *dst = ring + (rel % RING) * RS + lane;
+            const Real *src = p.in + (long long)gk * nx + gx;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                if (colA) cpAsync(dst + f * RC, src + f * n, bytes);
+                if (colB) cpAsync(dst + f * RC + 32, src + f * n + 32, bytes);
+            }
+        }
+    };
+    // per-node words of row block blk into buffer blk & 1
+    auto stagePoint = [&](int blk) {
+        const int k = z0 + blk * SB + wy, i = i0 + lane;
+        if (k >= kEnd || i >= iEnd) return;
+        const long long q = i + nx * k;
+        Real *dst = pw + (blk & 1) * (PW * T) + tid;
+        if (STAGE > 0) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                cpAsync(dst + (PW_U + f) * T, p.base + f * n + q, bytes);
+                cpAsync(dst + (PW_A + f) * T, p.acc + f * n + q, bytes);
+            }
+        }
+        cpAsync(dst + PW_a * T, m.a + q, bytes);
+        cpAsync(dst + PW_b * T, m.b + q, bytes);
+        cpAsync(dst + PW_lam * T, m.lambda + q, bytes);
+        cpAsync(dst + PW_mu * T, m.mu + q, bytes);
+        cpAsync(dst + PW_rho * T, m.rho + q, bytes);
+        if (STAGE == 3) cpAsync(dst + PW_jac * T, m.jac + q, bytes);
+    };
+    stageRows(0, SB + 6);
+    stagePoint(0);
+    cpAsyncCommit();
+    if (blocks > 1) stageRows(SB + 6, SB), stagePoint(1);
+    cpAsyncCommit();
+    Partial diag{0, 0, 0, 0, 0};
+    const bool withDiag = STAGE == 3 && p.partials != nullptr;
+#pragma unroll 1
+    for (int blk = 0; blk < blocks; ++blk) {
+        cpAsyncWaitPrior(); // this block's group has landed (the next one may still fly)
+        __syncthreads();
+        const int k = z0 + blk * SB + wy, i = i0 + lane;
+        if (k < kEnd && i < iEnd) {
+            StreamNode<Real, EXACT, STAGE> s;
+            s.col = ring + lane + 3;
+            s.pw = pw + (blk & 1) * (PW * T) + tid;
+            s.q = i + nx * k;
+            const int c = SB * (blk % 3) + wy + 3; // ring slot of row k (rel = SB*blk + wy + 3)
+            s.centre = c >= RING ? c - RING : c;
+            stageNode<Real, DX, DZ, 0, STAGE>(p, s, i, k, diag, withDiag);
+        }
+        __syncthreads(); // block blk's ring rows and buffer are free
+        if (blk + 2 < blocks) stageRows(SB * (blk + 2) + 6, SB), stagePoint(blk + 2);
+        cpAsyncCommit();
+    }
+    cpAsyncWaitAll();
+    if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
+}
+
+// The streaming elastic stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.
+template <class Real, int DX, int DZ, int STAGE>
+__global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream2d(const __grid_constant__ StageArgs<Real> p) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    if (p.clock->faulted) return; // uniform across the grid
+    Real *ring = reinterpret_cast<Real *>(smemRaw);
+    Real *pw = ring + RING * RS;
+    if constexpr (sizeof(Real) == 4) streamBody<Real, DX, DZ, STAGE, true>(p, ring, pw);
+    else if (p.m.hinvExact) streamBody<Real, DX, DZ, STAGE, true>(p, ring, pw);
+    else streamBody<Real, DX, DZ, STAGE, false>(p, ring, pw);
 }
 
 // ---------------------------------------------------------------- diagnostics ------------
