@@ -134,7 +134,10 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     bool cpml_{};
     std::vector<DeviceBuffer> model_;
     DeviceBuffer sets_, psets_, recIdx_, traces_, forcing_, clock_, partials_;
-    Real *set_[4]{}, *pset_[4]{};
+    // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
+    // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
+    static constexpr int kSets = k2::kahan<Real>() ? 6 : 4;
+    Real *set_[6]{}, *pset_[6]{};
     int u_{0}, a_{1};       // state / accumulator roles among set 0 and 1
     bool previous_{false};  // set a_ holds the state before the last step
     int nrec_{}, traceCap_{}, forcingCap_{};
@@ -183,6 +186,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         p.weight = stage == 2 ? static_cast<Real>(dt_) : static_cast<Real>(dt_ / 2);
         p.delta = static_cast<Real>(dt_);
         p.partials = nullptr;
+        if (k2::kahan<Real>()) p.cin = set_[4 + u_], p.cout = set_[4 + a_], p.pcin = pset_[4 + u_], p.pcout = pset_[4 + a_];
         return p;
     }
     double dt_{};
@@ -212,8 +216,9 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // and the GSLS strengths) plus 17 values per CFS-PML memory.
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.nz - 6);
-        const double F = fc_ * s, M = (5 + 2 * mech_) * s;
-        return points * (17 * F + 4 * M) + double(pcount_) * 17 * s;
+        // FP32 adds the read and write of the compensation terms in stage 3: 19 F + 4 M
+        const double F = fc_ * s, M = (5 + 2 * mech_) * s, words = k2::kahan<Real>() ? 19 : 17;
+        return points * (words * F + 4 * M) + double(pcount_) * words * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -347,10 +352,10 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             m_.dS[l] = arr(g.delta_s[l], n, "delta_s");
         }
         m_.fc = fc_;
-        sets_.allocate(4 * std::size_t(fc_) * n * sizeof(Real));
-        for (int s = 0; s < 4; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * fc_ * n;
-        psets_.allocate(4 * std::size_t(std::max<long long>(pcount_, 1)) * sizeof(Real));
-        for (int s = 0; s < 4; ++s) pset_[s] = psets_.as<Real>() + std::size_t(s) * std::max<long long>(pcount_, 1);
+        sets_.allocate(kSets * std::size_t(fc_) * n * sizeof(Real));
+        for (int s = 0; s < kSets; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * fc_ * n;
+        psets_.allocate(kSets * std::size_t(std::max<long long>(pcount_, 1)) * sizeof(Real));
+        for (int s = 0; s < kSets; ++s) pset_[s] = psets_.as<Real>() + std::size_t(s) * std::max<long long>(pcount_, 1);
         std::vector<long long> idx(nrec);
         for (int r = 0; r < nrec; ++r) {
             if (rec[r] < 0 || rec[r] >= g.count) throw Error(SWL_ERR_INVALID, "receiver node outside the padded grid");
@@ -625,6 +630,10 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         else throw Error(SWL_ERR_INVALID, "load field out of range");
         std::vector<Real> tmp(in, in + len);
         if (len) check(cudaMemcpy(dst, tmp.data(), len * sizeof(Real), cudaMemcpyHostToDevice), "field upload");
+        if (k2::kahan<Real>() && len) { // a loaded value starts without a compensation term
+            Real *comp = field == -1 ? pset_[4 + u_] : set_[4 + u_] + std::size_t(field) * count_;
+            check(cudaMemset(comp, 0, len * sizeof(Real)), "clear compensation");
+        }
         previous_ = false;
     }
     void probes(const int64_t *nodes, int n, double *out5) override {

@@ -70,7 +70,10 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     long long count_{};
     std::vector<DeviceBuffer> model_;
     DeviceBuffer sets_, recIdx_, traces_, forcing_, clock_, partials_, surfRate_;
-    Real *set_[4]{};
+    // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
+    // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
+    static constexpr int kSets = k2::kahan<Real>() ? 6 : 4;
+    Real *set_[6]{};
     int u_{0}, a_{1};
     bool previous_{false};
     int nrec_{}, traceCap_{}, forcingCap_{};
@@ -127,6 +130,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         p.w6 = static_cast<Real>(dt_ / 6.0);
         p.w3 = static_cast<Real>(dt_ / 3.0);
         p.surfRate = surfRate_.as<double>();
+        if (k2::kahan<Real>()) p.cin = set_[4 + u_], p.cout = set_[4 + a_];
         return p;
     }
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
@@ -151,11 +155,12 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     }
     // Algorithmic HBM bytes of the four stage kernels of one step: 16 F + 4 M per physical node
     // (the accumulator carries the partial state sum, so the last stage does not read U); M =
-    // nine metrics plus lambda, mu, rho when the material varies.
+    // nine metrics plus lambda, mu, rho when the material varies.  FP32 reads U and reads and
+    // writes the compensation terms in the last stage: 19 F + 4 M.
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
         const double F = 9 * s, M = (m_.mlambda ? 12 : 9) * s;
-        return points * (16 * F + 4 * M);
+        return points * ((k2::kahan<Real>() ? 19 : 16) * F + 4 * M);
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -278,8 +283,8 @@ template <class Real> class TypedEngine3D final : public Engine3D {
                         }
             if (ok) m_.dmp_i0 = i0, m_.dmp_i1 = i1, m_.dmp_j0 = j0, m_.dmp_j1 = j1, m_.dmp_k1 = kk >= g.nz - 3 ? g.nz : kk;
         }
-        sets_.allocate(4 * 9 * n * sizeof(Real));
-        for (int s = 0; s < 4; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * 9 * n;
+        sets_.allocate(kSets * 9 * n * sizeof(Real));
+        for (int s = 0; s < kSets; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * 9 * n;
         surfRate_.allocate(2 * std::size_t(m_.plane) * sizeof(double));
         std::vector<long long> idx(nrec);
         for (int r = 0; r < nrec; ++r) {
@@ -530,6 +535,8 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         std::vector<Real> tmp(in, in + count_);
         check(cudaMemcpy(set_[u_] + std::size_t(field) * count_, tmp.data(), count_ * sizeof(Real), cudaMemcpyHostToDevice),
               "field upload");
+        if (k2::kahan<Real>()) // a loaded value starts without a compensation term
+            check(cudaMemset(set_[4 + u_] + std::size_t(field) * count_, 0, count_ * sizeof(Real)), "clear compensation");
         previous_ = false;
     }
     int64_t residentBytes() const override {

@@ -152,8 +152,9 @@ struct Session2D {
     }
     bool completed() const { return step >= model.total; }
     int64_t estimateBytes() const {
-        const double s = params.precision == SWL_FP32 ? 4 : 8, n = double(model.nx) * model.nz;
-        return int64_t(n * s * (4 * model.fieldCount + 12 + 2 * model.mechanisms) + 4 * s * model.cpmlCount) + (64 << 20);
+        // four state sets, six in FP32 (the Kahan compensation of the state and accumulator)
+        const double s = params.precision == SWL_FP32 ? 4 : 8, n = double(model.nx) * model.nz, sets = s == 4 ? 6 : 4;
+        return int64_t(n * s * (sets * model.fieldCount + 12 + 2 * model.mechanisms) + sets * s * model.cpmlCount) + (64 << 20);
     }
     void reset() {
         if (engine) ok(swl2d_reset(engine)), ok(swl2d_diagnostics(engine, &diag));
@@ -312,7 +313,8 @@ struct Session3D {
     bool completed() const { return step >= model.total; }
     int64_t estimateBytes() const {
         const double s = params.precision == SWL_FP32 ? 4 : 8, n = double(model.nx) * model.ny * model.nz;
-        return int64_t(n * s * (36 + 9 + 2 + (model.materialLambda.empty() ? 0 : 3) + (model.sourceGradient[0].empty() ? 0 : 3))) + (64 << 20);
+        const double fields = (s == 4 ? 6 : 4) * 9; // state sets, with the FP32 compensation sets
+        return int64_t(n * s * (fields + 9 + 2 + (model.materialLambda.empty() ? 0 : 3) + (model.sourceGradient[0].empty() ? 0 : 3))) + (64 << 20);
     }
     void reset() {
         if (engine) ok(swl3d_reset(engine)), ok(swl3d_diagnostics(engine, &diag));

@@ -74,12 +74,22 @@ template <class Real> struct StageArgs {
     Real *pout;
     const Real *pbase;
     Real *pacc;
+    // FP32 only: Kahan compensation of U (read) and of the new state (written by stage 3),
+    // for the fields and for the CFS-PML memories
+    const Real *cin;
+    Real *cout;
+    const Real *pcin;
+    Real *pcout;
     const Real *forcing; // 3 values per step of the batch: t, t+dt/2, t+dt
     const Clock *clock;
     Real weight;         // dt/2, dt/2, dt for stages 0..2
     Real delta;          // dt
     Partial *partials;   // stage 3: per-CTA diagnostics of the new state (null: none)
 };
+
+// The FP32 form adds each step's increment to the state with compensated (Kahan) summation;
+// the FP64 form keeps the reference's plain sum.
+template <class Real> constexpr bool kahan() { return sizeof(Real) == 4; }
 
 template <class Real> __device__ __forceinline__ Real ld(const Real *p) { return __ldg(p); }
 
@@ -152,6 +162,7 @@ template <class Real, bool EXACT> struct TileNode {
     __device__ __forceinline__ Real at(int f, int dx, int dz) const { return c[f * (HZ * HX) + dz * HX + dx]; }
     __device__ __forceinline__ Real u(const StageArgs<Real> &p, int f) const { return stage0 ? at(f, 0, 0) : ld(p.base + f * n + q); }
     __device__ __forceinline__ Real acc(const StageArgs<Real> &p, int f) const { return p.acc[f * n + q]; }
+    __device__ __forceinline__ Real comp(const StageArgs<Real> &p, int f) const { return p.cin[f * n + q]; }
     __device__ __forceinline__ Real a(const Mesh<Real> &m) const { return ld(m.a + q); }
     __device__ __forceinline__ Real b(const Mesh<Real> &m) const { return ld(m.b + q); }
     __device__ __forceinline__ Real lam(const Mesh<Real> &m) const { return ld(m.lambda + q); }
@@ -164,10 +175,12 @@ template <class Real, bool EXACT> struct TileNode {
 // node rows, and walks down the segment one block of SB rows (one row per warp) at a time.
 // Shared memory holds a ring of RING stencil rows (five fields, SW + 6 columns each) and two
 // buffers of the per-node words of a row block.
-constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, RING = 3 * SB, RC = 40, RS = 5 * RC, PW = 16;
+constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, RING = 3 * SB, RC = 40, RS = 5 * RC;
 constexpr int STREAM_THREADS = SW * SB;
-enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15 };
-template <class Real> constexpr std::size_t streamBytes() { return sizeof(Real) * (RING * RS + 2 * PW * STREAM_THREADS); }
+enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15, PW_C = 16 };
+// per-node words: U, A, five model words and J, plus the five compensation terms in FP32
+template <class Real> constexpr int pwWords() { return kahan<Real>() ? PW_C + 5 : PW_C; }
+template <class Real> constexpr std::size_t streamBytes() { return sizeof(Real) * (RING * RS + 2 * pwWords<Real>() * STREAM_THREADS); }
 
 template <class Real, bool EXACT, int STAGE> struct StreamNode {
     static constexpr bool exact = EXACT;
@@ -183,6 +196,7 @@ template <class Real, bool EXACT, int STAGE> struct StreamNode {
     __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
     __device__ __forceinline__ Real u(const StageArgs<Real> &, int f) const { return STAGE == 0 ? at(f, 0, 0) : word(PW_U + f); }
     __device__ __forceinline__ Real acc(const StageArgs<Real> &, int f) const { return word(PW_A + f); }
+    __device__ __forceinline__ Real comp(const StageArgs<Real> &, int f) const { return word(PW_C + f); }
     __device__ __forceinline__ Real a(const Mesh<Real> &) const { return word(PW_a); }
     __device__ __forceinline__ Real b(const Mesh<Real> &) const { return word(PW_b); }
     __device__ __forceinline__ Real lam(const Mesh<Real> &) const { return word(PW_lam); }
@@ -300,8 +314,10 @@ __device__ __forceinline__ void cpAsyncWaitPrior() { asm volatile("cp.async.wait
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
 // `acc` is the node's A (unused in stage 0); `accOut` receives the new A (stages 0-2).
+// FP32 stage 3 adds the increment d = dt (A + k) / 6 to U by Kahan's compensated summation
+// (y = d - c, t = U + y, c' = (t - U) - y): `cin` is c and `accOut` receives c'.
 template <class Real, int STAGE>
-__device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real acc, Real u, Real r, Real &accOut) {
+__device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real acc, Real u, Real r, Real cin, Real &accOut) {
     if (STAGE == 0) {
         accOut = r;
         return u + p.weight * r;
@@ -309,10 +325,17 @@ __device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real acc, Real
         accOut = acc + 2 * r;
         return u + p.weight * r;
     }
+    if constexpr (kahan<Real>()) {
+        const Real y = p.delta * (acc + r) / Real(6) - cin;
+        const Real t = u + y;
+        accOut = (t - u) - y;
+        return t;
+    }
     accOut = Real(0);
     return u + p.delta * (acc + r) / Real(6);
 }
-// Stages 0-2 write A and the stage output; stage 3 writes the new state over A.
+// Stages 0-2 write A and the stage output; stage 3 writes the new state over A (and, in FP32,
+// its compensation term).
 template <class Real, int STAGE>
 __device__ __forceinline__ void store(const StageArgs<Real> &p, long long at, Real out, Real accOut) {
     if (STAGE < 3) {
@@ -320,6 +343,7 @@ __device__ __forceinline__ void store(const StageArgs<Real> &p, long long at, Re
         p.out[at] = out;
     } else {
         p.acc[at] = out;
+        if constexpr (kahan<Real>()) p.cout[at] = accOut;
     }
 }
 // ADE memory update of one slot value (same scheme as the fields).
@@ -333,7 +357,14 @@ __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long lon
         p.pacc[at] = p.pacc[at] + 2 * rate;
         p.pout[at] = u + p.weight * rate;
     } else {
-        const Real v = u + p.delta * (p.pacc[at] + rate) / Real(6);
+        Real v;
+        if constexpr (kahan<Real>()) {
+            const Real y = p.delta * (p.pacc[at] + rate) / Real(6) - p.pcin[at];
+            v = u + y;
+            p.pcout[at] = (v - u) - y;
+        } else {
+            v = u + p.delta * (p.pacc[at] + rate) / Real(6);
+        }
         p.pacc[at] = v;
         if (withDiag && !isfinite(v)) diag.bad = 1;
     }
@@ -344,14 +375,17 @@ __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long lon
 // rates -> combine/store of the velocities.  Every expression keeps the reference's operation
 // order (src/two_d/PointKernels2D.hpp:121-172); only independent computations are reordered.
 // GSLS memory fields (index >= 5) are read and written in global memory directly.
-template <class Real, int DX, int DZ, int MECH, int STAGE, class S>
+// FULL = false compiles the interior form: the caller guarantees that the node lies outside the
+// CFS-PML strips, the sponge, the source support and the four surface rows.
+template <class Real, int DX, int DZ, int MECH, int STAGE, bool FULL, class S>
 __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, int i, int k, Partial &diag, bool withDiag) {
     const Mesh<Real> &m = p.m;
-    const bool CPML = m.wz > 0;
+    constexpr bool KAHAN3 = STAGE == 3 && kahan<Real>();
+    const bool CPML = FULL && m.wz > 0;
     const long long n = m.count, q = t.q;
-    const int depth = k - 3;
+    const int depth = FULL ? k - 3 : 4; // any depth past the near-surface rows
     const Real *__restrict__ w = p.in;
-    const bool damped = !(i >= m.dmp_i0 && i < m.dmp_i1 && k < m.dmp_k1);
+    const bool damped = FULL && !(i >= m.dmp_i0 && i < m.dmp_i1 && k < m.dmp_k1);
     const Real damp = damped ? ld(m.damping + q) : Real(0);
 
     // CFS-PML slots of this node (src/two_d/PointKernels2D.hpp:50-56)
@@ -431,7 +465,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 if (damped) rm -= damp * wm[f];
                 const long long at = (mm + f) * n + q;
                 Real an;
-                const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), rm, an);
+                const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), rm, KAHAN3 ? p.cin[at] : Real(0), an);
                 store<Real, STAGE>(p, at, o, an);
                 if (withDiag && !isfinite(o)) diag.bad = 1;
             }
@@ -439,7 +473,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         if (damped) r5 -= damp * ld(w + 5 * n + q);
         const long long at = 5 * n + q;
         Real an;
-        const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), r5, an);
+        const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), r5, KAHAN3 ? p.cin[at] : Real(0), an);
         store<Real, STAGE>(p, at, o, an);
         if (withDiag && !isfinite(o)) diag.bad = 1;
     }
@@ -449,9 +483,9 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         r4 -= damp * t.at(4, 0, 0);
     }
     Real a2, a3, a4;
-    Real o2 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 2) : Real(0), t.u(p, 2), r2, a2);
-    Real o3 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 3) : Real(0), t.u(p, 3), r3, a3);
-    Real o4 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 4) : Real(0), t.u(p, 4), r4, a4);
+    Real o2 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 2) : Real(0), t.u(p, 2), r2, KAHAN3 ? t.comp(p, 2) : Real(0), a2);
+    Real o3 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 3) : Real(0), t.u(p, 3), r3, KAHAN3 ? t.comp(p, 3) : Real(0), a3);
+    Real o4 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 4) : Real(0), t.u(p, 4), r4, KAHAN3 ? t.comp(p, 4) : Real(0), a4);
     Real nx_ = 0, nz_ = 0;
     if (depth == 0) { // free-surface projection, PointKernels2D.hpp:70-78
         nx_ = ld(m.normals + 2 * q), nz_ = ld(m.normals + 2 * q + 1);
@@ -510,7 +544,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         if (slot1 >= 0)
             for (int v = 0; v < 2; ++v) combineMemory<Real, STAGE>(p, slot1 + 2 + v, mrate[2 + v], diag, withDiag);
     }
-    if (i >= m.src_i0 && i < m.src_i1 && k >= m.src_k0 && k < m.src_k1) {
+    if (FULL && i >= m.src_i0 && i < m.src_i1 && k >= m.src_k0 && k < m.src_k1) {
         const Clock *clk = p.clock;
         const Real forcing = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
         if (m.sgx) {
@@ -527,8 +561,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         r1 -= damp * t.at(1, 0, 0);
     }
     Real a0, a1;
-    const Real o0 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 0) : Real(0), t.u(p, 0), r0, a0);
-    const Real o1 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 1) : Real(0), t.u(p, 1), r1, a1);
+    const Real o0 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 0) : Real(0), t.u(p, 0), r0, KAHAN3 ? t.comp(p, 0) : Real(0), a0);
+    const Real o1 = combine<Real, STAGE>(p, STAGE ? t.acc(p, 1) : Real(0), t.u(p, 1), r1, KAHAN3 ? t.comp(p, 1) : Real(0), a1);
     store<Real, STAGE>(p, q, o0, a0);
     store<Real, STAGE>(p, n + q, o1, a1);
 
@@ -606,7 +640,7 @@ __device__ __forceinline__ void tileBody(const StageArgs<Real> &p, Real *tile) {
         const int i = i0 + threadIdx.x, k = k0 + lz;
         if (i < m.nx - 3 && k < m.nz - 3) {
             const TileNode<Real, EXACT> t{tile + (lz + 3) * HX + threadIdx.x + 3, i + (long long)m.nx * k, n, STAGE == 0};
-            stageNode<Real, DX, DZ, MECH, STAGE>(p, t, i, k, diag, withDiag);
+            stageNode<Real, DX, DZ, MECH, STAGE, true>(p, t, i, k, diag, withDiag);
         }
     }
     if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
@@ -629,11 +663,23 @@ __global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage
 // copies of block b+1 (its 8 new stencil rows and the U, A and model words of its 256 nodes)
 // are in flight; after block b it issues those of block b+2.  The evaluation therefore reads
 // shared memory only, and each thread keeps one block of copies in flight.
-template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 4; }
+// Resident CTAs per SM allowed by shared memory: 2 x 101.5 KB (FP64), 3 x 60.8 KB (FP32).
+template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 3; }
 
-template <class Real, int DX, int DZ, int STAGE, bool EXACT>
+// Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
+// strips, the sponge, the source support and the surface rows 3..6).
+template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<Real> &m, int i0, int z0) {
+    const int i1 = i0 + SW, z1 = z0 + SB * SEG_BLOCKS; // exclusive ends
+    const bool pml = i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || z1 - 3 > m.nz - 6 - m.wz;
+    const bool surface = z0 < 7;
+    const bool source = i0 < m.src_i1 && i1 > m.src_i0 && z0 < m.src_k1 && z1 > m.src_k0;
+    const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && z1 <= m.dmp_k1);
+    return !(pml || surface || source || sponge);
+}
+
+template <class Real, int DX, int DZ, int STAGE, bool EXACT, bool FULL>
 __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, Real *ring, Real *pw) {
-    constexpr int T = STREAM_THREADS;
+    constexpr int T = STREAM_THREADS, PW = pwWords<Real>();
     constexpr int bytes = int(sizeof(Real));
     const Mesh<Real> &m = p.m;
     const int lane = threadIdx.x, wy = threadIdx.y, tid = lane + SW * wy;
@@ -676,6 +722,9 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, Real *ring,
         cpAsync(dst + PW_mu * T, m.mu + q, bytes);
         cpAsync(dst + PW_rho * T, m.rho + q, bytes);
         if (STAGE == 3) cpAsync(dst + PW_jac * T, m.jac + q, bytes);
+        if (STAGE == 3 && kahan<Real>())
+#pragma unroll
+            for (int f = 0; f < 5; ++f) cpAsync(dst + (PW_C + f) * T, p.cin + f * n + q, bytes);
     };
     stageRows(0, SB + 6);
     stagePoint(0);
@@ -696,7 +745,7 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, Real *ring,
             s.q = i + nx * k;
             const int c = SB * (blk % 3) + wy + 3; // ring slot of row k (rel = SB*blk + wy + 3)
             s.centre = c >= RING ? c - RING : c;
-            stageNode<Real, DX, DZ, 0, STAGE>(p, s, i, k, diag, withDiag);
+            stageNode<Real, DX, DZ, 0, STAGE, FULL>(p, s, i, k, diag, withDiag);
         }
         __syncthreads(); // block blk's ring rows and buffer are free
         if (blk + 2 < blocks) stageRows(SB * (blk + 2) + 6, SB), stagePoint(blk + 2);
@@ -713,9 +762,17 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream
     if (p.clock->faulted) return; // uniform across the grid
     Real *ring = reinterpret_cast<Real *>(smemRaw);
     Real *pw = ring + RING * RS;
-    if constexpr (sizeof(Real) == 4) streamBody<Real, DX, DZ, STAGE, true>(p, ring, pw);
-    else if (p.m.hinvExact) streamBody<Real, DX, DZ, STAGE, true>(p, ring, pw);
-    else streamBody<Real, DX, DZ, STAGE, false>(p, ring, pw);
+    const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * SEG_BLOCKS));
+    if constexpr (sizeof(Real) == 4) {
+        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, true, true>(p, ring, pw);
+    } else if (p.m.hinvExact) {
+        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, true, true>(p, ring, pw);
+    } else {
+        if (interior) streamBody<Real, DX, DZ, STAGE, false, false>(p, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, false, true>(p, ring, pw);
+    }
 }
 
 // ---------------------------------------------------------------- diagnostics ------------

@@ -45,6 +45,8 @@ template <class Real> struct StageArgs {
     Real weight;         // stage combine weight: dt/2, dt/2, dt
     Real w6, w3;         // dt/6, dt/3
     double *surfRate;    // stage 3: |traction rate| and rate norm per surface node (2 x nx*ny)
+    const Real *cin;     // FP32 only: Kahan compensation of U (read) and of the new state (written)
+    Real *cout;
 };
 
 using k2::ld;
@@ -200,17 +202,26 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
         p.surfRate[sq] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
         p.surfRate[plane + sq] = sqrt(norm2);
     }
-    Real o[9];
+    // FP64: A = U + dt/6 k1, A += dt/3 k2, A += dt/3 k3, new = A + dt/6 k4 (the reference's
+    // order).  FP32: A accumulates the increment alone (A = dt/6 k1, ...), and stage 3 adds
+    // d = A + dt/6 k4 to U by Kahan's compensated summation (y = d - c, t = U + y,
+    // c' = (t - U) - y).
+    Real o[9], comp[9];
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
         if (STAGE == 0) {
             const Real u = ld(p.base + f * n + q);
-            p.acc[f * n + q] = u + p.w6 * r[f];
+            p.acc[f * n + q] = k2::kahan<Real>() ? p.w6 * r[f] : u + p.w6 * r[f];
             o[f] = u + p.weight * r[f];
         } else if (STAGE < 3) {
             const Real u = ld(p.base + f * n + q);
             p.acc[f * n + q] = p.acc[f * n + q] + p.w3 * r[f];
             o[f] = u + p.weight * r[f];
+        } else if constexpr (k2::kahan<Real>()) {
+            const Real u = ld(p.base + f * n + q);
+            const Real y = (p.acc[f * n + q] + p.w6 * r[f]) - p.cin[f * n + q];
+            o[f] = u + y;
+            comp[f] = (o[f] - u) - y;
         } else {
             o[f] = p.acc[f * n + q] + p.w6 * r[f];
         }
@@ -238,6 +249,9 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
     Real *dst = STAGE == 3 ? p.acc : p.out;
 #pragma unroll
     for (int f = 0; f < 9; ++f) dst[f * n + q] = o[f];
+    if (STAGE == 3 && k2::kahan<Real>())
+#pragma unroll
+        for (int f = 0; f < 9; ++f) p.cout[f * n + q] = comp[f];
 }
 
 struct Partial {

@@ -94,6 +94,23 @@ def test_rollback_restores_previous_step(swl):
     np.testing.assert_array_equal(e.fields(), before)
 
 
+@pytest.mark.parametrize("name", ["sponge_force", "cpml_external_moment_layers"])
+def test_fp32_rollback_restores_compensation(name, swl):
+    # FP32 keeps a Kahan compensation term per value beside the state; a rolled-back step must
+    # restore it with the state, so the run continues bit for bit as if the step never happened.
+    case, res, mesh = load_2d(name)
+    dt, f, s = float(res["dt"]), mesh["frequency"], mesh["scale"]
+    a = swl.Engine2D(mesh, receivers_2d(res), precision=swl.SWL_FP32)
+    a.advance(0, 12, dt, f, s)
+    a.advance(12, 1, dt, f, s)
+    a.rollback()
+    a.advance(12, 8, dt, f, s)
+    b = swl.Engine2D(mesh, receivers_2d(res), precision=swl.SWL_FP32)
+    b.advance(0, 20, dt, f, s)
+    np.testing.assert_array_equal(a.fields(), b.fields())
+    np.testing.assert_array_equal(a.field(-1), b.field(-1))
+
+
 def test_reset_clears_state(swl):
     case, res, mesh = load_2d("gsls3_cpml_surface_force")
     e = swl.Engine2D(mesh, receivers_2d(res))

@@ -54,6 +54,20 @@ def test_eager_step_matches_advance(swl):
     np.testing.assert_array_equal(a.fields(), b.fields())
 
 
+def test_fp32_rollback_restores_compensation(swl):
+    # the FP32 Kahan compensation terms roll back with the state
+    case, res, mesh = load_3d("moment_layered")
+    dt, f, g = float(res["dt"]), mesh["frequency"], 3.0 / mesh["frequency"]
+    a = swl.Engine3D(mesh, receivers_3d(res), precision=swl.SWL_FP32)
+    a.advance(0, 5, dt, f, g)
+    a.advance(5, 1, dt, f, g)
+    a.rollback()
+    a.advance(5, 4, dt, f, g)
+    b = swl.Engine3D(mesh, receivers_3d(res), precision=swl.SWL_FP32)
+    b.advance(0, 9, dt, f, g)
+    np.testing.assert_array_equal(a.fields(), b.fields())
+
+
 def test_diagnostics(swl):
     case, res, mesh = load_3d("force")
     e, _ = run(swl, mesh, res, swl.SWL_FP64)
