@@ -133,7 +133,12 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     long long count_{}, pcount_{};
     bool cpml_{};
     std::vector<DeviceBuffer> model_;
+    DeviceBuffer pack_; // a, b, lambda, mu, rho, J: six consecutive pitched arrays (one tensor map)
     DeviceBuffer sets_, psets_, recIdx_, traces_, forcing_, clock_, partials_;
+    int pitch_{}, nx_{}, nz_{};
+    // tensor maps of the streaming kernel: stage-input ring boxes of sets 0-3, word boxes of the
+    // state / accumulator sets 0-1 and of their compensation sets 4-5, model words without / with J
+    CUtensorMap ringMap_[4]{}, pwMap_[2]{}, compMap_[2]{}, modelMap_[2]{};
     // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
     // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
     static constexpr int kSets = k2::kahan<Real>() ? 6 : 4;
@@ -157,6 +162,16 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         if (inflight_) finish();
     }
 
+    // Memory offset of padded node q = i + nx k of the caller's layout.
+    long long memIndex(long long q) const { return q % nx_ + 1 + (long long)pitch_ * (q / nx_); }
+    // The caller's nx x nz layout (`per` values per node) in the pitched layout.
+    std::vector<Real> pitched(const std::vector<Real> &v, int per) const {
+        std::vector<Real> out(std::size_t(count_) * per, Real(0));
+        for (int k = 0; k < nz_; ++k)
+            std::copy(v.begin() + std::size_t(k) * nx_ * per, v.begin() + std::size_t(k + 1) * nx_ * per,
+                      out.begin() + (std::size_t(k) * pitch_ + 1) * per);
+        return out;
+    }
     Real *upload(const std::vector<Real> &v) {
         model_.emplace_back(v.size() * sizeof(Real));
         check(cudaMemcpy(model_.back().ptr, v.data(), v.size() * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
@@ -187,6 +202,14 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         p.delta = static_cast<Real>(dt_);
         p.partials = nullptr;
         if (k2::kahan<Real>()) p.cin = set_[4 + u_], p.cout = set_[4 + a_], p.pcin = pset_[4 + u_], p.pcout = pset_[4 + a_];
+        if (mech_ == 0) {
+            const int in = stage == 0 ? u_ : stage == 2 ? 3 : 2;
+            p.ringMap = ringMap_[in];
+            p.uMap = pwMap_[u_];
+            p.aMap = pwMap_[a_];
+            p.modelMap = modelMap_[stage == 3 ? 1 : 0];
+            p.compMap = compMap_[u_];
+        }
         return p;
     }
     double dt_{};
@@ -253,6 +276,13 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
         check(cudaStreamSynchronize(stream_), "2D batch completion");
         hostClock_ = *pinnedClock_.as<k2::Clock>();
+        checkStalled();
+    }
+    // A stage kernel whose bounded copy wait ran out flags the clock; report it as a CUDA error.
+    void checkStalled() {
+        if (!hostClock_.stalled) return;
+        hostClock_.stalled = 0;
+        throw Error(SWL_ERR_CUDA, "CUDA 2D stage: a tensor-copy wait ran out");
     }
 
   public:
@@ -265,18 +295,25 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
         check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "create stream");
         stream_ = ownStream_;
-        const std::size_t n = std::size_t(g.count);
-        count_ = g.count;
+        nx_ = g.nx, nz_ = g.nz;
+        pitch_ = (g.nx + 1 + 7) / 8 * 8;
+        count_ = (long long)pitch_ * g.nz;
+        const std::size_t n = std::size_t(count_), nu = std::size_t(g.count); // device and caller node counts
         mech_ = g.mechanisms;
         fc_ = g.field_count;
         nrec_ = nrec;
         const int ap = g.array_precision;
-        auto arr = [&](const void *src, std::size_t len, const char *name) {
+        auto arr = [&](const void *src, std::size_t len, const char *name) { // non-node arrays
             return upload(detail2::convert<Real>(src, len, ap, name));
+        };
+        auto node = [&](const void *src, int per, const char *name) { // per-node arrays, pitched
+            return upload(pitched(detail2::convert<Real>(src, nu * per, ap, name), per));
         };
         m_.nx = g.nx;
         m_.nz = g.nz;
-        m_.count = g.count;
+        m_.pitch = pitch_;
+        m_.xoff = 1;
+        m_.count = count_;
         m_.h = static_cast<Real>(g.h);
         {
             // x/h equals x*(1/h) bit for bit when h is a power of two; the FP32 form always
@@ -286,23 +323,29 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             m_.hinv = static_cast<Real>(1.0 / g.h);
             m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
         }
-        m_.a = arr(g.a, n, "a");
-        m_.b = arr(g.b, n, "b");
-        m_.jac = arr(g.jac, n, "jac");
-        m_.normals = arr(g.normals, 2 * n, "normals");
-        m_.lambda = arr(g.lambda, n, "lambda");
-        m_.mu = arr(g.mu, n, "mu");
-        m_.rho = arr(g.rho, n, "rho");
-        const auto damping = detail2::convert<Real>(g.damping, n, ap, "damping");
-        m_.damping = upload(damping);
-        const auto source = detail2::convert<Real>(g.source, n, ap, "source");
-        m_.source = upload(source);
+        {
+            pack_.allocate(6 * n * sizeof(Real));
+            const void *src[6] = {g.a, g.b, g.lambda, g.mu, g.rho, g.jac};
+            const char *names[6] = {"a", "b", "lambda", "mu", "rho", "jac"};
+            Real *dst[6];
+            for (int w = 0; w < 6; ++w) {
+                dst[w] = pack_.as<Real>() + w * n;
+                const auto v = pitched(detail2::convert<Real>(src[w], nu, ap, names[w]), 1);
+                check(cudaMemcpy(dst[w], v.data(), n * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
+            }
+            m_.a = dst[0], m_.b = dst[1], m_.lambda = dst[2], m_.mu = dst[3], m_.rho = dst[4], m_.jac = dst[5];
+        }
+        m_.normals = node(g.normals, 2, "normals");
+        const auto damping = detail2::convert<Real>(g.damping, nu, ap, "damping");
+        m_.damping = upload(pitched(damping, 1));
+        const auto source = detail2::convert<Real>(g.source, nu, ap, "source");
+        m_.source = upload(pitched(source, 1));
         std::vector<Real> sg[2];
         if (g.source_gradient[0] || g.source_gradient[1]) {
-            sg[0] = detail2::convert<Real>(g.source_gradient[0], n, ap, "source_gradient[0]");
-            sg[1] = detail2::convert<Real>(g.source_gradient[1], n, ap, "source_gradient[1]");
-            m_.sgx = upload(sg[0]);
-            m_.sgz = upload(sg[1]);
+            sg[0] = detail2::convert<Real>(g.source_gradient[0], nu, ap, "source_gradient[0]");
+            sg[1] = detail2::convert<Real>(g.source_gradient[1], nu, ap, "source_gradient[1]");
+            m_.sgx = upload(pitched(sg[0], 1));
+            m_.sgz = upload(pitched(sg[1], 1));
         }
         m_.sdx = static_cast<Real>(g.source_direction[0]);
         m_.sdz = static_cast<Real>(g.source_direction[2]);
@@ -348,8 +391,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         }
         for (int l = 0; l < mech_; ++l) {
             m_.rates[l] = static_cast<Real>(g.rates[l]);
-            m_.dP[l] = arr(g.delta_p[l], n, "delta_p");
-            m_.dS[l] = arr(g.delta_s[l], n, "delta_s");
+            m_.dP[l] = node(g.delta_p[l], 1, "delta_p");
+            m_.dS[l] = node(g.delta_s[l], 1, "delta_s");
         }
         m_.fc = fc_;
         sets_.allocate(kSets * std::size_t(fc_) * n * sizeof(Real));
@@ -359,7 +402,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         std::vector<long long> idx(nrec);
         for (int r = 0; r < nrec; ++r) {
             if (rec[r] < 0 || rec[r] >= g.count) throw Error(SWL_ERR_INVALID, "receiver node outside the padded grid");
-            idx[r] = rec[r];
+            idx[r] = memIndex(rec[r]);
         }
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
@@ -371,6 +414,18 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         nparts_ = grid_.x * grid_.y;
         partials_.allocate(std::max<std::size_t>(nparts_, stageGrid_.x * stageGrid_.y) * sizeof(k2::Partial));
         detail2::Launch<Real>::prepare(mech_);
+        if (mech_ == 0) {
+            const bool f64 = sizeof(Real) == 8;
+            const uint64_t d5[3] = {uint64_t(pitch_), uint64_t(nz_), 5}, d6[3] = {uint64_t(pitch_), uint64_t(nz_), 6};
+            const uint64_t st[2] = {uint64_t(pitch_) * sizeof(Real), uint64_t(n) * sizeof(Real)};
+            const uint32_t ring[3] = {k2::RC, k2::SB, 5}, w5[3] = {k2::SW, k2::SB, 5}, w6[3] = {k2::SW, k2::SB, 6};
+            for (int s = 0; s < 4; ++s) encodeTensorMap3D(&ringMap_[s], f64, set_[s], d5, st, ring);
+            for (int r = 0; r < 2; ++r) encodeTensorMap3D(&pwMap_[r], f64, set_[r], d5, st, w5);
+            if (k2::kahan<Real>())
+                for (int r = 0; r < 2; ++r) encodeTensorMap3D(&compMap_[r], f64, set_[4 + r], d5, st, w5);
+            encodeTensorMap3D(&modelMap_[0], f64, pack_.ptr, d6, st, w5);
+            encodeTensorMap3D(&modelMap_[1], f64, pack_.ptr, d6, st, w6);
+        }
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
@@ -461,6 +516,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         previous_ = accepted > 0;
         faulted_ = hostClock_.faulted != 0;
         inflight_ = false;
+        checkStalled();
     }
     int finish() override {
         if (!inflight_) return hostClock_.accepted;
@@ -617,7 +673,12 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         else throw Error(SWL_ERR_INVALID, "snapshot field out of range");
         std::vector<Real> tmp(len);
         if (len) check(cudaMemcpy(tmp.data(), src, len * sizeof(Real), cudaMemcpyDeviceToHost), "snapshot download");
-        for (std::size_t i = 0; i < len; ++i) out[i] = double(tmp[i]);
+        if (field == -1) {
+            for (std::size_t i = 0; i < len; ++i) out[i] = double(tmp[i]);
+        } else { // pitched rows -> the caller's nx x nz layout
+            for (int k = 0; k < nz_; ++k)
+                for (int i = 0; i < nx_; ++i) out[std::size_t(k) * nx_ + i] = double(tmp[std::size_t(k) * pitch_ + 1 + i]);
+        }
     }
     void load(int field, const double *in) override {
         settle();
@@ -628,7 +689,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         if (field == -1) dst = pset_[u_], len = std::size_t(pcount_);
         else if (field >= 0 && field < fc_) dst = set_[u_] + std::size_t(field) * count_, len = std::size_t(count_);
         else throw Error(SWL_ERR_INVALID, "load field out of range");
-        std::vector<Real> tmp(in, in + len);
+        std::vector<Real> tmp = field == -1 ? std::vector<Real>(in, in + len)
+                                            : pitched(std::vector<Real>(in, in + std::size_t(nx_) * nz_), 1);
         if (len) check(cudaMemcpy(dst, tmp.data(), len * sizeof(Real), cudaMemcpyHostToDevice), "field upload");
         if (k2::kahan<Real>() && len) { // a loaded value starts without a compensation term
             Real *comp = field == -1 ? pset_[4 + u_] : set_[4 + u_] + std::size_t(field) * count_;
@@ -639,12 +701,17 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     void probes(const int64_t *nodes, int n, double *out5) override {
         settle();
         DeviceScope scope(device_);
-        gather(nodes, n, 5, out5);
+        std::vector<int64_t> idx(nodes, nodes + std::max(n, 0));
+        for (auto &q : idx) {
+            if (q < 0 || q >= (long long)nx_ * nz_) throw Error(SWL_ERR_INVALID, "probe node outside the padded grid");
+            q = memIndex(q);
+        }
+        gather(idx.data(), n, 5, out5);
     }
     int64_t residentBytes() const override {
         int64_t b = 0;
         for (const auto &x : model_) b += x.bytes;
-        for (const auto *x : {&sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_}) b += x->bytes;
+        for (const auto *x : {&pack_, &sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_}) b += x->bytes;
         return b;
     }
 };

@@ -3,6 +3,7 @@
 // into a status, cf. src/common/CudaSupport.cuh:5-8), device selection scope and RAII
 // device/pinned buffers.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -111,5 +112,12 @@ inline int direction(int step, int stage, int axis) {
 
 // Ricker wavelet of src/two_d/CurvilinearSolver2D.cpp:31-34.
 double ricker(double t, double f);
+
+// A 3D tiled tensor map (no swizzle, zero fill outside the tensor) over `base`: dims[0] is the
+// contiguous axis; strides are the byte strides of dims 1 and 2 (multiples of 16); box[0] *
+// element size must be a multiple of 16 bytes.  The driver's encoder is reached through the
+// runtime's entry-point query, so the library does not link libcuda.
+void encodeTensorMap3D(CUtensorMap *map, bool fp64, const void *base, const uint64_t dims[3], const uint64_t strides[2],
+                       const uint32_t box[3]);
 
 } // namespace swl

@@ -20,14 +20,19 @@
 #pragma once
 #include "runtime.cuh"
 #include <cstdint>
+#include <cuda.h>
 
 namespace swl::k2 {
 
 // Device view of the model (Point::MeshT, src/two_d/PointKernels2D.hpp:14-27), plus the
 // boxes outside which the sparse source and sponge arrays are exactly zero.
+// Arrays are stored with a row pitch: node (i, k) of the padded nx x nz grid lives at
+// i + xoff + pitch * k, with pitch a multiple of 8 >= nx + 1 and xoff = 1, so that every row
+// and every 32-column strip starts on a 16-byte boundary (the alignment tensor copies need).
 template <class Real> struct Mesh {
     int nx, nz; // padded
-    long long count;
+    int pitch, xoff;
+    long long count; // pitch * nz: the stride between fields
     Real h, hinv;   // hinv = 1/h, used only when it is exact (h a power of two) or in FP32
     int hinvExact;
     const Real *a, *b, *jac, *normals, *lambda, *mu, *rho, *damping, *source, *sgx, *sgz;
@@ -50,7 +55,7 @@ struct Clock {
     int faulted;     // set by the verdict on a rejected step
     int fault_step;  // the rejected step
     int trace_steps; // capacity of the trace table in steps
-    int pad;
+    int stalled;     // set by a stage kernel whose copy wait ran out (the host reports an error)
     double peak_energy;
     double energy, max_velocity, traction;
     int finite;
@@ -85,6 +90,10 @@ template <class Real> struct StageArgs {
     Real weight;         // dt/2, dt/2, dt for stages 0..2
     Real delta;          // dt
     Partial *partials;   // stage 3: per-CTA diagnostics of the new state (null: none)
+    // Tensor maps of the streaming kernel (elastic only): the stage input as 40x8x5 boxes,
+    // U, A and the compensation terms as 32x8x5 boxes, the model words as 32x8x5 (stages 0-2) or
+    // 32x8x6 (stage 3, with J) boxes.
+    CUtensorMap ringMap, uMap, aMap, modelMap, compMap;
 };
 
 // The FP32 form adds each step's increment to the state with compensated (Kahan) summation;
@@ -173,25 +182,30 @@ template <class Real, bool EXACT> struct TileNode {
 
 // Streaming geometry: a CTA owns a strip of SW node columns and a segment of SB*SEG_BLOCKS
 // node rows, and walks down the segment one block of SB rows (one row per warp) at a time.
-// Shared memory holds a ring of RING stencil rows (five fields, SW + 6 columns each) and two
-// buffers of the per-node words of a row block.
-constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, RING = 3 * SB, RC = 40, RS = 5 * RC;
-constexpr int STREAM_THREADS = SW * SB;
+// Shared memory holds a ring of three chunks of SB stencil rows (five fields, SW + 8 columns:
+// the strip and four columns either side) and two buffers of the per-node words of a row block.
+// Both are filled by tensor copies, so their layout is the copy box: [chunk][field][row][column]
+// and [word][row][column].
+constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, CHUNKS = 3, RC = SW + 8, RF = SB * RC, CH = 5 * RF;
+constexpr int RING = CHUNKS * SB, STREAM_THREADS = SW * SB;
 enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15, PW_C = 16 };
 // per-node words: U, A, five model words and J, plus the five compensation terms in FP32
 template <class Real> constexpr int pwWords() { return kahan<Real>() ? PW_C + 5 : PW_C; }
-template <class Real> constexpr std::size_t streamBytes() { return sizeof(Real) * (RING * RS + 2 * pwWords<Real>() * STREAM_THREADS); }
+// two mbarriers, then the ring and the two word buffers (128-byte aligned), plus alignment slack
+template <class Real> constexpr std::size_t streamBytes() {
+    return 128 + sizeof(Real) * (CHUNKS * CH + 2 * pwWords<Real>() * STREAM_THREADS) + 128;
+}
 
 template <class Real, bool EXACT, int STAGE> struct StreamNode {
     static constexpr bool exact = EXACT;
-    const Real *col; // ring slot 0, field 0, this node's column
+    const Real *col; // ring chunk 0, field 0, row 0, this node's column
     const Real *pw;  // this node's per-node words (stride STREAM_THREADS)
     long long q;
-    int centre;      // ring slot of this node's row
+    int centre;      // ring row (0..RING-1) of this node
     __device__ __forceinline__ Real at(int f, int dx, int dz) const {
         int s = centre + dz;
         s = s < 0 ? s + RING : s >= RING ? s - RING : s;
-        return col[s * RS + f * RC + dx];
+        return col[(s / SB) * CH + f * RF + (s % SB) * RC + dx];
     }
     __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
     __device__ __forceinline__ Real u(const StageArgs<Real> &, int f) const { return STAGE == 0 ? at(f, 0, 0) : word(PW_U + f); }
@@ -259,7 +273,7 @@ template <class Real, int DIR, class S> __device__ __forceinline__ Real tnear3(c
 // Traction flux J (x sigma_a + z sigma_b) at the tap (dx, dz) (PointKernels2D.hpp:90-93).
 template <class Real, class S>
 __device__ __forceinline__ Real flux(const Mesh<Real> &m, const S &t, int dx, int dz, int axis, int comp) {
-    const long long qq = t.q + dx + (long long)dz * m.nx;
+    const long long qq = t.q + dx + (long long)dz * m.pitch;
     const Real x = axis ? ld(m.a + qq) : Real(1), z = axis ? ld(m.b + qq) : Real(0);
     return ld(m.jac + qq) * (x * t.at(comp ? 4 : 2, dx, dz) + z * t.at(comp ? 3 : 4, dx, dz));
 }
@@ -309,7 +323,6 @@ __device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes)
 }
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitPrior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
@@ -627,7 +640,7 @@ __device__ __forceinline__ void tileBody(const StageArgs<Real> &p, Real *tile) {
     for (int e = tid; e < 5 * HZ * HX; e += TILE_THREADS) {
         const int f = e / (HZ * HX), r = e - f * (HZ * HX), zz = r / HX, xx = r - zz * HX;
         const int gi = i0 - 3 + xx, gk = k0 - 3 + zz;
-        if (gi < m.nx && gk < m.nz) cpAsync(tile + e, p.in + f * n + gi + (long long)m.nx * gk, int(sizeof(Real)));
+        if (gi < m.nx && gk < m.nz) cpAsync(tile + e, p.in + f * n + gi + m.xoff + (long long)m.pitch * gk, int(sizeof(Real)));
     }
     cpAsyncCommit();
     cpAsyncWaitAll();
@@ -639,7 +652,7 @@ __device__ __forceinline__ void tileBody(const StageArgs<Real> &p, Real *tile) {
         const int lz = threadIdx.y + (TILE_THREADS / TX) * j;
         const int i = i0 + threadIdx.x, k = k0 + lz;
         if (i < m.nx - 3 && k < m.nz - 3) {
-            const TileNode<Real, EXACT> t{tile + (lz + 3) * HX + threadIdx.x + 3, i + (long long)m.nx * k, n, STAGE == 0};
+            const TileNode<Real, EXACT> t{tile + (lz + 3) * HX + threadIdx.x + 3, i + m.xoff + (long long)m.pitch * k, n, STAGE == 0};
             stageNode<Real, DX, DZ, MECH, STAGE, true>(p, t, i, k, diag, withDiag);
         }
     }
@@ -659,11 +672,41 @@ __global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage
 }
 
 // ------------------------------------------------------------- streaming stage (elastic)
-// A CTA walks its strip down one block of 8 rows at a time.  While it evaluates block b, the
-// copies of block b+1 (its 8 new stencil rows and the U, A and model words of its 256 nodes)
-// are in flight; after block b it issues those of block b+2.  The evaluation therefore reads
-// shared memory only, and each thread keeps one block of copies in flight.
-// Resident CTAs per SM allowed by shared memory: 2 x 101.5 KB (FP64), 3 x 60.8 KB (FP32).
+// A CTA walks its strip down one block of 8 rows at a time.  One thread issues tensor copies;
+// group g (ring chunk g + 1 -- chunks 0 and 1 for g = 0 -- and the U, A and model words of block
+// g) completes on mbarrier g & 1.  While the CTA evaluates block b from shared memory, group b+1
+// is in flight; after block b, group b+2 reuses the ring chunk and word buffer block b released.
+// Waits are bounded: a wait that runs out flags the clock (`stalled`) and the CTA stops.
+__device__ __forceinline__ unsigned smemAddr(const void *p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbarInit(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t *bar, unsigned parity) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smemAddr(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// Bounded wait for the phase of `parity`; false when the limit ran out.
+__device__ __forceinline__ bool mbarWait(uint64_t *bar, unsigned parity) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbarTryWait(bar, parity)) return true;
+    return false;
+}
+// 3D tiled tensor copy global -> shared (no multicast), completing on `bar`.
+__device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+                     smemAddr(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smemAddr(bar))
+                 : "memory");
+}
+
+// Resident CTAs per SM allowed by shared memory: 2 x 101.8 KB (FP64), 3 x 61 KB (FP32).
 template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 3; }
 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
@@ -678,80 +721,73 @@ template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<R
 }
 
 template <class Real, int DX, int DZ, int STAGE, bool EXACT, bool FULL>
-__device__ __forceinline__ void streamBody(const StageArgs<Real> &p, Real *ring, Real *pw) {
+__device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw) {
     constexpr int T = STREAM_THREADS, PW = pwWords<Real>();
-    constexpr int bytes = int(sizeof(Real));
+    constexpr unsigned S = sizeof(Real);
+    constexpr unsigned chunkBytes = S * CH, fiveBytes = S * 5 * T, modelBytes = S * (STAGE == 3 ? 6 : 5) * T;
+    constexpr unsigned wordBytes = (STAGE > 0 ? 2 * fiveBytes : 0) + modelBytes + (STAGE == 3 && kahan<Real>() ? fiveBytes : 0);
     const Mesh<Real> &m = p.m;
     const int lane = threadIdx.x, wy = threadIdx.y, tid = lane + SW * wy;
     const int i0 = 3 + blockIdx.x * SW, z0 = 3 + blockIdx.y * (SB * SEG_BLOCKS), zb = z0 - 3;
     const int iEnd = m.nx - 3, kEnd = m.nz - 3;
-    const long long n = m.count, nx = m.nx;
     const int blocks = min(SEG_BLOCKS, (kEnd - z0 + SB - 1) / SB);
-    const int gx = i0 - 3 + lane; // first staged column of this lane (and gx + 32 for lanes 0-5)
-    const bool colA = gx < m.nx, colB = lane < 6 && gx + 32 < m.nx;
-    // ring rows [rel0, rel0 + rows) relative to row zb; warp wy stages every SB-th row
-    auto stageRows = [&](int rel0, int rows) {
-        for (int r = wy; r < rows; r += SB) {
-            const int rel = rel0 + r, gk = zb + rel;
-            if (gk >= m.nz) break;
-            Real *dst = ring + (rel % RING) * RS + lane;
-            const Real *src = p.in + (long long)gk * nx + gx;
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                if (colA) cpAsync(dst + f * RC, src + f * n, bytes);
-                if (colB) cpAsync(dst + f * RC + 32, src + f * n + 32, bytes);
-            }
-        }
-    };
-    // per-node words of row block blk into buffer blk & 1
-    auto stagePoint = [&](int blk) {
-        const int k = z0 + blk * SB + wy, i = i0 + lane;
-        if (k >= kEnd || i >= iEnd) return;
-        const long long q = i + nx * k;
-        Real *dst = pw + (blk & 1) * (PW * T) + tid;
+    __shared__ int stop;
+    // thread 0: issue copy group g (x of the ring box: node i0 - 4; of the word boxes: node i0)
+    auto issue = [&](int g) {
+        uint64_t *b = bar + (g & 1);
+        const int c0 = g == 0 ? 0 : g + 1, c1 = g + 1;
+        mbarExpectTx(b, (c1 - c0 + 1) * chunkBytes + wordBytes);
+        for (int c = c0; c <= c1; ++c) tmaLoad3(ring + (c % CHUNKS) * CH, &p.ringMap, i0 - 4 + m.xoff, zb + SB * c, 0, b);
+        Real *dst = pw + (g & 1) * (PW * T);
+        const int x = i0 + m.xoff, y = z0 + SB * g;
         if (STAGE > 0) {
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                cpAsync(dst + (PW_U + f) * T, p.base + f * n + q, bytes);
-                cpAsync(dst + (PW_A + f) * T, p.acc + f * n + q, bytes);
-            }
+            tmaLoad3(dst + PW_U * T, &p.uMap, x, y, 0, b);
+            tmaLoad3(dst + PW_A * T, &p.aMap, x, y, 0, b);
         }
-        cpAsync(dst + PW_a * T, m.a + q, bytes);
-        cpAsync(dst + PW_b * T, m.b + q, bytes);
-        cpAsync(dst + PW_lam * T, m.lambda + q, bytes);
-        cpAsync(dst + PW_mu * T, m.mu + q, bytes);
-        cpAsync(dst + PW_rho * T, m.rho + q, bytes);
-        if (STAGE == 3) cpAsync(dst + PW_jac * T, m.jac + q, bytes);
-        if (STAGE == 3 && kahan<Real>())
-#pragma unroll
-            for (int f = 0; f < 5; ++f) cpAsync(dst + (PW_C + f) * T, p.cin + f * n + q, bytes);
+        tmaLoad3(dst + PW_a * T, &p.modelMap, x, y, 0, b);
+        if (STAGE == 3 && kahan<Real>()) tmaLoad3(dst + PW_C * T, &p.compMap, x, y, 0, b);
     };
-    stageRows(0, SB + 6);
-    stagePoint(0);
-    cpAsyncCommit();
-    if (blocks > 1) stageRows(SB + 6, SB), stagePoint(1);
-    cpAsyncCommit();
+    if (tid == 0) {
+        stop = 0;
+        mbarInit(bar, 1);
+        mbarInit(bar + 1, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        issue(0);
+        if (blocks > 1) issue(1);
+    }
     Partial diag{0, 0, 0, 0, 0};
     const bool withDiag = STAGE == 3 && p.partials != nullptr;
+    int waited = 0; // groups this CTA has seen complete
 #pragma unroll 1
     for (int blk = 0; blk < blocks; ++blk) {
-        cpAsyncWaitPrior(); // this block's group has landed (the next one may still fly)
+        if (!mbarWait(bar + (blk & 1), (blk >> 1) & 1)) stop = 1;
         __syncthreads();
+        if (stop) break;
+        waited = blk + 1;
         const int k = z0 + blk * SB + wy, i = i0 + lane;
         if (k < kEnd && i < iEnd) {
             StreamNode<Real, EXACT, STAGE> s;
-            s.col = ring + lane + 3;
+            s.col = ring + lane + 4;
             s.pw = pw + (blk & 1) * (PW * T) + tid;
-            s.q = i + nx * k;
-            const int c = SB * (blk % 3) + wy + 3; // ring slot of row k (rel = SB*blk + wy + 3)
+            s.q = i + m.xoff + (long long)m.pitch * k;
+            const int c = SB * (blk % 3) + wy + 3; // ring row of row k (rows counted from zb)
             s.centre = c >= RING ? c - RING : c;
             stageNode<Real, DX, DZ, 0, STAGE, FULL>(p, s, i, k, diag, withDiag);
         }
-        __syncthreads(); // block blk's ring rows and buffer are free
-        if (blk + 2 < blocks) stageRows(SB * (blk + 2) + 6, SB), stagePoint(blk + 2);
-        cpAsyncCommit();
+        __syncthreads(); // block blk's ring chunk and word buffer are free
+        if (tid == 0 && blk + 2 < blocks) issue(blk + 2);
     }
-    cpAsyncWaitAll();
+    if (stop) { // a copy wait ran out: flag it, let the copies still in flight land, and stop
+        if (tid == 0) {
+            atomicExch(const_cast<int *>(&p.clock->stalled), 1);
+            const int issued = min(blocks, waited + 2);
+            for (int g = waited; g < issued; ++g) mbarWait(bar + (g & 1), (g >> 1) & 1);
+        }
+        return;
+    }
     if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
 }
 
@@ -760,18 +796,20 @@ template <class Real, int DX, int DZ, int STAGE>
 __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream2d(const __grid_constant__ StageArgs<Real> p) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     if (p.clock->faulted) return; // uniform across the grid
-    Real *ring = reinterpret_cast<Real *>(smemRaw);
-    Real *pw = ring + RING * RS;
+    unsigned char *base = smemRaw + ((128 - (smemAddr(smemRaw) & 127)) & 127);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(base);
+    Real *ring = reinterpret_cast<Real *>(base + 128);
+    Real *pw = ring + CHUNKS * CH;
     const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * SEG_BLOCKS));
     if constexpr (sizeof(Real) == 4) {
-        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, true, true>(p, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, true, true>(p, bar, ring, pw);
     } else if (p.m.hinvExact) {
-        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, true, true>(p, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, true, true>(p, bar, ring, pw);
     } else {
-        if (interior) streamBody<Real, DX, DZ, STAGE, false, false>(p, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, false, true>(p, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, STAGE, false, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, STAGE, false, true>(p, bar, ring, pw);
     }
 }
 
@@ -788,7 +826,7 @@ __global__ void __launch_bounds__(256) stats2d(const Mesh<Real> m, const Real *_
     const int k = 3 + blockIdx.y * blockDim.y + threadIdx.y;
     Partial s{0, 0, 0, 0, 0};
     if (i < m.nx - 3 && k < m.nz - 3 && !(clk && clk->faulted)) {
-        const long long n = m.count, q = i + (long long)m.nx * k;
+        const long long n = m.count, q = i + m.xoff + (long long)m.pitch * k;
         for (int f = 0; f < m.fc; ++f)
             if (!isfinite(ld(w + f * n + q))) s.bad = 1;
         if (m.wx || m.wz) {
