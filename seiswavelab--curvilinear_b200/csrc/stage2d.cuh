@@ -324,6 +324,24 @@ __device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes)
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Correctly rounded y / 6 without a division instruction sequence.  y/6 = (y/2)/3 with y/2 exact,
+// and x/3 by Markstein's correction (P. W. Markstein, "Computation of elementary functions on the
+// IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with c = RN(1/3) -- here
+// 3c = 1 - 2^-54 (FP32: 1 + 2^-25), so q0 = RN(x c) is within one ulp of x/3 -- the remainder
+// r = x - 3 q0 is exact under an FMA and RN(q0 + r c) = RN(x/3).  The theorem excludes
+// underflow, so tiny, huge and non-finite x take the plain division.
+template <class Real> __device__ __forceinline__ Real div6(Real y) {
+    constexpr Real c = Real(1) / Real(3);
+    constexpr Real tiny = sizeof(Real) == 8 ? Real(0x1p-960) : Real(0x1p-100f);
+    constexpr Real huge = sizeof(Real) == 8 ? Real(0x1p+1000) : Real(0x1p+120f);
+    const Real x = y * Real(0.5);
+    const Real ax = fabs(x);
+    if (!(ax >= tiny && ax <= huge)) return y / Real(6);
+    const Real q0 = x * c;
+    const Real r = fma(-q0, Real(3), x);
+    return fma(r, c, q0);
+}
+
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
 // `acc` is the node's A (unused in stage 0); `accOut` receives the new A (stages 0-2).
@@ -339,13 +357,13 @@ __device__ __forceinline__ Real combine(const StageArgs<Real> &p, Real acc, Real
         return u + p.weight * r;
     }
     if constexpr (kahan<Real>()) {
-        const Real y = p.delta * (acc + r) / Real(6) - cin;
+        const Real y = div6(p.delta * (acc + r)) - cin;
         const Real t = u + y;
         accOut = (t - u) - y;
         return t;
     }
     accOut = Real(0);
-    return u + p.delta * (acc + r) / Real(6);
+    return u + div6(p.delta * (acc + r));
 }
 // Stages 0-2 write A and the stage output; stage 3 writes the new state over A (and, in FP32,
 // its compensation term).
@@ -372,11 +390,11 @@ __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long lon
     } else {
         Real v;
         if constexpr (kahan<Real>()) {
-            const Real y = p.delta * (p.pacc[at] + rate) / Real(6) - p.pcin[at];
+            const Real y = div6(p.delta * (p.pacc[at] + rate)) - p.pcin[at];
             v = u + y;
             p.pcout[at] = (v - u) - y;
         } else {
-            v = u + p.delta * (p.pacc[at] + rate) / Real(6);
+            v = u + div6(p.delta * (p.pacc[at] + rate));
         }
         p.pacc[at] = v;
         if (withDiag && !isfinite(v)) diag.bad = 1;
@@ -580,14 +598,14 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
     store<Real, STAGE>(p, n + q, o1, a1);
 
     if (STAGE == 3 && withDiag) { // energy, |v|^2, surface traction, finiteness (PointKernels2D.hpp:173-184)
-        if (!isfinite(o0) || !isfinite(o1) || !isfinite(o2) || !isfinite(o3) || !isfinite(o4)) diag.bad = 1;
+        diag.bad |= int(!isfinite(o0)) | int(!isfinite(o1)) | int(!isfinite(o2)) | int(!isfinite(o3)) | int(!isfinite(o4));
         const double l = lam, mu_ = mu, xx = o2, zz = o3, xz = o4, vx = o0, vz = o1;
         // (l+2m)(xx^2+zz^2) - 2 l xx zz over 8m(l+m), plus xz^2/(2m), over one division
         const double e = (.5 * double(rho) * (vx * vx + vz * vz) +
                           (((l + 2 * mu_) * (xx * xx + zz * zz) - 2 * l * xx * zz) + 4 * (l + mu_) * xz * xz) / (8 * mu_ * (l + mu_))) *
                          double(t.jac(m)) * double(m.h) * double(m.h);
         const double v2 = vx * vx + vz * vz;
-        if (!isfinite(e)) diag.bad = 1;
+        diag.bad |= int(!isfinite(e));
         diag.energy += e;
         diag.velocity = fmax(diag.velocity, v2); // squared; the root is taken once per CTA
         if (depth == 0) {
