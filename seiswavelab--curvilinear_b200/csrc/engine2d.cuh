@@ -320,6 +320,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             // multiplies by the reciprocal.
             int e2 = 0;
             const bool pow2 = g.h > 0 && std::frexp(g.h, &e2) == 0.5;
+            if (!(g.h >= 0x1p-20 && g.h <= 0x1p+20)) throw Error(SWL_ERR_INVALID, "2D grid spacing must lie in [2^-20, 2^20]");
             m_.hinv = static_cast<Real>(1.0 / g.h);
             m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
         }

@@ -220,6 +220,15 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         m_.count = g.count;
         m_.plane = (long long)g.nx * g.ny;
         m_.h = static_cast<Real>(g.h);
+        {
+            // x/h equals x*(1/h) bit for bit when h is a power of two; otherwise the kernels form
+            // the correctly rounded quotient from RN(1/h).  FP32 always multiplies.
+            if (!(g.h >= 0x1p-20 && g.h <= 0x1p+20)) throw Error(SWL_ERR_INVALID, "3D grid spacing must lie in [2^-20, 2^20]");
+            int e2 = 0;
+            const bool pow2 = std::frexp(g.h, &e2) == 0.5;
+            m_.hinv = static_cast<Real>(1.0 / g.h);
+            m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
+        }
         m_.lambda = static_cast<Real>(g.lambda), m_.mu = static_cast<Real>(g.mu), m_.density = static_cast<Real>(g.density);
         for (int c = 0; c < 9; ++c) m_.metric[c] = upload(conv(g.metrics, n, 9, c));
         m_.jac = upload(conv(g.jacobian, n));

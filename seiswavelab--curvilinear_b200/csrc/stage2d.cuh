@@ -33,8 +33,8 @@ template <class Real> struct Mesh {
     int nx, nz; // padded
     int pitch, xoff;
     long long count; // pitch * nz: the stride between fields
-    Real h, hinv;   // hinv = 1/h, used only when it is exact (h a power of two) or in FP32
-    int hinvExact;
+    Real h, hinv;   // hinv = RN(1/h); x/h is x*hinv when h is a power of two (or in FP32),
+    int hinvExact;  // else the correctly rounded divBy(x, h, hinv)
     const Real *a, *b, *jac, *normals, *lambda, *mu, *rho, *damping, *source, *sgx, *sgz;
     Real sdx, sdz;             // unit force direction (x, z)
     int src_i0, src_i1, src_k0, src_k1; // source support box [i0,i1) x [k0,k1), padded indices
@@ -102,54 +102,41 @@ template <class Real> constexpr bool kahan() { return sizeof(Real) == 4; }
 
 template <class Real> __device__ __forceinline__ Real ld(const Real *p) { return __ldg(p); }
 
-// ------------------------------------------------------------- pointer stencils (3D engine)
-// 5-point DRP derivative (include/SeisCommon/FiniteDifference.hpp:14-26, PointKernels2D.hpp:38-47):
-// forward taps at offsets -1..3, backward at +1..-3 with negated coefficients.
-template <class Real, int DIR>
-__device__ __forceinline__ Real drp5(const Real *__restrict__ v, long long q, long long s, Real h) {
-    Real r = Real(0);
-    if (DIR == 0) {
-        r += Real(-.30874) * ld(v + q - s);
-        r += Real(-.6326) * ld(v + q);
-        r += Real(1.233) * ld(v + q + s);
-        r += Real(-.3334) * ld(v + q + 2 * s);
-        r += Real(.04168) * ld(v + q + 3 * s);
-    } else {
-        r += -Real(-.30874) * ld(v + q + s);
-        r += -Real(-.6326) * ld(v + q);
-        r += -Real(1.233) * ld(v + q - s);
-        r += -Real(-.3334) * ld(v + q - 2 * s);
-        r += -Real(.04168) * ld(v + q - 3 * s);
-    }
-    return r / h;
+// Correctly rounded y / 6 without a division instruction sequence.  y/6 = (y/2)/3 with y/2 exact,
+// and x/3 by Markstein's correction (P. W. Markstein, "Computation of elementary functions on the
+// IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with c = RN(1/3) -- here
+// 3c = 1 - 2^-54 (FP32: 1 + 2^-25), so q0 = RN(x c) is within one ulp of x/3 -- the remainder
+// r = x - 3 q0 is exact under an FMA and RN(q0 + r c) = RN(x/3).  The theorem excludes
+// underflow, so tiny (but nonzero), huge and non-finite x take the plain division -- out of line,
+// so that the compiler cannot evaluate that division speculatively on the common path.  A zero
+// passes through the FMA form exactly.
+template <class Real> __device__ __noinline__ Real plainDiv6(Real y) { return y / Real(6); }
+template <class Real> __device__ __forceinline__ Real div6(Real y) {
+    constexpr Real c = Real(1) / Real(3);
+    constexpr Real tiny = sizeof(Real) == 8 ? Real(0x1p-960) : Real(0x1p-100f);
+    constexpr Real huge = sizeof(Real) == 8 ? Real(0x1p+1000) : Real(0x1p+120f);
+    const Real x = y * Real(0.5);
+    const Real ax = fabs(x);
+    if (!(ax <= huge) || (ax < tiny && ax != Real(0))) return plainDiv6(y);
+    const Real q0 = x * c;
+    const Real r = fma(-q0, Real(3), x);
+    return fma(r, c, q0);
 }
-// One-sided near-surface velocity stencils: 2 points at depth 1, 3 points at depth 2.
-template <class Real, int DIR>
-__device__ __forceinline__ Real near2(const Real *__restrict__ v, long long q, long long s, Real h) {
-    Real r = Real(0);
-    if (DIR == 0) {
-        r += Real(-1) * ld(v + q);
-        r += Real(1) * ld(v + q + s);
-    } else {
-        r += -Real(-1) * ld(v + q);
-        r += -Real(1) * ld(v + q - s);
-    }
-    return r / h;
-}
-template <class Real, int DIR>
-__device__ __forceinline__ Real near3(const Real *__restrict__ v, long long q, long long s, Real h) {
-    const Real c0 = Real(-7) / Real(6), c1 = Real(8) / Real(6), c2 = Real(-1) / Real(6);
-    Real r = Real(0);
-    if (DIR == 0) {
-        r += c0 * ld(v + q);
-        r += c1 * ld(v + q + s);
-        r += c2 * ld(v + q + 2 * s);
-    } else {
-        r += -c0 * ld(v + q);
-        r += -c1 * ld(v + q - s);
-        r += -c2 * ld(v + q - 2 * s);
-    }
-    return r / h;
+
+// Correctly rounded x / d from dinv = RN(1/d) without a division instruction sequence, by two
+// Markstein corrections: q0 = RN(x dinv) is within 1.5 ulp of x/d, q1 = RN(q0 + (x - d q0) dinv)
+// is within one ulp, and then RN(q1 + (x - d q1) dinv) = RN(x/d) (P. W. Markstein, IBM J. Res.
+// Dev. 34(1), 1990; each remainder is exact under an FMA).  The divisor must lie in
+// [2^-20, 2^20]; tiny (nonzero), huge and non-finite x take the plain division out of line.
+template <class Real> __device__ __noinline__ Real plainDiv(Real x, Real d) { return x / d; }
+template <class Real> __device__ __forceinline__ Real divBy(Real x, Real d, Real dinv) {
+    constexpr Real tiny = sizeof(Real) == 8 ? Real(0x1p-960) : Real(0x1p-100f);
+    constexpr Real huge = sizeof(Real) == 8 ? Real(0x1p+1000) : Real(0x1p+100f);
+    const Real ax = fabs(x);
+    if (!(ax <= huge) || (ax < tiny && ax != Real(0))) return plainDiv(x, d);
+    const Real q0 = x * dinv;
+    const Real q1 = fma(fma(-q0, d, x), dinv, q0);
+    return fma(fma(-q1, d, x), dinv, q1);
 }
 
 // ------------------------------------------------------------- node sources
@@ -224,7 +211,7 @@ template <class Real, bool EXACT, int STAGE> struct StreamNode {
 // from the first product gives the same value (0 + x == x, up to the sign of a zero result).
 template <class Real, class S> __device__ __forceinline__ Real scaled(const Mesh<Real> &m, Real r) {
     if constexpr (S::exact) return r * m.hinv;
-    else return r / m.h;
+    else return divBy(r, m.h, m.hinv);
 }
 template <class Real, int DIR, class S> __device__ __forceinline__ Real tdrp(const S &t, const Mesh<Real> &m, int f, int axis) {
     const int sx = axis ? 0 : 1, sz = axis ? 1 : 0;
@@ -323,24 +310,6 @@ __device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes)
 }
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Correctly rounded y / 6 without a division instruction sequence.  y/6 = (y/2)/3 with y/2 exact,
-// and x/3 by Markstein's correction (P. W. Markstein, "Computation of elementary functions on the
-// IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with c = RN(1/3) -- here
-// 3c = 1 - 2^-54 (FP32: 1 + 2^-25), so q0 = RN(x c) is within one ulp of x/3 -- the remainder
-// r = x - 3 q0 is exact under an FMA and RN(q0 + r c) = RN(x/3).  The theorem excludes
-// underflow, so tiny, huge and non-finite x take the plain division.
-template <class Real> __device__ __forceinline__ Real div6(Real y) {
-    constexpr Real c = Real(1) / Real(3);
-    constexpr Real tiny = sizeof(Real) == 8 ? Real(0x1p-960) : Real(0x1p-100f);
-    constexpr Real huge = sizeof(Real) == 8 ? Real(0x1p+1000) : Real(0x1p+120f);
-    const Real x = y * Real(0.5);
-    const Real ax = fabs(x);
-    if (!(ax >= tiny && ax <= huge)) return y / Real(6);
-    const Real q0 = x * c;
-    const Real r = fma(-q0, Real(3), x);
-    return fma(r, c, q0);
-}
 
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.

@@ -23,6 +23,8 @@ template <class Real> struct Mesh {
     int nx, ny, nz;
     long long count, plane;
     Real h, lambda, mu, density;    // uniform material (used when the material arrays are null)
+    Real hinv;                      // RN(1/h)
+    int hinvExact;                  // h is a power of two (or FP32): x/h = x*hinv
     const Real *metric[9];          // d(xi,eta,zeta)/d(x,y,z), row-major 3x3 per node
     const Real *jac, *damping, *source, *sg[3];
     const Real *mlambda, *mmu, *mdensity;
@@ -51,9 +53,59 @@ template <class Real> struct StageArgs {
 
 using k2::ld;
 
-template <class Real, int DIR>
-__device__ __forceinline__ Real drp5(const Real *__restrict__ v, long long q, long long s, Real h) {
-    return k2::drp5<Real, DIR>(v, q, s, h);
+// x / h as the reference forms it: the product with 1/h when that is exact, else the correctly
+// rounded FMA quotient (both equal the IEEE division bit for bit).
+template <class Real, bool EXACT> __device__ __forceinline__ Real overH(const Mesh<Real> &m, Real r) {
+    if constexpr (EXACT) return r * m.hinv;
+    else return k2::divBy(r, m.h, m.hinv);
+}
+// DRP derivatives along stride s (include/SeisCommon/FiniteDifference.hpp:14-26): 5 taps, and the
+// 2- and 3-point one-sided stencils of depths 1 and 2.  Sums start from the first product (the
+// reference adds it to zero: the same value up to the sign of a zero).
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real d5(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    Real r;
+    if (DIR == 0) {
+        r = Real(-.30874) * ld(v + q - s);
+        r += Real(-.6326) * ld(v + q);
+        r += Real(1.233) * ld(v + q + s);
+        r += Real(-.3334) * ld(v + q + 2 * s);
+        r += Real(.04168) * ld(v + q + 3 * s);
+    } else {
+        r = -Real(-.30874) * ld(v + q + s);
+        r += -Real(-.6326) * ld(v + q);
+        r += -Real(1.233) * ld(v + q - s);
+        r += -Real(-.3334) * ld(v + q - 2 * s);
+        r += -Real(.04168) * ld(v + q - 3 * s);
+    }
+    return overH<Real, EXACT>(m, r);
+}
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real d2(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    Real r;
+    if (DIR == 0) {
+        r = Real(-1) * ld(v + q);
+        r += Real(1) * ld(v + q + s);
+    } else {
+        r = -Real(-1) * ld(v + q);
+        r += -Real(1) * ld(v + q - s);
+    }
+    return overH<Real, EXACT>(m, r);
+}
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real d3(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    const Real c0 = Real(-7) / Real(6), c1 = Real(8) / Real(6), c2 = Real(-1) / Real(6);
+    Real r;
+    if (DIR == 0) {
+        r = c0 * ld(v + q);
+        r += c1 * ld(v + q + s);
+        r += c2 * ld(v + q + 2 * s);
+    } else {
+        r = -c0 * ld(v + q);
+        r += -c1 * ld(v + q - s);
+        r += -c2 * ld(v + q - 2 * s);
+    }
+    return overH<Real, EXACT>(m, r);
 }
 
 template <class Real>
@@ -67,7 +119,7 @@ __device__ __forceinline__ Real tractionFlux(const Mesh<Real> &m, const Real *__
 
 // src/three_d/PointKernels3D.hpp:73-91
 template <class Real, int DX, int DY, int DZ>
-__device__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, Real rho) {
+__device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, Real rho) {
     const Real C[5] = {Real(-.30874), Real(-.6326), Real(1.233), Real(-.3334), Real(.04168)};
     Real sum = Real(0);
     for (int axis = 0; axis < 3; ++axis) {
@@ -96,20 +148,20 @@ __device__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w,
 // SM and the memory system mostly idle (tighter bounds spill heavily in this kernel).
 template <class Real> constexpr int minBlocks3() { return 2; }
 
-template <class Real, int DX, int DY, int DZ, int STAGE>
-__global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const StageArgs<Real> p) {
+// FULL = false compiles the interior form: the caller guarantees that the node lies below the
+// four surface rows, outside the sponge and outside the source support.
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool FULL>
+__device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = 3 + blockIdx.z;
     if (i >= m.nx - 3 || j >= m.ny - 3) return;
     const Clock *clk = p.clock;
-    if (clk->faulted) return;
     const long long n = m.count, nx = m.nx, plane = m.plane;
     const long long q = i + nx * j + plane * k;
-    const int depth = k - 3;
+    const int depth = FULL ? k - 3 : 4; // any depth past the near-surface rows
     const Real *__restrict__ w = p.in;
-    const Real h = m.h;
     const Real lam = m.mlambda ? ld(m.mlambda + q) : m.lambda;
     const Real mu = m.mmu ? ld(m.mmu + q) : m.mu;
     const Real rho = m.mdensity ? ld(m.mdensity + q) : m.density;
@@ -121,8 +173,8 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
     Real dv[3][2];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        dv[v][0] = drp5<Real, DX>(w + v * n, q, 1, h);
-        dv[v][1] = drp5<Real, DY>(w + v * n, q, nx, h);
+        dv[v][0] = d5<Real, DX, EXACT>(w + v * n, q, 1, m);
+        dv[v][1] = d5<Real, DY, EXACT>(w + v * n, q, nx, m);
     }
     Real dzs[3] = {0, 0, 0};
     if (depth == 0) { // src/three_d/PointKernels3D.hpp:52-66
@@ -146,21 +198,21 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
     Real gr[9][3];
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
-        Real d0, d1, d2;
+        Real dx, dy, dz;
         if (f < 3) {
-            d0 = dv[f][0];
-            d1 = dv[f][1];
-            if (depth == 0) d2 = dzs[f];
-            else if (depth == 1) d2 = k2::near2<Real, DZ>(w + f * n, q, plane, h);
-            else if (depth == 2) d2 = k2::near3<Real, DZ>(w + f * n, q, plane, h);
-            else d2 = drp5<Real, DZ>(w + f * n, q, plane, h);
+            dx = dv[f][0];
+            dy = dv[f][1];
+            if (depth == 0) dz = dzs[f];
+            else if (depth == 1) dz = d2<Real, DZ, EXACT>(w + f * n, q, plane, m);
+            else if (depth == 2) dz = d3<Real, DZ, EXACT>(w + f * n, q, plane, m);
+            else dz = d5<Real, DZ, EXACT>(w + f * n, q, plane, m);
         } else {
-            d0 = drp5<Real, DX>(w + f * n, q, 1, h);
-            d1 = drp5<Real, DY>(w + f * n, q, nx, h);
-            d2 = drp5<Real, DZ>(w + f * n, q, plane, h);
+            dx = d5<Real, DX, EXACT>(w + f * n, q, 1, m);
+            dy = d5<Real, DY, EXACT>(w + f * n, q, nx, m);
+            dz = d5<Real, DZ, EXACT>(w + f * n, q, plane, m);
         }
 #pragma unroll
-        for (int a = 0; a < 3; ++a) gr[f][a] = M[a] * d0 + M[3 + a] * d1 + M[6 + a] * d2;
+        for (int a = 0; a < 3; ++a) gr[f][a] = M[a] * dx + M[3 + a] * dy + M[6 + a] * dz;
     }
     Real r[9];
     if (depth <= (DZ ? 3 : 1)) {
@@ -171,7 +223,7 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
         r[1] = (gr[6][0] + gr[4][1] + gr[8][2]) / rho;
         r[2] = (gr[7][0] + gr[8][1] + gr[5][2]) / rho;
     }
-    if (i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
+    if (FULL && i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
         const Real s = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
         const Real ratio = m.density / rho;
 #pragma unroll
@@ -184,7 +236,7 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
     r[6] = mu * (gr[0][1] + gr[1][0]);
     r[7] = mu * (gr[0][2] + gr[2][0]);
     r[8] = mu * (gr[1][2] + gr[2][1]);
-    if (!(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
+    if (FULL && !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
         const Real d = ld(m.damping + q);
 #pragma unroll
         for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
@@ -252,6 +304,30 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const Stage
     if (STAGE == 3 && k2::kahan<Real>())
 #pragma unroll
         for (int f = 0; f < 9; ++f) p.cout[f * n + q] = comp[f];
+}
+
+// One RK stage of a 3D shot: block 32x8 nodes of one z layer.  A CTA whose nodes are all below
+// the surface rows, outside the sponge and outside the source support runs the interior form.
+template <class Real, int DX, int DY, int DZ, int STAGE>
+__global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __grid_constant__ StageArgs<Real> p) {
+    const Mesh<Real> &m = p.m;
+    if (p.clock->faulted) return;
+    const int i0 = 3 + blockIdx.x * blockDim.x, i1 = i0 + blockDim.x, j0 = 3 + blockIdx.y * blockDim.y, j1 = j0 + blockDim.y;
+    const int k = 3 + blockIdx.z;
+    const bool surface = k < 7;
+    const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
+    const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
+    const bool interior = !(surface || source || sponge);
+    if constexpr (sizeof(Real) == 4) {
+        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, true, false>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true, true>(p);
+    } else if (m.hinvExact) {
+        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, true, false>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true, true>(p);
+    } else {
+        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, false, false>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, false, true>(p);
+    }
 }
 
 struct Partial {
