@@ -103,6 +103,11 @@ class ClockSampler:
         self.thread = threading.Thread(target=lambda: [self.lines.append(l) for l in self.proc.stdout], daemon=True)
         self.thread.start()
 
+    def wait_first(self, timeout: float = 5.0):
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
     def stop(self) -> dict | None:
         if not self.proc:
             return None
@@ -170,6 +175,8 @@ def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
     acc = C.c_int32()
     set_stream = L.swl2d_set_stream if dim == 2 else L.swl3d_set_stream
     swl._check(set_stream(eng, C.c_void_p(stream.cuda_stream)))
+    # trace and forcing tables sized for the timed batch: it allocates nothing and records no graph
+    swl._check((L.swl2d_reserve if dim == 2 else L.swl3d_reserve)(eng, max(steps, warmup)))
 
     def run(first, n):
         if dim == 2:
@@ -179,7 +186,7 @@ def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
         swl._check(st)
 
     step = info["step"]
-    run(step, warmup)
+    run(step, warmup)  # a multiple of 8: the timed batch replays the CUDA graph the warm-up recorded
     step += warmup
     torch.cuda.synchronize()
     if dist:
@@ -295,6 +302,7 @@ def gpu_arm(args):
         sampler = ClockSampler(local) if precision == 0 and rank == 0 else None
         if sampler:
             sampler.start()
+            sampler.wait_first()  # the sampler is up before the timed region starts
         ms, prof = time_engine(swl, sim, dim, params, args.steps, args.warmup, torch, dist, rank)
         clocks = sampler.stop() if sampler else None
         if dist:
@@ -315,7 +323,7 @@ def gpu_arm(args):
     # e2e: the same K steps through the public session API (host forcing upload and trace
     # download inside the timed region), from a reset shot.
     sim64.reset()
-    sim64.advance(max(1, args.warmup))
+    sim64.advance(args.warmup)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -405,6 +413,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    # Batches run as CUDA graphs of 8 steps keyed by the step phase; a warm-up that is a multiple
+    # of 8 leaves the timed batch on the graph the warm-up already recorded (no capture inside the
+    # timed region).  The line reports the warm-up actually run.
+    args.warmup = (args.warmup + 7) // 8 * 8
     if args.impl == "reference":
         reference_arm(args)
     else:

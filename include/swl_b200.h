@@ -145,6 +145,10 @@ swl_status swl2d_profile(swl2d_engine *engine, int32_t first, int32_t count, dou
 /* Run the engine's work on a caller-provided cudaStream_t (NULL restores its own stream).
  * No counterpart in the reference (its engines launch on the legacy default stream). */
 swl_status swl2d_set_stream(swl2d_engine *engine, void *cuda_stream);
+/* Preallocate the forcing and trace tables for batches of up to `steps` steps, so that later
+ * batches within that size allocate nothing and record no new CUDA graphs.  No counterpart in
+ * the reference (it reads traces back every step). */
+swl_status swl2d_reserve(swl2d_engine *engine, int32_t steps);
 
 /* A 2D FP64 state held in caller-owned device memory (padded nx x nz grid, x fastest). */
 typedef struct swl_state2d_view {
@@ -225,6 +229,7 @@ int64_t swl3d_resident_bytes(const swl3d_engine *engine);
 swl_status swl3d_profile(swl3d_engine *engine, int32_t first, int32_t count, double dt, double frequency,
                          swl_profile *out);
 swl_status swl3d_set_stream(swl3d_engine *engine, void *cuda_stream);
+swl_status swl3d_reserve(swl3d_engine *engine, int32_t steps); /* as swl2d_reserve */
 
 #ifdef __cplusplus
 }

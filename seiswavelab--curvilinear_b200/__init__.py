@@ -137,6 +137,8 @@ def library() -> C.CDLL:
     L.swl3d_profile.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(Profile)]
     L.swl2d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.swl3d_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.swl2d_reserve.argtypes = [C.c_void_p, C.c_int32]
+    L.swl3d_reserve.argtypes = [C.c_void_p, C.c_int32]
     L.swl2d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
     L.swl2d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.swl2d_wait.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
@@ -297,6 +299,9 @@ class Engine2D:
     def set_stream(self, stream_handle: int | None):
         _check(library().swl2d_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 
+    def reserve(self, steps: int):
+        _check(library().swl2d_reserve(self._h, int(steps)))
+
 
 class Engine3D:
     """GPU engine for one 3D shot.  Mesh keys: nx, ny, nz (padded), h, lambda, mu, density,
@@ -392,3 +397,6 @@ class Engine3D:
 
     def set_stream(self, stream_handle: int | None):
         _check(library().swl3d_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def reserve(self, steps: int):
+        _check(library().swl3d_reserve(self._h, int(steps)))

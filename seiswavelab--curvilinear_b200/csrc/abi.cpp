@@ -209,6 +209,9 @@ swl_status swl2d_profile(swl2d_engine *e, int32_t first, int32_t count, double d
 swl_status swl2d_set_stream(swl2d_engine *e, void *stream) {
     return guarded([&] { ENGINE(e); E.setStream(static_cast<cudaStream_t>(stream)); });
 }
+swl_status swl2d_reserve(swl2d_engine *e, int32_t steps) {
+    return guarded([&] { ENGINE(e); E.reserve(steps); });
+}
 
 // ----------------------------------------------------------------------------- 3D
 swl_status swl3d_create(const swl_mesh3d *mesh, const int64_t *receivers, int32_t n, int32_t dev, swl3d_engine **out) {
@@ -324,6 +327,9 @@ swl_status swl3d_profile(swl3d_engine *e, int32_t first, int32_t count, double d
 }
 swl_status swl3d_set_stream(swl3d_engine *e, void *stream) {
     return guarded([&] { ENGINE(e); E.setStream(static_cast<cudaStream_t>(stream)); });
+}
+swl_status swl3d_reserve(swl3d_engine *e, int32_t steps) {
+    return guarded([&] { ENGINE(e); E.reserve(steps); });
 }
 
 } // extern "C"

@@ -40,6 +40,9 @@ class Engine2D {
     virtual bool faulted() const = 0;
     virtual void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) = 0;
     virtual void setStream(cudaStream_t stream) = 0;
+    // Preallocate the forcing and trace tables for batches of up to `steps` steps, so that such
+    // batches record no new CUDA graphs.
+    virtual void reserve(int steps) = 0;
     // Asynchronous batches: launch returns once the batch is enqueued; query polls and finish
     // waits; both return the accepted step count of the batch.
     virtual void launch(int first, int count, double dt, double frequency, double scale, double growthAfter) = 0;
@@ -444,6 +447,12 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
+    void reserve(int steps) override {
+        settle();
+        DeviceScope scope(device_);
+        if (steps < 0) throw Error(SWL_ERR_INVALID, "reserve needs steps >= 0");
+        ensureCapacity(steps);
+    }
     void setStream(cudaStream_t s) override {
         settle();
         DeviceScope scope(device_);

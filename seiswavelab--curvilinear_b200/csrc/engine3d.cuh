@@ -29,6 +29,9 @@ class Engine3D {
     virtual bool faulted() const = 0;
     virtual void profile(int first, int count, double dt, double frequency, swl_profile &out) = 0;
     virtual void setStream(cudaStream_t stream) = 0;
+    // Preallocate the forcing and trace tables for batches of up to `steps` steps, so that such
+    // batches record no new CUDA graphs.
+    virtual void reserve(int steps) = 0;
     virtual void launch(int first, int count, double dt, double frequency, double growthAfter) = 0;
     virtual bool query(int &accepted) = 0;
     virtual int finish() = 0;
@@ -320,6 +323,12 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         if (ownStream_) cudaStreamDestroy(ownStream_);
     }
     bool faulted() const override { return faulted_; }
+    void reserve(int steps) override {
+        settle();
+        DeviceScope scope(device_);
+        if (steps < 0) throw Error(SWL_ERR_INVALID, "reserve needs steps >= 0");
+        ensureCapacity(steps);
+    }
     void setStream(cudaStream_t s) override {
         settle();
         DeviceScope scope(device_);

@@ -101,6 +101,7 @@ struct Session2D {
                 m.rates[l] = model.rates[l], m.delta_p[l] = model.deltaP[l].data(), m.delta_s[l] = model.deltaS[l].data();
             m.precision = params.precision, m.array_precision = SWL_FP64;
             ok(swl2d_create(&m, model.receiverNodes.data(), int32_t(model.receiverNodes.size()), device, &engine));
+            ok(swl2d_reserve(engine, std::min(model.total, maxBatch))); // batch tables sized once, at creation
             ok(swl2d_diagnostics(engine, &diag));
         }
         initMs = millis(t0);
@@ -258,6 +259,7 @@ struct Session3D {
             m.source_amplitude = model.sourceAmplitude;
             m.precision = params.precision;
             ok(swl3d_create(&m, model.receiverNodes.data(), int32_t(model.receiverNodes.size()), device, &engine));
+            ok(swl3d_reserve(engine, std::min(model.total, maxBatch))); // batch tables sized once, at creation
             ok(swl3d_diagnostics(engine, &diag));
         }
         initMs = millis(t0);

@@ -144,13 +144,71 @@ __device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__
     return sum / (m.h * ld(m.jac + q) * rho);
 }
 
-// Two CTAs of 256 threads per SM: without the bound the register allocation leaves one CTA per
-// SM and the memory system mostly idle (tighter bounds spill heavily in this kernel).
-template <class Real> constexpr int minBlocks3() { return 2; }
+// Three CTAs of 256 threads per SM (80 registers).  The kernel waits on its L1/L2 loads, and the
+// extra resident warps hide more of that latency than the ~200 bytes of spills per thread this
+// bound costs: measured at 400x288x200, three CTAs per SM run the stages 1.3x faster than two.
+template <class Real> constexpr int minBlocks3() { return 3; }
 
-// FULL = false compiles the interior form: the caller guarantees that the node lies below the
-// four surface rows, outside the sponge and outside the source support.
-template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool FULL>
+// RK combine, surface projection and stores of the nine rates of one node.
+template <class Real, int STAGE>
+__device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r)[9], long long q, int depth, long long sq) {
+    const Mesh<Real> &m = p.m;
+    const long long n = m.count;
+    // FP64: A = U + dt/6 k1, A += dt/3 k2, A += dt/3 k3, new = A + dt/6 k4 (the reference's
+    // order).  FP32: A accumulates the increment alone (A = dt/6 k1, ...), and stage 3 adds
+    // d = A + dt/6 k4 to U by Kahan's compensated summation (y = d - c, t = U + y,
+    // c' = (t - U) - y).
+    Real o[9], comp[9];
+#pragma unroll
+    for (int f = 0; f < 9; ++f) {
+        if (STAGE == 0) {
+            const Real u = ld(p.base + f * n + q);
+            p.acc[f * n + q] = k2::kahan<Real>() ? p.w6 * r[f] : u + p.w6 * r[f];
+            o[f] = u + p.weight * r[f];
+        } else if (STAGE < 3) {
+            const Real u = ld(p.base + f * n + q);
+            p.acc[f * n + q] = p.acc[f * n + q] + p.w3 * r[f];
+            o[f] = u + p.weight * r[f];
+        } else if constexpr (k2::kahan<Real>()) {
+            const Real u = ld(p.base + f * n + q);
+            const Real y = (p.acc[f * n + q] + p.w6 * r[f]) - p.cin[f * n + q];
+            o[f] = u + y;
+            comp[f] = (o[f] - u) - y;
+        } else {
+            o[f] = p.acc[f * n + q] + p.w6 * r[f];
+        }
+    }
+    if (depth == 0) { // tangential stress projection (PointKernels3D.hpp:36-51)
+        const Real nn[3] = {ld(m.normals + 3 * sq), ld(m.normals + 3 * sq + 1), ld(m.normals + 3 * sq + 2)};
+        const Real s[9] = {o[3], o[6], o[7], o[6], o[4], o[8], o[7], o[8], o[5]};
+        Real t[3] = {0, 0, 0}, x[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) t[a] += s[3 * a + b] * nn[b];
+        const Real nnn = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) x[3 * a + b] = s[3 * a + b] - nn[a] * t[b] - t[a] * nn[b] + nnn * nn[a] * nn[b];
+        o[3] = x[0];
+        o[4] = x[4];
+        o[5] = x[8];
+        o[6] = Real(0.5) * (x[1] + x[3]);
+        o[7] = Real(0.5) * (x[2] + x[6]);
+        o[8] = Real(0.5) * (x[5] + x[7]);
+    }
+    Real *dst = STAGE == 3 ? p.acc : p.out;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) dst[f * n + q] = o[f];
+    if (STAGE == 3 && k2::kahan<Real>())
+#pragma unroll
+        for (int f = 0; f < 9; ++f) p.cout[f * n + q] = comp[f];
+}
+
+// The general node: surface rows (traction-free derivative, traction-image momentum,
+// projection), sponge damping and the source.
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
 __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,7 +218,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Clock *clk = p.clock;
     const long long n = m.count, nx = m.nx, plane = m.plane;
     const long long q = i + nx * j + plane * k;
-    const int depth = FULL ? k - 3 : 4; // any depth past the near-surface rows
+    const int depth = k - 3;
     const Real *__restrict__ w = p.in;
     const Real lam = m.mlambda ? ld(m.mlambda + q) : m.lambda;
     const Real mu = m.mmu ? ld(m.mmu + q) : m.mu;
@@ -223,7 +281,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
         r[1] = (gr[6][0] + gr[4][1] + gr[8][2]) / rho;
         r[2] = (gr[7][0] + gr[8][1] + gr[5][2]) / rho;
     }
-    if (FULL && i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
+    if (i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
         const Real s = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
         const Real ratio = m.density / rho;
 #pragma unroll
@@ -236,7 +294,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     r[6] = mu * (gr[0][1] + gr[1][0]);
     r[7] = mu * (gr[0][2] + gr[2][0]);
     r[8] = mu * (gr[1][2] + gr[2][1]);
-    if (FULL && !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
+    if (!(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
         const Real d = ld(m.damping + q);
 #pragma unroll
         for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
@@ -254,56 +312,65 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
         p.surfRate[sq] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
         p.surfRate[plane + sq] = sqrt(norm2);
     }
-    // FP64: A = U + dt/6 k1, A += dt/3 k2, A += dt/3 k3, new = A + dt/6 k4 (the reference's
-    // order).  FP32: A accumulates the increment alone (A = dt/6 k1, ...), and stage 3 adds
-    // d = A + dt/6 k4 to U by Kahan's compensated summation (y = d - c, t = U + y,
-    // c' = (t - U) - y).
-    Real o[9], comp[9];
+    finish3<Real, STAGE>(p, r, q, depth, sq);
+}
+
+// The interior node (below the surface rows, outside the sponge and the source support).  The
+// stress fields are differentiated one at a time and their physical gradients folded into the
+// momentum sums as they come, in the reference's order r0 = (gxx,x + gxy,y) + gxz,z,
+// r1 = (gxy,x + gyy,y) + gyz,z, r2 = (gxz,x + gyz,y) + gzz,z (src/three_d/PointKernels3D.hpp:92-112),
+// so only a few gradients are live at a time.
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
+__device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
+    const Mesh<Real> &m = p.m;
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    if (i >= m.nx - 3 || j >= m.ny - 3) return;
+    const long long n = m.count, nx = m.nx, plane = m.plane;
+    const long long q = i + nx * j + plane * k;
+    const Real *__restrict__ w = p.in;
+    Real M[9];
 #pragma unroll
-    for (int f = 0; f < 9; ++f) {
-        if (STAGE == 0) {
-            const Real u = ld(p.base + f * n + q);
-            p.acc[f * n + q] = k2::kahan<Real>() ? p.w6 * r[f] : u + p.w6 * r[f];
-            o[f] = u + p.weight * r[f];
-        } else if (STAGE < 3) {
-            const Real u = ld(p.base + f * n + q);
-            p.acc[f * n + q] = p.acc[f * n + q] + p.w3 * r[f];
-            o[f] = u + p.weight * r[f];
-        } else if constexpr (k2::kahan<Real>()) {
-            const Real u = ld(p.base + f * n + q);
-            const Real y = (p.acc[f * n + q] + p.w6 * r[f]) - p.cin[f * n + q];
-            o[f] = u + y;
-            comp[f] = (o[f] - u) - y;
-        } else {
-            o[f] = p.acc[f * n + q] + p.w6 * r[f];
-        }
+    for (int c = 0; c < 9; ++c) M[c] = ld(m.metric[c] + q);
+    // physical gradient component a of field f: ((M_a dxi + M_3+a deta) + M_6+a dzeta)
+    auto grad = [&](int f, Real (&g)[3], bool x, bool y, bool z) {
+        const Real dx = d5<Real, DX, EXACT>(w + f * n, q, 1, m);
+        const Real dy = d5<Real, DY, EXACT>(w + f * n, q, nx, m);
+        const Real dz = d5<Real, DZ, EXACT>(w + f * n, q, plane, m);
+        if (x) g[0] = M[0] * dx + M[3] * dy + M[6] * dz;
+        if (y) g[1] = M[1] * dx + M[4] * dy + M[7] * dz;
+        if (z) g[2] = M[2] * dx + M[5] * dy + M[8] * dz;
+    };
+    Real r[9];
+    {
+        Real gv[3][3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) grad(v, gv[v], true, true, true);
+        const Real lam = m.mlambda ? ld(m.mlambda + q) : m.lambda;
+        const Real mu = m.mmu ? ld(m.mmu + q) : m.mu;
+        const Real div = gv[0][0] + gv[1][1] + gv[2][2];
+        r[3] = lam * div + 2 * mu * gv[0][0];
+        r[4] = lam * div + 2 * mu * gv[1][1];
+        r[5] = lam * div + 2 * mu * gv[2][2];
+        r[6] = mu * (gv[0][1] + gv[1][0]);
+        r[7] = mu * (gv[0][2] + gv[2][0]);
+        r[8] = mu * (gv[1][2] + gv[2][1]);
     }
-    if (depth == 0) { // tangential stress projection (PointKernels3D.hpp:36-51)
-        const Real nn[3] = {ld(m.normals + 3 * sq), ld(m.normals + 3 * sq + 1), ld(m.normals + 3 * sq + 2)};
-        const Real s[9] = {o[3], o[6], o[7], o[6], o[4], o[8], o[7], o[8], o[5]};
-        Real t[3] = {0, 0, 0}, x[9];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) t[a] += s[3 * a + b] * nn[b];
-        const Real nnn = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) x[3 * a + b] = s[3 * a + b] - nn[a] * t[b] - t[a] * nn[b] + nnn * nn[a] * nn[b];
-        o[3] = x[0];
-        o[4] = x[4];
-        o[5] = x[8];
-        o[6] = Real(0.5) * (x[1] + x[3]);
-        o[7] = Real(0.5) * (x[2] + x[6]);
-        o[8] = Real(0.5) * (x[5] + x[7]);
+    {
+        Real g[3], m0, m1, m2, t41, t52, t70;
+        grad(3, g, true, false, false), m0 = g[0];
+        grad(4, g, false, true, false), t41 = g[1];
+        grad(5, g, false, false, true), t52 = g[2];
+        grad(6, g, true, true, false), m0 = m0 + g[1], m1 = g[0] + t41;
+        grad(7, g, true, false, true), m0 = m0 + g[2], t70 = g[0];
+        grad(8, g, false, true, true), m1 = m1 + g[2], m2 = (t70 + g[1]) + t52;
+        const Real rho = m.mdensity ? ld(m.mdensity + q) : m.density;
+        r[0] = m0 / rho;
+        r[1] = m1 / rho;
+        r[2] = m2 / rho;
     }
-    Real *dst = STAGE == 3 ? p.acc : p.out;
-#pragma unroll
-    for (int f = 0; f < 9; ++f) dst[f * n + q] = o[f];
-    if (STAGE == 3 && k2::kahan<Real>())
-#pragma unroll
-        for (int f = 0; f < 9; ++f) p.cout[f * n + q] = comp[f];
+    finish3<Real, STAGE>(p, r, q, 4, i + nx * j);
 }
 
 // One RK stage of a 3D shot: block 32x8 nodes of one z layer.  A CTA whose nodes are all below
@@ -319,14 +386,14 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __gri
     const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
     const bool interior = !(surface || source || sponge);
     if constexpr (sizeof(Real) == 4) {
-        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, true, false>(p);
-        else stageBody3<Real, DX, DY, DZ, STAGE, true, true>(p);
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p);
     } else if (m.hinvExact) {
-        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, true, false>(p);
-        else stageBody3<Real, DX, DY, DZ, STAGE, true, true>(p);
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p);
     } else {
-        if (interior) stageBody3<Real, DX, DY, DZ, STAGE, false, false>(p);
-        else stageBody3<Real, DX, DY, DZ, STAGE, false, true>(p);
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, false>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, false>(p);
     }
 }
 
