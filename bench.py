@@ -165,6 +165,26 @@ def traffic_from_profiles(workload_name: str, dtype: str):
         return None
 
 
+def reference_gpu(params: dict, steps: int, warmup: int) -> dict | None:
+    """The reference's own CUDA engine (src/two_d/CudaEngine2D.cu, built from its sources for
+    sm_100a) on the same 2D shot, FP64 and FP32: production advance() with its per-step stats and
+    receiver readback, timed by the reference driver after a warm-up."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    if not O.REF2D_CUDA.exists():
+        return None
+    out = {"engine": "reference CudaEngine (src/two_d/CudaEngine2D.cu), sm_100a build", "steps": steps, "warmup": warmup}
+    for prec, key in ((0, "fp64"), (1, "fp32")):
+        p = dict(params)
+        p["maxSteps"] = warmup + steps
+        p["precision"] = prec
+        r = O.run_reference_2d(p, steps=steps, threads=1, dump_mesh=False, warmup=warmup, backend="cuda", timeout=600)
+        pts = float((int(r["nx"]) - 6) * (int(r["nz"]) - 6))
+        sec = float(r["runMs"]) / 1e3
+        out[key] = {"value": pts * steps / sec / 1e6, "unit": UNIT, "ms_per_step": float(r["msPerStep"])}
+    return out
+
+
 def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
     """Device time of `steps` engine steps on torch's current stream; returns (ms, profile)."""
     L = swl.library()
@@ -348,6 +368,9 @@ def gpu_arm(args):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu:
         base = cpu_baseline(r64["params"], dim, args.cpu_steps, 1)
+    ref_gpu = None
+    if rank == 0 and world == 1 and dim == 2 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu(r64["params"], args.ref_gpu_steps, 2)
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = serving_leg(args, local)
@@ -366,6 +389,8 @@ def gpu_arm(args):
         if r32:
             line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],
                             "roofline": r32["roofline"], "speedup_vs_fp64": r32["value"] / r64["value"]}
+        if ref_gpu:
+            line["reference_gpu"] = ref_gpu
         if serving:
             line["serving"] = serving
         line["profile_fp64"] = r64["profile"]
@@ -406,6 +431,8 @@ def main():
                     choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d", "small_3d"])
     ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA engine")
+    ap.add_argument("--ref-gpu-steps", type=int, default=10, help="timed steps of the reference CUDA engine")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=48, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")

@@ -20,6 +20,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REF2D = HERE / "_ref" / "ref2d"
 REF3D = HERE / "_ref" / "ref3d"
+REF2D_CUDA = HERE / "_ref" / "ref2d_cuda"  # the 2D driver with the reference's own CUDA engine
 LIB = HERE / "liboracle.so"
 
 _dp = C.POINTER(C.c_double)
@@ -266,10 +267,13 @@ def _load_dir(d: Path) -> dict:
 
 
 def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_mesh: bool = True,
-                  workdir: Path | None = None, timeout: float | None = None, warmup: int = 0) -> dict:
-    exe = REF2D if dim == 2 else REF3D
+                  workdir: Path | None = None, timeout: float | None = None, warmup: int = 0,
+                  backend: str = "cpu") -> dict:
+    """Run the reference solver built from its sources: its CPU loops, or (2D, backend="cuda")
+    its own CUDA engine."""
+    exe = REF2D_CUDA if backend == "cuda" else REF2D if dim == 2 else REF3D
     if not exe.exists():
-        raise FileNotFoundError(f"{exe} is not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{exe} is not built (make -C oracle ref ref-cuda)")
     tmp = None
     if workdir is None:
         tmp = tempfile.TemporaryDirectory()
@@ -279,7 +283,7 @@ def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_
     write_case(case, workdir / "case.txt")
     out = workdir / "out"
     proc = subprocess.run([str(exe), str(workdir / "case.txt"), str(out), str(steps), str(threads),
-                           "1" if dump_mesh else "0", str(int(warmup))], capture_output=True, text=True,
+                           "1" if dump_mesh else "0", str(int(warmup)), backend], capture_output=True, text=True,
                           timeout=timeout)
     if proc.returncode != 0:
         raise RuntimeError(f"reference {dim}D run failed ({proc.returncode}): {proc.stderr.strip()}")

@@ -4,7 +4,7 @@
 // float64 files.  Nothing in the product links or runs this program; tests use it as
 // the parity truth and bench.py times it as the reference CPU arm.
 //
-// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps]
+// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps] [cpu|cuda]
 //   steps  : accepted RK4 steps to run (default: the session's total)
 //   threads: ComputeSettings3D::cpuThreads (0 = reference default)
 //
@@ -150,7 +150,7 @@ template <class A> std::vector<double> doubles(const A &a) { return a.toDouble()
 int main(int argc, char **argv) {
     try {
         if (argc < 3) {
-            std::cerr << "usage: ref2d case.txt outdir [steps] [threads] [dump_mesh] [warmup]\n";
+            std::cerr << "usage: ref2d case.txt outdir [steps] [threads] [dump_mesh] [warmup] [cpu|cuda]\n";
             return 2;
         }
         const Case c{readCase(argv[1])};
@@ -162,7 +162,10 @@ int main(int argc, char **argv) {
         Simulation sim;
         std::string error;
         const auto t0 = std::chrono::steady_clock::now();
-        if (!sim.initialize(p, error, BackendKind3D::Cpu, ComputeSettings3D{threads, -1})) {
+        // backend: the reference's CPU loops, or its own CUDA engine (src/two_d/CudaEngine2D.cu) when
+        // this driver is built with SEIS3D_HAS_CUDA
+        const BackendKind3D kind = argc > 7 && std::string(argv[7]) == "cuda" ? BackendKind3D::Cuda : BackendKind3D::Cpu;
+        if (!sim.initialize(p, error, kind, ComputeSettings3D{threads, -1})) {
             std::ofstream(out / "error.txt") << error << '\n';
             std::cerr << "initialize failed: " << error << '\n';
             return 3;
