@@ -144,10 +144,11 @@ __device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__
     return sum / (m.h * ld(m.jac + q) * rho);
 }
 
-// Three CTAs of 256 threads per SM (80 registers).  The kernel waits on its L1/L2 loads, and the
-// extra resident warps hide more of that latency than the ~200 bytes of spills per thread this
-// bound costs: measured at 400x288x200, three CTAs per SM run the stages 1.3x faster than two.
-template <class Real> constexpr int minBlocks3() { return 3; }
+// Four CTAs of 256 threads per SM (64 registers).  The kernel waits on its L1/L2 loads, and the
+// extra resident warps hide more of that latency than the spills this bound costs: measured at
+// 400x288x200, the stages run 1.3x faster with three CTAs per SM than with two, and 1.09x faster
+// again with four.
+template <class Real> constexpr int minBlocks3() { return 4; }
 
 // RK combine, surface projection and stores of the nine rates of one node.
 template <class Real, int STAGE>
