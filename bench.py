@@ -242,7 +242,7 @@ def serving_leg(args, device: int) -> dict:
                          steps_scale=args.serving_steps)
     a0 = reqs[0]["arrival"]
     # batched FP32
-    srv = V.Server(device=device, batch_steps=64)
+    srv = V.Server(device=device, batch_steps=64, build_threads=min(16, os.cpu_count() or 4))
     t0 = time.perf_counter()
     ids = []
     for r in reqs:
@@ -254,6 +254,8 @@ def serving_leg(args, device: int) -> dict:
     st = [srv.status(i) for i in ids]
     failed = [s["error"] for s in st if s["state"] != "done"]
     lat32 = np.array([s["finish_s"] - s["submit_s"] for s in st])
+    build32 = np.array([s["run_s"] - s["start_s"] for s in st])  # host model build + engine creation
+    gpu32 = np.array([s["finish_s"] - s["run_s"] for s in st])   # first batch to last batch
     span32 = max(s["finish_s"] for s in st) - min(s["submit_s"] for s in st)
     rec32 = [srv.records(i) for i in ids]
     stats = srv.stats()
@@ -284,7 +286,8 @@ def serving_leg(args, device: int) -> dict:
                                   f"steps x{args.serving_steps} of the full mix",
         "batched_fp32": {"shots_per_hour": shots / span32 * 3600, "p50_s": float(np.percentile(lat32, 50)),
                          "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32,
-                         "peak_running": stats["peak_running"], "failed": failed},
+                         "peak_running": stats["peak_running"], "failed": failed,
+                         "mean_build_s": float(build32.mean()), "mean_run_s": float(gpu32.mean())},
         "sequential_fp64": {"shots_per_hour": shots / span64 * 3600, "p50_s": float(np.percentile(lat64, 50)),
                             "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64},
         "shots_per_hour_ratio": (shots / span32) / (shots / span64),

@@ -36,6 +36,7 @@ typedef struct swl_shot_status {
     int32_t dim, state, steps_done, total_steps, receivers, pad;
     int64_t samples, resident_bytes;
     double submit_s, start_s, finish_s; /* seconds since the server was created */
+    double run_s;                       /* model built, first batch about to launch (0 before) */
     char error[256];
 } swl_shot_status;
 

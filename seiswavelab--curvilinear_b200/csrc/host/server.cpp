@@ -22,7 +22,7 @@ struct Shot {
     Params3D p3;
     std::unique_ptr<Session2D> s2;
     std::unique_ptr<Session3D> s3;
-    double submit{}, start{}, finish{};
+    double submit{}, start{}, finish{}, run{};
     std::string error;
     int64_t bytes{}; // device bytes charged against the budget
     int steps() const { return dim == 2 ? (s2 ? s2->step : 0) : (s3 ? s3->step : 0); }
@@ -62,6 +62,7 @@ class Server {
         }
         for (int t = 0; t < cfg_.build_threads; ++t) builders_.emplace_back([this] { buildLoop(); });
         loop_ = std::thread([this] { schedule(); });
+        reaper_ = std::thread([this] { reapLoop(); });
     }
     ~Server() {
         {
@@ -71,8 +72,10 @@ class Server {
         cvBuild_.notify_all();
         cvWork_.notify_all();
         cvDone_.notify_all();
+        cvReap_.notify_all();
         for (auto &t : builders_) t.join();
         loop_.join();
+        reaper_.join();
     }
     int64_t submit(std::shared_ptr<Shot> s) {
         std::lock_guard<std::mutex> g(mu_);
@@ -88,6 +91,7 @@ class Server {
         const auto s = find(id);
         swl_shot_status o{};
         o.id = id, o.dim = s->dim, o.state = s->state, o.submit_s = s->submit, o.start_s = s->start, o.finish_s = s->finish;
+        o.run_s = s->run;
         o.resident_bytes = s->bytes;
         if (s->state >= SWL_SHOT_RUNNING || s->state == SWL_SHOT_FAILED) {
             o.steps_done = s->steps(), o.total_steps = s->total();
@@ -145,7 +149,9 @@ class Server {
     int64_t budget_{}, used_{}, peakUsed_{};
     std::chrono::steady_clock::time_point t0_;
     std::mutex mu_;
-    std::condition_variable cvWork_, cvDone_, cvBuild_;
+    std::condition_variable cvWork_, cvDone_, cvBuild_, cvReap_;
+    std::deque<std::shared_ptr<Shot>> reap_; // finished shots whose engines are still to be destroyed
+    std::thread reaper_;
     std::deque<int64_t> queue_, unreported_;
     std::deque<std::shared_ptr<Shot>> toBuild_, built_;
     std::map<int64_t, std::shared_ptr<Shot>> shots_;
@@ -163,11 +169,13 @@ class Server {
         return it->second;
     }
     // caller holds mu_
-    void finishShot(const std::shared_ptr<Shot> &s, int state, const std::string &error) {
+    // `release`: the shot holds no engine, so its reserved bytes are free now (otherwise the reaper
+    // frees them once the engine is destroyed).
+    void finishShot(const std::shared_ptr<Shot> &s, int state, const std::string &error, bool release = true) {
         s->state = state;
         s->error = error;
         s->finish = now();
-        used_ -= s->bytes;
+        if (release) used_ -= s->bytes;
         ++finished_;
         unreported_.push_back(s->id);
         cvDone_.notify_all();
@@ -212,6 +220,23 @@ class Server {
             }
         }
     }
+    void reapLoop() {
+        for (;;) {
+            std::shared_ptr<Shot> s;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                cvReap_.wait(g, [&] { return stop_ || !reap_.empty(); });
+                if (reap_.empty()) return; // stopping, nothing left
+                s = reap_.front();
+                reap_.pop_front();
+            }
+            if (s->s2 && s->s2->engine) swl2d_destroy(s->s2->engine), s->s2->engine = nullptr;
+            if (s->s3 && s->s3->engine) swl3d_destroy(s->s3->engine), s->s3->engine = nullptr;
+            std::lock_guard<std::mutex> g(mu_);
+            used_ -= s->bytes;
+            cvWork_.notify_all();
+        }
+    }
     // Admission in arrival order; caller holds mu_.
     void admit(int running) {
         while (!queue_.empty()) {
@@ -246,6 +271,7 @@ class Server {
                 if (stop_) break;
                 while (!built_.empty()) {
                     built_.front()->state = SWL_SHOT_RUNNING;
+                    built_.front()->run = now();
                     running.push_back(built_.front());
                     built_.pop_front();
                 }
@@ -282,11 +308,13 @@ class Server {
                     finished = true;
                 }
                 if (finished) {
-                    // free the device memory now; the records stay with the shot
-                    if (s->s2 && s->s2->engine) swl2d_destroy(s->s2->engine), s->s2->engine = nullptr;
-                    if (s->s3 && s->s3->engine) swl3d_destroy(s->s3->engine), s->s3->engine = nullptr;
+                    // The records stay with the shot.  Its engine is destroyed by the reaper thread:
+                    // freeing device memory waits for the whole device, which would stall the other
+                    // shots' batches if this loop did it.
                     std::lock_guard<std::mutex> g(mu_);
-                    finishShot(s, error.empty() ? SWL_SHOT_DONE : SWL_SHOT_FAILED, error);
+                    finishShot(s, error.empty() ? SWL_SHOT_DONE : SWL_SHOT_FAILED, error, false);
+                    reap_.push_back(s);
+                    cvReap_.notify_one();
                     running.erase(running.begin() + i);
                     progressed = true;
                     continue;

@@ -21,7 +21,7 @@ class ShotStatus(C.Structure):
     _fields_ = [("id", C.c_int64), ("dim", C.c_int32), ("state", C.c_int32), ("steps_done", C.c_int32),
                 ("total_steps", C.c_int32), ("receivers", C.c_int32), ("pad", C.c_int32), ("samples", C.c_int64),
                 ("resident_bytes", C.c_int64), ("submit_s", C.c_double), ("start_s", C.c_double),
-                ("finish_s", C.c_double), ("error", C.c_char * 256)]
+                ("finish_s", C.c_double), ("run_s", C.c_double), ("error", C.c_char * 256)]
 
 
 class Stats(C.Structure):
