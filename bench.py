@@ -185,6 +185,22 @@ def reference_gpu(params: dict, steps: int, warmup: int) -> dict | None:
     return out
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """The largest value of x over all ranks: a multi-GPU job takes as long as its slowest rank."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(points: int, steps: int, ms: float, world: int) -> float:
+    """Whole-job Mpt-updates/s: each of `world` ranks advances its own shot of `points` nodes by
+    `steps` steps, and the job takes `ms` (the slowest rank's time)."""
+    return world * points * steps / (ms * 1e-3) / 1e6
+
+
 def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
     """Device time of `steps` engine steps on torch's current stream; returns (ms, profile)."""
     L = swl.library()
@@ -328,13 +344,10 @@ def gpu_arm(args):
             sampler.wait_first()  # the sampler is up before the timed region starts
         ms, prof = time_engine(swl, sim, dim, params, args.steps, args.warmup, torch, dist, rank)
         clocks = sampler.stop() if sampler else None
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, "cuda")
         stage_ms = sum(prof["stage_ms"])
         achieved = prof["bytes_per_step"] / (stage_ms * 1e-3) / 1e9
-        res = {"value": world * pts * args.steps / (ms * 1e-3) / 1e6, "ms_per_step": ms / args.steps, "points": pts,
+        res = {"value": job_throughput(pts, args.steps, ms, world), "ms_per_step": ms / args.steps, "points": pts,
                "init_s": init_s, "profile": prof, "desc": desc, "params": params, "clocks": clocks,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                             "traffic": traffic_from_profiles(args.workload, "f64" if precision == 0 else "f32"),
@@ -354,10 +367,7 @@ def gpu_arm(args):
     sim64.advance(args.steps)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     info = sim64.info()
     nrec = info["receivers"]
     e2e = {"value": world * r64["points"] * args.steps / e2e_s / 1e6, "unit": UNIT,
