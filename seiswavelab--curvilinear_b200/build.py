@@ -26,6 +26,10 @@ UNITS = {
     "runtime.cu": [],
     "engine2d_f64.cu": ["--fmad=false"],
     "engine2d_f32.cu": [],
+    # the 2D stage kernels, one unit per (precision, GSLS mechanism count), built in parallel
+    **{f"stages2d.cu@{r}{m}": (["--fmad=false"] if r == "f64" else []) +
+       [f"-DSWL_STAGE_REAL={'double' if r == 'f64' else 'float'}", f"-DSWL_STAGE_MECH={m}"]
+       for r in ("f64", "f32") for m in range(4)},
     "engine3d_f64.cu": ["--fmad=false"],
     "engine3d_f32.cu": [],
     "abi.cpp": ["-x", "cu"],
@@ -53,8 +57,9 @@ def _deps() -> float:
 
 
 def _compile(unit: str, flags: list[str], verbose: bool, newest: float) -> Path:
-    src = SRC / unit
-    obj = OUT / (unit.replace("/", "_") + ".o")
+    # "file@tag" compiles `file` once more under another object name (with its own flags)
+    src = SRC / unit.split("@")[0]
+    obj = OUT / (unit.replace("/", "_").replace("@", "_") + ".o")
     cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
     stamp = obj.with_suffix(".cmd")  # the command an object was built with; a change rebuilds it
     if (obj.exists() and stamp.exists() and stamp.read_text() == " ".join(cmd)

@@ -13,6 +13,7 @@
 #pragma once
 #include "../../include/swl_b200.h"
 #include "runtime.cuh"
+#include "launch2d.cuh"
 #include "stage2d.cuh"
 #include <algorithm>
 #include <cmath>
@@ -55,57 +56,31 @@ std::unique_ptr<Engine2D> makeEngine2D32(const swl_mesh2d &, const int64_t *, in
 
 namespace detail2 {
 
+// Dispatch on the GSLS mechanism count to the separately compiled stage instantiations.
 template <class Real> struct Launch {
-    // Elastic stages run the streaming kernel, GSLS stages the tiled one.
-    template <int DX, int DZ, int MECH, int ST> static void go(dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-        if constexpr (MECH == 0) k2::stream2d<Real, DX, DZ, ST><<<g, b, k2::streamBytes<Real>(), s>>>(a);
-        else k2::stage2d<Real, DX, DZ, MECH, ST><<<g, b, k2::tileBytes<Real>(), s>>>(a);
-    }
-    template <class K> static void allowKernel(K kernel, std::size_t bytes) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)), "2D stage shared memory");
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)),
-              "2D stage shared-memory carveout");
-    }
-    // Opt every instantiation into its dynamic shared memory (above the 48 KB default).
-    template <int DX, int DZ, int MECH, int ST> static void allow() {
-        if constexpr (MECH == 0) allowKernel(k2::stream2d<Real, DX, DZ, ST>, k2::streamBytes<Real>());
-        else allowKernel(k2::stage2d<Real, DX, DZ, MECH, ST>, k2::tileBytes<Real>());
-    }
-    template <int DX, int DZ, int MECH> static void allowStages() {
-        allow<DX, DZ, MECH, 0>(), allow<DX, DZ, MECH, 1>(), allow<DX, DZ, MECH, 2>(), allow<DX, DZ, MECH, 3>();
-    }
-    template <int DX, int DZ> static void allowMech(int mech) {
+    static void stage(int dx, int dz, int mech, int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
         switch (mech) {
-        case 0: allowStages<DX, DZ, 0>(); break;
-        case 1: allowStages<DX, DZ, 1>(); break;
-        case 2: allowStages<DX, DZ, 2>(); break;
-        default: allowStages<DX, DZ, 3>(); break;
+        case 0: launchStage2D<Real, 0>(dx, dz, stage, g, b, s, a); break;
+        case 1: launchStage2D<Real, 1>(dx, dz, stage, g, b, s, a); break;
+        case 2: launchStage2D<Real, 2>(dx, dz, stage, g, b, s, a); break;
+        default: launchStage2D<Real, 3>(dx, dz, stage, g, b, s, a); break;
         }
     }
     static void prepare(int mech) {
-        allowMech<0, 0>(mech), allowMech<0, 1>(mech), allowMech<1, 0>(mech), allowMech<1, 1>(mech);
-    }
-    template <int DX, int DZ, int MECH> static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-        switch (stage) {
-        case 0: go<DX, DZ, MECH, 0>(g, b, s, a); break;
-        case 1: go<DX, DZ, MECH, 1>(g, b, s, a); break;
-        case 2: go<DX, DZ, MECH, 2>(g, b, s, a); break;
-        default: go<DX, DZ, MECH, 3>(g, b, s, a); break;
-        }
-    }
-    template <int DX, int DZ> static void mech(int mech, int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
         switch (mech) {
-        case 0: st<DX, DZ, 0>(stage, g, b, s, a); break;
-        case 1: st<DX, DZ, 1>(stage, g, b, s, a); break;
-        case 2: st<DX, DZ, 2>(stage, g, b, s, a); break;
-        default: st<DX, DZ, 3>(stage, g, b, s, a); break;
+        case 0: prepareStages2D<Real, 0>(); break;
+        case 1: prepareStages2D<Real, 1>(); break;
+        case 2: prepareStages2D<Real, 2>(); break;
+        default: prepareStages2D<Real, 3>(); break;
         }
     }
-    static void stage(int dx, int dz, int mechs, int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-        if (dx == 0 && dz == 0) mech<0, 0>(mechs, stage, g, b, s, a);
-        else if (dx == 0) mech<0, 1>(mechs, stage, g, b, s, a);
-        else if (dz == 0) mech<1, 0>(mechs, stage, g, b, s, a);
-        else mech<1, 1>(mechs, stage, g, b, s, a);
+    static cudaFuncAttributes attributes(int mech) {
+        switch (mech) {
+        case 0: return stageAttributes2D<Real, 0>();
+        case 1: return stageAttributes2D<Real, 1>();
+        case 2: return stageAttributes2D<Real, 2>();
+        default: return stageAttributes2D<Real, 3>();
+        }
     }
 };
 
@@ -150,7 +125,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     bool previous_{false};  // set a_ holds the state before the last step
     int nrec_{}, traceCap_{}, forcingCap_{};
     dim3 grid_, block_{32, 8};                               // one node per thread (diagnostics kernel)
-    dim3 stageGrid_, stageBlock_{32, 8}; // strips x segments (elastic) or 32x32-node tiles (GSLS)
+    dim3 stageGrid_, stageBlock_{32, 8}; // strips of 32 columns x segments of 64 rows
     int nparts_{};
     k2::Clock hostClock_{};
     PinnedBuffer pinnedForcing_, pinnedClock_;
@@ -205,7 +180,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         p.delta = static_cast<Real>(dt_);
         p.partials = nullptr;
         if (k2::kahan<Real>()) p.cin = set_[4 + u_], p.cout = set_[4 + a_], p.pcin = pset_[4 + u_], p.pcout = pset_[4 + a_];
-        if (mech_ == 0) {
+        {
             const int in = stage == 0 ? u_ : stage == 2 ? 3 : 2;
             p.ringMap = ringMap_[in];
             p.uMap = pwMap_[u_];
@@ -411,14 +386,11 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.nz - 6 + block_.y - 1) / block_.y);
-        if (mech_ == 0)
-            stageGrid_ = dim3((g.nx - 6 + k2::SW - 1) / k2::SW, (g.nz - 6 + k2::SB * k2::SEG_BLOCKS - 1) / (k2::SB * k2::SEG_BLOCKS));
-        else
-            stageGrid_ = dim3((g.nx - 6 + k2::TX - 1) / k2::TX, (g.nz - 6 + k2::TZ - 1) / k2::TZ);
+        stageGrid_ = dim3((g.nx - 6 + k2::SW - 1) / k2::SW, (g.nz - 6 + k2::SB * k2::SEG_BLOCKS - 1) / (k2::SB * k2::SEG_BLOCKS));
         nparts_ = grid_.x * grid_.y;
         partials_.allocate(std::max<std::size_t>(nparts_, stageGrid_.x * stageGrid_.y) * sizeof(k2::Partial));
         detail2::Launch<Real>::prepare(mech_);
-        if (mech_ == 0) {
+        {
             const bool f64 = sizeof(Real) == 8;
             const uint64_t d5[3] = {uint64_t(pitch_), uint64_t(nz_), 5}, d6[3] = {uint64_t(pitch_), uint64_t(nz_), 6};
             const uint64_t st[2] = {uint64_t(pitch_) * sizeof(Real), uint64_t(n) * sizeof(Real)};
@@ -434,9 +406,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         pinnedClock_.reserve(sizeof(k2::Clock));
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
-        cudaFuncAttributes attr{};
-        if (mech_ == 0) check(cudaFuncGetAttributes(&attr, k2::stream2d<Real, 0, 0, 1>), "2D kernel compatibility");
-        else check(cudaFuncGetAttributes(&attr, k2::stage2d<Real, 0, 0, 1, 1>), "2D kernel compatibility");
+        const cudaFuncAttributes attr = detail2::Launch<Real>::attributes(mech_);
         registers_ = attr.numRegs;
         localBytes_ = attr.localSizeBytes;
     }

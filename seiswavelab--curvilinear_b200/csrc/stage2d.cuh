@@ -4,12 +4,10 @@
 // fields (Vx, Vz, Sxx, Szz, Sxz), the metric-transformed right-hand side
 // (src/two_d/PointKernels2D.hpp:121-172) with the traction-image surface rows, CFS-PML ADE
 // memories and GSLS relaxation, and immediately its part of the RK combine and the
-// free-surface projection -- the rates never touch HBM.  Two kernel shapes share that node code:
-//   stream2d (elastic): a CTA walks a 32-column strip down 64 rows, 8 rows at a time, with
-//     every operand (a ring of stencil rows, U, A and the model words) staged in shared memory
-//     by asynchronous copies one row block ahead of the arithmetic;
-//   stage2d (GSLS): a CTA stages a 32x32 tile plus a 3-node halo of the stencil fields and
-//     reads the per-node words (6 + 4L fields) from global memory.
+// free-surface projection -- the rates never touch HBM.  A CTA walks a 32-column strip down 64
+// rows, 8 rows at a time, with the five stencil fields (a ring of rows), U, A and the model words
+// staged in shared memory by tensor copies one row block ahead of the arithmetic; the GSLS
+// fields (Syy and the memories, index >= 5) and strengths are read from global memory per node.
 // Three state sets stay resident beside the stage outputs:
 //   U (state at the start of the step), A (running RK accumulator), S (stage state).
 // Stage 0 writes A = k1 and S = U + dt/2 k1; stages 1-2 add 2k to A and write
@@ -142,31 +140,9 @@ template <class Real> __device__ __forceinline__ Real divBy(Real x, Real d, Real
 // ------------------------------------------------------------- node sources
 // The node arithmetic reads its operands through a source: the five stencil fields of the
 // stage input at (dx, dz) from the node, the start-of-step state U and the RK accumulator A of
-// the node, and its model words.  TileNode serves the tiled kernel (taps staged in shared
-// memory, the other words read from global memory); StreamNode serves the streaming kernel
-// (every word staged in shared memory one row block ahead of use).  `exact`: h is a power of
-// two, so x/h is formed as x*(1/h) -- the same value -- and no division is compiled in.
-constexpr int TX = 32, TZ = 32, HX = TX + 6, HZ = TZ + 6; // tile and halo'd tile
-constexpr int TILE_THREADS = 256, ROWS_PER_THREAD = TZ / (TILE_THREADS / TX);
-template <class Real> constexpr std::size_t tileBytes() { return sizeof(Real) * 5 * HZ * HX; }
-
-template <class Real, bool EXACT> struct TileNode {
-    static constexpr bool exact = EXACT;
-    const Real *c; // centre element of field 0 in the tile
-    long long q, n;
-    int stage0;    // stage 0 reads U from the tile (U is the stage input)
-    __device__ __forceinline__ Real at(int f, int dx, int dz) const { return c[f * (HZ * HX) + dz * HX + dx]; }
-    __device__ __forceinline__ Real u(const StageArgs<Real> &p, int f) const { return stage0 ? at(f, 0, 0) : ld(p.base + f * n + q); }
-    __device__ __forceinline__ Real acc(const StageArgs<Real> &p, int f) const { return p.acc[f * n + q]; }
-    __device__ __forceinline__ Real comp(const StageArgs<Real> &p, int f) const { return p.cin[f * n + q]; }
-    __device__ __forceinline__ Real a(const Mesh<Real> &m) const { return ld(m.a + q); }
-    __device__ __forceinline__ Real b(const Mesh<Real> &m) const { return ld(m.b + q); }
-    __device__ __forceinline__ Real lam(const Mesh<Real> &m) const { return ld(m.lambda + q); }
-    __device__ __forceinline__ Real mu(const Mesh<Real> &m) const { return ld(m.mu + q); }
-    __device__ __forceinline__ Real rho(const Mesh<Real> &m) const { return ld(m.rho + q); }
-    __device__ __forceinline__ Real jac(const Mesh<Real> &m) const { return ld(m.jac + q); }
-};
-
+// the node, and its model words.  StreamNode serves the streaming kernel (every word staged in
+// shared memory one row block ahead of use).  `exact`: h is a power of two, so x/h is formed as
+// x*(1/h) -- the same value; otherwise the correctly rounded divBy.
 // Streaming geometry: a CTA owns a strip of SW node columns and a segment of SB*SEG_BLOCKS
 // node rows, and walks down the segment one block of SB rows (one row per warp) at a time.
 // Shared memory holds a ring of three chunks of SB stencil rows (five fields, SW + 8 columns:
@@ -585,6 +561,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
     }
 }
 
+constexpr int TILE_THREADS = 256; // threads of a stage CTA (8 warps)
+
 // Block reduction of the per-thread diagnostics into one partial per CTA (256 threads).
 __device__ __forceinline__ void reducePartial(Partial s, Partial *out, int slot) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -610,55 +588,7 @@ __device__ __forceinline__ void reducePartial(Partial s, Partial *out, int slot)
     }
 }
 
-// ------------------------------------------------------------- tiled stage (GSLS)
-// CTAs per SM the register allocation must allow: three FP64 tiles (3 x 57.8 KB of shared
-// memory) or four FP32 tiles.  Fewer resident CTAs leave the memory system idle (measured:
-// one FP64 CTA per SM runs at half the throughput of three).
-// GSLS nodes carry 6 + 4L fields, so they get one CTA fewer instead of spilling.
-template <class Real, int MECH> constexpr int minBlocks() { return (sizeof(Real) == 8 ? 3 : 4) - (MECH ? 1 : 0); }
-
-template <class Real, int DX, int DZ, int MECH, int STAGE, bool EXACT>
-__device__ __forceinline__ void tileBody(const StageArgs<Real> &p, Real *tile) {
-    const Mesh<Real> &m = p.m;
-    const int i0 = 3 + blockIdx.x * TX, k0 = 3 + blockIdx.y * TZ;
-    const int tid = threadIdx.x + TX * threadIdx.y;
-    const long long n = m.count;
-    // stage the halo'd tile of the five stencil fields (rows of HX, x fastest)
-    for (int e = tid; e < 5 * HZ * HX; e += TILE_THREADS) {
-        const int f = e / (HZ * HX), r = e - f * (HZ * HX), zz = r / HX, xx = r - zz * HX;
-        const int gi = i0 - 3 + xx, gk = k0 - 3 + zz;
-        if (gi < m.nx && gk < m.nz) cpAsync(tile + e, p.in + f * n + gi + m.xoff + (long long)m.pitch * gk, int(sizeof(Real)));
-    }
-    cpAsyncCommit();
-    cpAsyncWaitAll();
-    __syncthreads();
-    Partial diag{0, 0, 0, 0, 0};
-    const bool withDiag = STAGE == 3 && p.partials != nullptr;
-#pragma unroll 1
-    for (int j = 0; j < ROWS_PER_THREAD; ++j) {
-        const int lz = threadIdx.y + (TILE_THREADS / TX) * j;
-        const int i = i0 + threadIdx.x, k = k0 + lz;
-        if (i < m.nx - 3 && k < m.nz - 3) {
-            const TileNode<Real, EXACT> t{tile + (lz + 3) * HX + threadIdx.x + 3, i + m.xoff + (long long)m.pitch * k, n, STAGE == 0};
-            stageNode<Real, DX, DZ, MECH, STAGE, true>(p, t, i, k, diag, withDiag);
-        }
-    }
-    if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
-}
-
-// The fused tiled stage.  DX/DZ: MacCormack directions of this (step, stage); MECH: GSLS
-// mechanisms; STAGE: 0..3.  Block 32x8, tile 32x32 nodes (4 per thread).
-template <class Real, int DX, int DZ, int MECH, int STAGE>
-__global__ void __launch_bounds__(TILE_THREADS, (minBlocks<Real, MECH>())) stage2d(const __grid_constant__ StageArgs<Real> p) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    if (p.clock->faulted) return; // uniform across the grid
-    Real *tile = reinterpret_cast<Real *>(smemRaw);
-    if constexpr (sizeof(Real) == 4) tileBody<Real, DX, DZ, MECH, STAGE, true>(p, tile);
-    else if (p.m.hinvExact) tileBody<Real, DX, DZ, MECH, STAGE, true>(p, tile);
-    else tileBody<Real, DX, DZ, MECH, STAGE, false>(p, tile);
-}
-
-// ------------------------------------------------------------- streaming stage (elastic)
+// ------------------------------------------------------------- streaming stage
 // A CTA walks its strip down one block of 8 rows at a time.  One thread issues tensor copies;
 // group g (ring chunk g + 1 -- chunks 0 and 1 for g = 0 -- and the U, A and model words of block
 // g) completes on mbarrier g & 1.  While the CTA evaluates block b from shared memory, group b+1
@@ -707,7 +637,7 @@ template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<R
     return !(pml || surface || source || sponge);
 }
 
-template <class Real, int DX, int DZ, int STAGE, bool EXACT, bool FULL>
+template <class Real, int DX, int DZ, int MECH, int STAGE, bool EXACT, bool FULL>
 __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw) {
     constexpr int T = STREAM_THREADS, PW = pwWords<Real>();
     constexpr unsigned S = sizeof(Real);
@@ -762,7 +692,7 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
             s.q = i + m.xoff + (long long)m.pitch * k;
             const int c = SB * (blk % 3) + wy + 3; // ring row of row k (rows counted from zb)
             s.centre = c >= RING ? c - RING : c;
-            stageNode<Real, DX, DZ, 0, STAGE, FULL>(p, s, i, k, diag, withDiag);
+            stageNode<Real, DX, DZ, MECH, STAGE, FULL>(p, s, i, k, diag, withDiag);
         }
         __syncthreads(); // block blk's ring chunk and word buffer are free
         if (tid == 0 && blk + 2 < blocks) issue(blk + 2);
@@ -778,8 +708,9 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
     if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
 }
 
-// The streaming elastic stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.
-template <class Real, int DX, int DZ, int STAGE>
+// The streaming stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.  DX/DZ:
+// MacCormack directions of this (step, stage); MECH: GSLS mechanisms (0: elastic); STAGE: 0..3.
+template <class Real, int DX, int DZ, int MECH, int STAGE>
 __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream2d(const __grid_constant__ StageArgs<Real> p) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     if (p.clock->faulted) return; // uniform across the grid
@@ -789,14 +720,14 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream
     Real *pw = ring + CHUNKS * CH;
     const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * SEG_BLOCKS));
     if constexpr (sizeof(Real) == 4) {
-        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, true, true>(p, bar, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw);
     } else if (p.m.hinvExact) {
-        if (interior) streamBody<Real, DX, DZ, STAGE, true, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, true, true>(p, bar, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw);
     } else {
-        if (interior) streamBody<Real, DX, DZ, STAGE, false, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, STAGE, false, true>(p, bar, ring, pw);
+        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, false, false>(p, bar, ring, pw);
+        else streamBody<Real, DX, DZ, MECH, STAGE, false, true>(p, bar, ring, pw);
     }
 }
 
