@@ -150,6 +150,20 @@ swl_status swl2d_set_stream(swl2d_engine *engine, void *cuda_stream);
  * the reference (it reads traces back every step). */
 swl_status swl2d_reserve(swl2d_engine *engine, int32_t steps);
 
+/* FP64 node geometry of the 2D terrain-following map (src/two_d/CurvilinearSolver2D.cpp:344-361),
+ * built on the GPU: coordinates (2 per node), metric_a, metric_b, jacobian and normals (2 per
+ * node) of the padded nx x nz grid (x fastest), written to host arrays, and the smallest
+ * Jacobian and largest metric norm sqrt(1 + a^2 + b^2) over the physical nodes for the dt plan.
+ * `surface` holds the surface height and slope of each padded column. */
+typedef struct swl_geometry2d {
+    int32_t nx, nz, ghost, offset_x; /* padded grid, ghost width, storage columns before the model */
+    double spacing, flatten_depth;
+    const double *surface;           /* 2 * nx values: (height, slope) per column */
+} swl_geometry2d;
+swl_status swl2d_build_geometry(const swl_geometry2d *geometry, int32_t device, double *coordinates, double *metric_a,
+                                double *metric_b, double *jacobian, double *normals, double *min_jacobian,
+                                double *max_metric);
+
 /* A 2D FP64 state held in caller-owned device memory (padded nx x nz grid, x fastest). */
 typedef struct swl_state2d_view {
     int32_t nx, nz;                             /* padded node counts */

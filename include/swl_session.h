@@ -39,6 +39,7 @@ typedef struct swl_params2d {
     int32_t imported_surface, n_surface;
     double surface_datum;
     const double *surface_xz; /* n_surface pairs (x, elevation) */
+    int32_t device_geometry;  /* 1: build the FP64 node geometry on the session's GPU (swl2d_build_geometry) */
 } swl_params2d;
 
 typedef struct swl_info2d {

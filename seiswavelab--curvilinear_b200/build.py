@@ -34,6 +34,7 @@ UNITS = {
     "engine3d_f32.cu": [],
     "abi.cpp": ["-x", "cu"],
     "noalloc.cu": ["--fmad=false"],
+    "geometry.cu": ["--fmad=false"],
     # C++20 host: model construction and sessions (no FMA on the host either, as in the reference)
     "host/gsls.cpp": [],
     "host/model2d.cpp": [],

@@ -62,6 +62,10 @@ struct Params2D {
     bool importedSurface{};
     double surfaceDatum{};
     std::vector<std::array<double, 2>> surfaceSamples;
+    // FP64 node geometry (coordinates, metrics, Jacobian, normals) built on this CUDA device
+    // (-1: the largest) instead of on the host; not part of the reference's Parameters.
+    bool deviceGeometry{false};
+    int geometryDevice{-1};
     std::vector<Layer2D> layers{{20, 1500, 700, 2050, 100, 60}, {50, 2500, 1300, 2250, 100, 60}, {0, 4000, 2300, 2650, 100, 60}};
 };
 

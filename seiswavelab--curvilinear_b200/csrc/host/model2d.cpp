@@ -3,6 +3,7 @@
 // sponge / CFS-PML profiles, source kernel and moment pattern, dt plan, receivers).  The
 // arithmetic follows the reference expression by expression so the arrays are identical.
 #include "model.hpp"
+#include "../../../include/swl_b200.h"
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -160,27 +161,42 @@ Model2D buildModel2D(const Params2D &requested) {
         g.qp.assign(count, 0), g.qs.assign(count, 0);
         for (int l = 0; l < L; ++l) g.deltaP[l].assign(count, 0), g.deltaS[l].assign(count, 0);
     }
+    if (p.deviceGeometry) { // the per-node geometry below, computed on the GPU
+        std::vector<double> columns(2 * std::size_t(g.nx));
+        for (int i = 0; i < g.nx; ++i) columns[2 * i] = surface[i][0], columns[2 * i + 1] = surface[i][1];
+        const swl_geometry2d geo{g.nx, g.nz, ghost, offsetX, p.spacing, g.flattenDepth, columns.data()};
+        double minJ = 0, maxM = 0;
+        if (swl2d_build_geometry(&geo, p.geometryDevice, g.coordinates.data(), g.metricA.data(), g.metricB.data(),
+                                 g.jacobian.data(), g.normals.data(), &minJ, &maxM) != SWL_OK)
+            throw std::runtime_error(swl_last_error());
+    }
     g.minJacobian = std::numeric_limits<double>::max();
     double maxVp = 0, minVs = std::numeric_limits<double>::max(), maxSigma = 0;
     for (int k = 0; k < g.nz; ++k)
         for (int i = 0; i < g.nx; ++i) {
             const auto q = index(i, k);
-            const double x = (i - ghost - offsetX) * p.spacing, eta = (k - ghost) * p.spacing,
-                         t = std::clamp(eta / g.flattenDepth, 0.0, 1.0);
-            // ninth-order blend with four vanishing derivatives at both ends
-            const double fade = 1 - std::pow(t, 5) * (126 + t * (-420 + t * (540 + t * (-315 + 70 * t))));
-            const double fadeDerivative =
-                eta > 0 && eta < g.flattenDepth ? -630 * std::pow(t, 4) * std::pow(1 - t, 4) / g.flattenDepth : 0;
-            const double zx = surface[i][1] * fade, j = 1 + surface[i][0] * fadeDerivative;
+            const double eta = (k - ghost) * p.spacing;
+            double j;
+            if (p.deviceGeometry) {
+                j = g.jacobian[q];
+            } else {
+                const double x = (i - ghost - offsetX) * p.spacing, t = std::clamp(eta / g.flattenDepth, 0.0, 1.0);
+                // ninth-order blend with four vanishing derivatives at both ends
+                const double fade = 1 - std::pow(t, 5) * (126 + t * (-420 + t * (540 + t * (-315 + 70 * t))));
+                const double fadeDerivative =
+                    eta > 0 && eta < g.flattenDepth ? -630 * std::pow(t, 4) * std::pow(1 - t, 4) / g.flattenDepth : 0;
+                const double zx = surface[i][1] * fade;
+                j = 1 + surface[i][0] * fadeDerivative;
+                g.coordinates[2 * q] = x;
+                g.coordinates[2 * q + 1] = eta + surface[i][0] * fade;
+                g.metricA[q] = -zx / j;
+                g.metricB[q] = 1 / j;
+                g.jacobian[q] = j;
+                const double n = std::hypot(zx, 1.0);
+                g.normals[2 * q] = -zx / n;
+                g.normals[2 * q + 1] = 1 / n;
+            }
             require(j > 1e-9 && std::isfinite(j), "Nonpositive curvilinear Jacobian.");
-            g.coordinates[2 * q] = x;
-            g.coordinates[2 * q + 1] = eta + surface[i][0] * fade;
-            g.metricA[q] = -zx / j;
-            g.metricB[q] = 1 / j;
-            g.jacobian[q] = j;
-            const double n = std::hypot(zx, 1.0);
-            g.normals[2 * q] = -zx / n;
-            g.normals[2 * q + 1] = 1 / n;
             double vp = p.vp, vs = p.vs, rho = p.density;
             std::size_t materialIndex = 0;
             if (p.layered) {

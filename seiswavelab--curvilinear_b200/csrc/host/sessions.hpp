@@ -82,6 +82,10 @@ struct Session2D {
     }
     void create(int device) {
         const auto t0 = std::chrono::steady_clock::now();
+        if (params.deviceGeometry) {
+            if (device == SWL_MODEL_ONLY) throw Failure(SWL_ERR_INVALID, "device geometry needs a CUDA device");
+            params.geometryDevice = device;
+        }
         model = buildModel2D(params);
         clearRecords();
         if (device != SWL_MODEL_ONLY) {
@@ -217,6 +221,7 @@ inline Params2D toParams(const swl_params2d &c) {
     p.importedSurface = c.imported_surface != 0, p.surfaceDatum = c.surface_datum;
     if (c.n_surface < 0 || (c.n_surface && !c.surface_xz)) throw std::runtime_error("Invalid surface sample list.");
     for (int i = 0; i < c.n_surface; ++i) p.surfaceSamples.push_back({c.surface_xz[2 * i], c.surface_xz[2 * i + 1]});
+    p.deviceGeometry = c.device_geometry != 0;
     return p;
 }
 

@@ -39,7 +39,7 @@ class Params2D(C.Structure):
         ("attenuation", C.c_int32), ("mechanisms", C.c_int32),
         *[(k, C.c_double) for k in ("q_min_frequency", "q_max_frequency", "q_reference_frequency", "qp", "qs")],
         ("imported_surface", C.c_int32), ("n_surface", C.c_int32), ("surface_datum", C.c_double),
-        ("surface_xz", _dp),
+        ("surface_xz", _dp), ("device_geometry", C.c_int32),
     ]
 
 
@@ -137,6 +137,7 @@ _MAP2D = {
     "attenuation": "attenuation", "mechanisms": "mechanisms", "qMinFrequency": "q_min_frequency",
     "qMaxFrequency": "q_max_frequency", "qReferenceFrequency": "q_reference_frequency", "qp": "qp", "qs": "qs",
     "importedSurface": "imported_surface", "surfaceDatum": "surface_datum",
+    "deviceGeometry": "device_geometry",
 }
 _MAP3D = {
     "precision": "precision", "nx": "nx", "ny": "ny", "nz": "nz", "spacing": "spacing", "vp": "vp", "vs": "vs",
