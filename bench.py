@@ -83,6 +83,39 @@ def measured_hbm_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+class UtilSampler:
+    """nvidia-smi GPU utilization (percent of time a kernel was running) every 100 ms."""
+
+    def __init__(self, gpu: int):
+        self.gpu, self.values, self.proc, self.thread = gpu, [], None, None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", "--query-gpu=utilization.gpu",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+
+        def read():
+            for line in self.proc.stdout:
+                try:
+                    self.values.append(float(line.strip()))
+                except ValueError:
+                    pass
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+        return self
+
+    def stop(self) -> float | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        return float(np.mean(self.values)) if self.values else None
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -259,6 +292,7 @@ def serving_leg(args, device: int) -> dict:
     a0 = reqs[0]["arrival"]
     # batched FP32
     srv = V.Server(device=device, batch_steps=64, build_threads=min(16, os.cpu_count() or 4))
+    util = UtilSampler(device).start()
     t0 = time.perf_counter()
     ids = []
     for r in reqs:
@@ -267,6 +301,7 @@ def serving_leg(args, device: int) -> dict:
             time.sleep(delay)
         ids.append(srv.submit(dict(r["params"], precision=1), r["dim"]))
     srv.drain()
+    util32 = util.stop()
     st = [srv.status(i) for i in ids]
     failed = [s["error"] for s in st if s["state"] != "done"]
     lat32 = np.array([s["finish_s"] - s["submit_s"] for s in st])
@@ -276,15 +311,22 @@ def serving_leg(args, device: int) -> dict:
     rec32 = [srv.records(i) for i in ids]
     stats = srv.stats()
     srv.close()
-    # sequential plain FP64 (same requests, arrival order, one at a time)
-    service, rec64 = [], []
-    for r in reqs:
-        t = time.perf_counter()
-        sim = (S.Simulation2D if r["dim"] == 2 else S.Simulation3D)(dict(r["params"], precision=0), device=device)
-        sim.advance(sim.info()["total_steps"])
-        rec64.append(sim.records())
-        del sim
-        service.append(time.perf_counter() - t)
+    # sequential (same requests, arrival order, one at a time): plain FP64 and, to separate the
+    # precision's share of the gain from the batching's, FP32
+    def sequential(precision):
+        service, records, init = [], [], []
+        u = UtilSampler(device).start()
+        for r in reqs:
+            t = time.perf_counter()
+            sim = (S.Simulation2D if r["dim"] == 2 else S.Simulation3D)(dict(r["params"], precision=precision), device=device)
+            init.append(time.perf_counter() - t)
+            sim.advance(sim.info()["total_steps"])
+            records.append(sim.records())
+            del sim
+            service.append(time.perf_counter() - t)
+        return service, records, float(np.sum(init)), u.stop()
+    service, rec64, init64, util64 = sequential(0)
+    service32, _, init32, util32s = sequential(1)
     finish, lat64, clock = [], [], 0.0
     for r, s in zip(reqs, service):
         start = max(clock, r["arrival"] - a0)
@@ -303,9 +345,12 @@ def serving_leg(args, device: int) -> dict:
         "batched_fp32": {"shots_per_hour": shots / span32 * 3600, "p50_s": float(np.percentile(lat32, 50)),
                          "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32,
                          "peak_running": stats["peak_running"], "failed": failed,
-                         "mean_build_s": float(build32.mean()), "mean_run_s": float(gpu32.mean())},
+                         "mean_build_s": float(build32.mean()), "mean_run_s": float(gpu32.mean()),
+                         "gpu_util_pct": util32},
         "sequential_fp64": {"shots_per_hour": shots / span64 * 3600, "p50_s": float(np.percentile(lat64, 50)),
-                            "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64},
+                            "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64,
+                            "sum_init_s": init64, "gpu_util_pct": util64},
+        "sequential_fp32": {"sum_service_s": float(np.sum(service32)), "sum_init_s": init32, "gpu_util_pct": util32s},
         "shots_per_hour_ratio": (shots / span32) / (shots / span64),
         "max_trace_rel_l2_fp32_vs_fp64": max(errs), "median_trace_rel_l2_fp32_vs_fp64": float(np.median(errs)),
     }
