@@ -164,6 +164,20 @@ swl_status swl2d_build_geometry(const swl_geometry2d *geometry, int32_t device, 
                                 double *metric_b, double *jacobian, double *normals, double *min_jacobian,
                                 double *max_metric);
 
+/* FP64 node geometry of the 3D terrain-following map (src/three_d/CurvilinearSolver.cpp:146-190,
+ * :330-364), built on the GPU: coordinates (3 per node), metrics (9 per node,
+ * d(xi,eta,zeta)/d(x,y,z) row-major), jacobian and the top-row normals (3 per node) of the padded
+ * nx x ny x nz grid (x fastest), plus the smallest Jacobian and the largest metric norm over the
+ * physical nodes.  `surface` holds the terrain displacement of each padded (i, j) column. */
+typedef struct swl_geometry3d {
+    int32_t nx, ny, nz, ghost;
+    double spacing, dz, flatten_depth;
+    int32_t terrain;           /* 0: flat (identity metrics) */
+    const double *surface;     /* nx * ny values, x fastest */
+} swl_geometry3d;
+swl_status swl3d_build_geometry(const swl_geometry3d *geometry, int32_t device, double *coordinates, double *metrics,
+                                double *jacobian, double *normals, double *min_jacobian, double *max_metric_norm);
+
 /* A 2D FP64 state held in caller-owned device memory (padded nx x nz grid, x fastest). */
 typedef struct swl_state2d_view {
     int32_t nx, nz;                             /* padded node counts */

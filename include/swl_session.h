@@ -97,6 +97,7 @@ typedef struct swl_params3d {
         receiver_stride_x, receiver_stride_y, receiver_limit;
     int32_t absorbing, absorbing_cells[3];
     double absorbing_strength;
+    int32_t device_geometry; /* 1: build the FP64 node geometry on the session's GPU (swl3d_build_geometry) */
 } swl_params3d;
 
 typedef struct swl_info3d {

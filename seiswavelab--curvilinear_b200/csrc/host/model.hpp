@@ -139,6 +139,9 @@ struct Params3D {
     std::array<int, 3> absorbingCells{8, 6, 8};
     double absorbingStrength{3};
     int receiverLimit{1024}; // the reference caps traces at 1024; the engine has no such limit
+    // FP64 node geometry built on this CUDA device (-1: the largest) instead of on the host
+    bool deviceGeometry{false};
+    int geometryDevice{-1};
 };
 struct Model3D {
     int nx{}, ny{}, nz{};

@@ -2,6 +2,7 @@
 // part of CpuSimulation3D::initialize (src/three_d/CurvilinearSolver.cpp:117-190, 258-442) with the
 // helpers of include/Seis3D/{AbsorbingBoundary3D,TimeStepPlan3D,MaterialModels3D,ReceiverGeometry3D}.hpp.
 #include "model.hpp"
+#include "../../../include/swl_b200.h"
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -125,6 +126,22 @@ Model3D buildModel3D(const Params3D &p) {
     g.metrics.assign(9 * count, 0);
     g.jacobian.assign(count, 0);
     g.normals.assign(3 * count, 0);
+    if (p.deviceGeometry) { // the node geometry below, computed on the GPU from the surface per column
+        std::vector<double> columns(terrain ? plane : 1, 0.0);
+        if (terrain)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const double x = (i - ghost) * p.spacing, y = (j - ghost) * p.spacing;
+                    const double phaseX = 2.0 * kPi * x / p.wavelength, phaseY = 2.0 * kPi * y / p.wavelength;
+                    columns[i + std::size_t(nx) * j] =
+                        p.surfaceGrid.empty() ? p.relief * std::cos(phaseX) * std::cos(phaseY) : p.surfaceGrid.displacement(x, y);
+                }
+        const swl_geometry3d geo{nx, ny, nz, ghost, p.spacing, dz, ttd, terrain ? 1 : 0, columns.data()};
+        double minJ = 0, maxM = 0;
+        if (swl3d_build_geometry(&geo, p.geometryDevice, g.coordinates.data(), g.metrics.data(), g.jacobian.data(),
+                                 g.normals.data(), &minJ, &maxM) != SWL_OK)
+            throw std::runtime_error(swl_last_error());
+    } else {
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i) {
@@ -174,6 +191,7 @@ Model3D buildModel3D(const Params3D &p) {
                     for (int c = 0; c < 3; ++c) g.normals[3 * q + c] = n[c];
                 }
             }
+    }
     // geometry diagnostics (:330-364)
     g.minJacobian = std::numeric_limits<double>::max();
     double maxMetricNorm = 0;

@@ -246,6 +246,10 @@ struct Session3D {
     }
     void create(int device) {
         const auto t0 = std::chrono::steady_clock::now();
+        if (params.deviceGeometry) {
+            if (device == SWL_MODEL_ONLY) throw Failure(SWL_ERR_INVALID, "device geometry needs a CUDA device");
+            params.geometryDevice = device;
+        }
         model = buildModel3D(params);
         clearRecords();
         if (device != SWL_MODEL_ONLY) {
@@ -368,6 +372,7 @@ inline Params3D toParams(const swl_params3d &c) {
     p.absorbing = c.absorbing != 0;
     for (int a = 0; a < 3; ++a) p.absorbingCells[a] = c.absorbing_cells[a];
     p.absorbingStrength = c.absorbing_strength;
+    p.deviceGeometry = c.device_geometry != 0;
     return p;
 }
 

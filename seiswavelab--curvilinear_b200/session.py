@@ -74,6 +74,7 @@ class Params3D(C.Structure):
                                    "receiver_count_x", "receiver_count_y", "receiver_stride_x", "receiver_stride_y",
                                    "receiver_limit")],
         ("absorbing", C.c_int32), ("absorbing_cells", C.c_int32 * 3), ("absorbing_strength", C.c_double),
+        ("device_geometry", C.c_int32),
     ]
 
 
@@ -146,6 +147,7 @@ _MAP3D = {
     "sourceForce": "source_force", "sourceMoment": "source_moment", "duration": "duration", "maxSteps": "max_steps",
     "cfl": "cfl", "relief": "relief", "wavelength": "wavelength", "flattenDepth": "flatten_depth",
     "absorbing": "absorbing", "absorbingStrength": "absorbing_strength", "receiverLimit": "receiver_limit",
+    "deviceGeometry": "device_geometry",
 }
 
 

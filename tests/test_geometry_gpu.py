@@ -48,3 +48,15 @@ def test_device_geometry_needs_a_device(S, swl):
     case, _, _ = load_2d("sponge_force")
     with pytest.raises(swl.SwlError):
         S.Simulation2D(dict(case, deviceGeometry=1), device=S.MODEL_ONLY)
+
+
+@pytest.mark.parametrize("name", ["moment_layered", "force"])
+def test_device_geometry_3d_matches_reference(name, S):
+    from helpers import fields_3d, load_3d
+    case, res, _ = load_3d(name)
+    sim = S.Simulation3D(dict(case, deviceGeometry=1), device=0)
+    for key in ("metrics", "jacobian", "normals"):
+        assert max_rel(sim.model(key), res[key]) <= GEOMETRY_TOL, key
+    sim.advance(sim.info()["total_steps"])
+    for f in range(9):
+        assert rel_l2(sim.field(f), fields_3d(res)[f]) <= TRACE_TOL, f
