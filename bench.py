@@ -313,20 +313,33 @@ def serving_leg(args, device: int) -> dict:
     srv.close()
     # sequential (same requests, arrival order, one at a time): plain FP64 and, to separate the
     # precision's share of the gain from the batching's, FP32
+    def kind(r):
+        return "3d" if r["dim"] == 3 else "2d_gsls" if r["params"].get("attenuation") else "2d_elastic"
+
     def sequential(precision):
         service, records, init = [], [], []
+        by_kind = {}
         u = UtilSampler(device).start()
         for r in reqs:
             t = time.perf_counter()
             sim = (S.Simulation2D if r["dim"] == 2 else S.Simulation3D)(dict(r["params"], precision=precision), device=device)
             init.append(time.perf_counter() - t)
-            sim.advance(sim.info()["total_steps"])
+            info = sim.info()
+            sim.advance(info["total_steps"])
             records.append(sim.records())
             del sim
             service.append(time.perf_counter() - t)
-        return service, records, float(np.sum(init)), u.stop()
-    service, rec64, init64, util64 = sequential(0)
-    service32, _, init32, util32s = sequential(1)
+            k = by_kind.setdefault(kind(r), {"shots": 0, "init_s": 0.0, "run_s": 0.0, "node_steps": 0.0})
+            nodes = (info["nx"] - 6) * (info["nz"] - 6) * ((info["ny"] - 6) if r["dim"] == 3 else 1)
+            k["shots"] += 1
+            k["init_s"] += init[-1]
+            k["run_s"] += service[-1] - init[-1]
+            k["node_steps"] += nodes * info["total_steps"]
+        for k in by_kind.values():
+            k["mpt_per_s"] = k["node_steps"] / k["run_s"] / 1e6 if k["run_s"] > 0 else None
+        return service, records, float(np.sum(init)), u.stop(), by_kind
+    service, rec64, init64, util64, kinds64 = sequential(0)
+    service32, _, init32, util32s, kinds32 = sequential(1)
     finish, lat64, clock = [], [], 0.0
     for r, s in zip(reqs, service):
         start = max(clock, r["arrival"] - a0)
@@ -349,8 +362,9 @@ def serving_leg(args, device: int) -> dict:
                          "gpu_util_pct": util32},
         "sequential_fp64": {"shots_per_hour": shots / span64 * 3600, "p50_s": float(np.percentile(lat64, 50)),
                             "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64,
-                            "sum_init_s": init64, "gpu_util_pct": util64},
-        "sequential_fp32": {"sum_service_s": float(np.sum(service32)), "sum_init_s": init32, "gpu_util_pct": util32s},
+                            "sum_init_s": init64, "gpu_util_pct": util64, "by_kind": kinds64},
+        "sequential_fp32": {"sum_service_s": float(np.sum(service32)), "sum_init_s": init32, "gpu_util_pct": util32s,
+                            "by_kind": kinds32},
         "shots_per_hour_ratio": (shots / span32) / (shots / span64),
         "max_trace_rel_l2_fp32_vs_fp64": max(errs), "median_trace_rel_l2_fp32_vs_fp64": float(np.median(errs)),
     }
