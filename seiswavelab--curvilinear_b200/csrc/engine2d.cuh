@@ -125,7 +125,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     bool previous_{false};  // set a_ holds the state before the last step
     int nrec_{}, traceCap_{}, forcingCap_{};
     dim3 grid_, block_{32, 8};                               // one node per thread (diagnostics kernel)
-    dim3 stageGrid_, stageBlock_{32, 8}; // strips of 32 columns x segments of 64 rows
+    dim3 stageGrid_, stageBlock_{32, 8}; // strips of 32 columns x segments of 8*seg rows
     int nparts_{};
     k2::Clock hostClock_{};
     PinnedBuffer pinnedForcing_, pinnedClock_;
@@ -386,9 +386,10 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.nz - 6 + block_.y - 1) / block_.y);
-        stageGrid_ = dim3((g.nx - 6 + k2::SW - 1) / k2::SW, (g.nz - 6 + k2::SB * k2::SEG_BLOCKS - 1) / (k2::SB * k2::SEG_BLOCKS));
+        setSegment(k2::MAX_SEG);
         nparts_ = grid_.x * grid_.y;
-        partials_.allocate(std::max<std::size_t>(nparts_, stageGrid_.x * stageGrid_.y) * sizeof(k2::Partial));
+        const std::size_t most = std::size_t(stageGrid_.x) * ((g.nz - 6 + k2::SB - 1) / k2::SB); // one-block segments
+        partials_.allocate(std::max<std::size_t>(nparts_, most) * sizeof(k2::Partial));
         detail2::Launch<Real>::prepare(mech_);
         {
             const bool f64 = sizeof(Real) == 8;
@@ -409,6 +410,31 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         const cudaFuncAttributes attr = detail2::Launch<Real>::attributes(mech_);
         registers_ = attr.numRegs;
         localBytes_ = attr.localSizeBytes;
+        tune();
+    }
+    // Streaming segment length: `seg` row blocks of 8 rows per CTA.
+    void setSegment(int seg) {
+        m_.seg = seg;
+        stageGrid_ = dim3((nx_ - 6 + k2::SW - 1) / k2::SW, (nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg));
+        dropGraphs(); // the graphs hold the launch shape
+    }
+    // The segment length for this grid, picked by timing a few steps per candidate on the fresh
+    // (zero, unforced) state: long segments stream more rows per CTA and re-read fewer halo rows;
+    // short ones put more CTAs in flight and shorten each CTA's chain of row blocks, which is
+    // what a small grid needs.  The state and the clock are reset afterwards.
+    void tune() {
+        swl_profile prof{};
+        profile(0, 1, 1e-6, 10.0, 0.0, prof); // first launches (module load) outside the timing
+        int best = k2::MAX_SEG;
+        double bestMs = 0;
+        for (int seg = k2::MAX_SEG; seg >= 1; seg /= 2) {
+            setSegment(seg);
+            profile(0, 3, 1e-6, 10.0, 0.0, prof);
+            const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
+            if (seg == k2::MAX_SEG || ms < bestMs) best = seg, bestMs = ms;
+        }
+        setSegment(best);
+        reset();
     }
     ~TypedEngine2D() override {
         if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
@@ -580,6 +606,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         check(cudaStreamSynchronize(stream_), "2D clear completion");
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
     }
+    int segment() const { return m_.seg; }
     void diagnostics(swl_diag2d &d) override {
         settle();
         DeviceScope scope(device_);

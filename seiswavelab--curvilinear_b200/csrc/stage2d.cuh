@@ -31,6 +31,7 @@ template <class Real> struct Mesh {
     int nx, nz; // padded
     int pitch, xoff;
     long long count; // pitch * nz: the stride between fields
+    int seg;         // row blocks per streaming segment (chosen per grid by the engine's tuner)
     Real h, hinv;   // hinv = RN(1/h); x/h is x*hinv when h is a power of two (or in FP32),
     int hinvExact;  // else the correctly rounded divBy(x, h, hinv)
     const Real *a, *b, *jac, *normals, *lambda, *mu, *rho, *damping, *source, *sgx, *sgz;
@@ -143,13 +144,14 @@ template <class Real> __device__ __forceinline__ Real divBy(Real x, Real d, Real
 // the node, and its model words.  StreamNode serves the streaming kernel (every word staged in
 // shared memory one row block ahead of use).  `exact`: h is a power of two, so x/h is formed as
 // x*(1/h) -- the same value; otherwise the correctly rounded divBy.
-// Streaming geometry: a CTA owns a strip of SW node columns and a segment of SB*SEG_BLOCKS
-// node rows, and walks down the segment one block of SB rows (one row per warp) at a time.
+// Streaming geometry: a CTA owns a strip of SW node columns and a segment of SB*seg node rows
+// (seg <= MAX_SEG row blocks, picked per grid), and walks down the segment one block of SB rows
+// (one row per warp) at a time.
 // Shared memory holds a ring of three chunks of SB stencil rows (five fields, SW + 8 columns:
 // the strip and four columns either side) and two buffers of the per-node words of a row block.
 // Both are filled by tensor copies, so their layout is the copy box: [chunk][field][row][column]
 // and [word][row][column].
-constexpr int SW = 32, SB = 8, SEG_BLOCKS = 8, CHUNKS = 3, RC = SW + 8, RF = SB * RC, CH = 5 * RF;
+constexpr int SW = 32, SB = 8, MAX_SEG = 8, CHUNKS = 3, RC = SW + 8, RF = SB * RC, CH = 5 * RF;
 constexpr int RING = CHUNKS * SB, STREAM_THREADS = SW * SB;
 enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15, PW_C = 16 };
 // per-node words: U, A, five model words and J, plus the five compensation terms in FP32
@@ -629,7 +631,7 @@ template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
 // strips, the sponge, the source support and the surface rows 3..6).
 template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<Real> &m, int i0, int z0) {
-    const int i1 = i0 + SW, z1 = z0 + SB * SEG_BLOCKS; // exclusive ends
+    const int i1 = i0 + SW, z1 = z0 + SB * m.seg; // exclusive ends
     const bool pml = i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || z1 - 3 > m.nz - 6 - m.wz;
     const bool surface = z0 < 7;
     const bool source = i0 < m.src_i1 && i1 > m.src_i0 && z0 < m.src_k1 && z1 > m.src_k0;
@@ -645,9 +647,9 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
     constexpr unsigned wordBytes = (STAGE > 0 ? 2 * fiveBytes : 0) + modelBytes + (STAGE == 3 && kahan<Real>() ? fiveBytes : 0);
     const Mesh<Real> &m = p.m;
     const int lane = threadIdx.x, wy = threadIdx.y, tid = lane + SW * wy;
-    const int i0 = 3 + blockIdx.x * SW, z0 = 3 + blockIdx.y * (SB * SEG_BLOCKS), zb = z0 - 3;
+    const int i0 = 3 + blockIdx.x * SW, z0 = 3 + blockIdx.y * (SB * m.seg), zb = z0 - 3;
     const int iEnd = m.nx - 3, kEnd = m.nz - 3;
-    const int blocks = min(SEG_BLOCKS, (kEnd - z0 + SB - 1) / SB);
+    const int blocks = min(m.seg, (kEnd - z0 + SB - 1) / SB);
     __shared__ int stop;
     // thread 0: issue copy group g (x of the ring box: node i0 - 4; of the word boxes: node i0)
     auto issue = [&](int g) {
@@ -718,7 +720,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream
     uint64_t *bar = reinterpret_cast<uint64_t *>(base);
     Real *ring = reinterpret_cast<Real *>(base + 128);
     Real *pw = ring + CHUNKS * CH;
-    const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * SEG_BLOCKS));
+    const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * p.m.seg));
     if constexpr (sizeof(Real) == 4) {
         if (interior) streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw);
         else streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw);
