@@ -20,6 +20,8 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace swl {
@@ -421,8 +423,22 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // The segment length for this grid, picked by timing a few steps per candidate on the fresh
     // (zero, unforced) state: long segments stream more rows per CTA and re-read fewer halo rows;
     // short ones put more CTAs in flight and shorten each CTA's chain of row blocks, which is
-    // what a small grid needs.  The state and the clock are reset afterwards.
+    // what a small grid needs.  The state and the clock are reset afterwards.  The choice is kept
+    // per grid shape for the life of the process, so that identical shots always run the same
+    // decomposition (FP32 rounding differs slightly between the interior and the boundary forms
+    // of a node, which the decomposition decides).
     void tune() {
+        static std::mutex mutex;
+        static std::map<std::tuple<int, int, int, int, int, int, int>, int> chosen;
+        const auto key = std::make_tuple(device_, nx_, nz_, mech_, m_.wx, m_.wz, m_.dmp_k1);
+        {
+            std::lock_guard<std::mutex> g(mutex);
+            const auto it = chosen.find(key);
+            if (it != chosen.end()) {
+                setSegment(it->second);
+                return;
+            }
+        }
         swl_profile prof{};
         profile(0, 1, 1e-6, 10.0, 0.0, prof); // first launches (module load) outside the timing
         int best = k2::MAX_SEG;
@@ -431,7 +447,11 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             setSegment(seg);
             profile(0, 3, 1e-6, 10.0, 0.0, prof);
             const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
-            if (seg == k2::MAX_SEG || ms < bestMs) best = seg, bestMs = ms;
+            if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
+        }
+        {
+            std::lock_guard<std::mutex> g(mutex);
+            best = chosen.emplace(key, best).first->second; // a concurrent creation may have decided first
         }
         setSegment(best);
         reset();
