@@ -287,7 +287,12 @@ def serving_leg(args, device: int) -> dict:
     W = importlib.import_module("swl_b200.workloads")
     S = importlib.import_module("swl_b200.session")
     V = importlib.import_module("swl_b200.server")
-    reqs = W.serving_mix(n=args.serving_requests, rate=20.0, seed=5, scale=args.serving_scale,
+    # The full mix arrives at 20 requests/s.  Shrinking every shot by scale^2 (grid) x steps (time)
+    # shrinks the offered work per second by the same factor, so the arrival rate is raised by it:
+    # the scaled stream then loads the GPU as the full stream does (throughput-bound), rather than
+    # leaving it idle between arrivals.
+    rate = args.serving_rate or 20.0 / (args.serving_scale ** 2 * args.serving_steps)
+    reqs = W.serving_mix(n=args.serving_requests, rate=rate, seed=5, scale=args.serving_scale,
                          steps_scale=args.serving_steps)
     a0 = reqs[0]["arrival"]
     # batched FP32
@@ -353,7 +358,8 @@ def serving_leg(args, device: int) -> dict:
         errs.append((num / den) ** 0.5 if den > 0 else 0.0)
     shots = len(reqs)
     return {
-        "requests": shots, "mix": f"seeded (seed 5) Poisson 20/s; 80% 2D elastic/GSLS, 20% 3D; grid edges x{args.serving_scale}, "
+        "requests": shots, "mix": f"seeded (seed 5) Poisson {rate:g}/s (the full mix's 20/s times the work shrink "
+                                  f"factor); 80% 2D elastic/GSLS, 20% 3D; grid edges x{args.serving_scale}, "
                                   f"steps x{args.serving_steps} of the full mix",
         "batched_fp32": {"shots_per_hour": shots / span32 * 3600, "p50_s": float(np.percentile(lat32, 50)),
                          "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32,
@@ -509,6 +515,8 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=48, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")
     ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
+    ap.add_argument("--serving-rate", type=float, default=0.0,
+                    help="arrivals per second (0: 20/s of the full mix scaled by the work shrink factor)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
