@@ -296,7 +296,8 @@ def serving_leg(args, device: int) -> dict:
                          steps_scale=args.serving_steps)
     a0 = reqs[0]["arrival"]
     # batched FP32
-    srv = V.Server(device=device, batch_steps=64, build_threads=min(16, os.cpu_count() or 4))
+    srv = V.Server(device=device, batch_steps=args.serving_batch, max_active=args.serving_active,
+                   build_threads=min(16, os.cpu_count() or 4))
     util = UtilSampler(device).start()
     t0 = time.perf_counter()
     ids = []
@@ -515,6 +516,8 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=48, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")
     ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
+    ap.add_argument("--serving-batch", type=int, default=64, help="steps per batch of a served shot")
+    ap.add_argument("--serving-active", type=int, default=0, help="shots built or running at once (0: memory-bound only)")
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (0: 20/s of the full mix scaled by the work shrink factor)")
     args = ap.parse_args()
