@@ -7,10 +7,9 @@
 // resident and rollback is a role swap (no per-step D2D copy).
 //
 // A batch of steps (swl2d_advance) is recorded once per (step phase mod 8, role parity) into a
-// CUDA graph of eight steps; each step is 4 fused stage kernels.  The last of them also reduces
-// the diagnostics, and its last CTA applies the reference's acceptance rule on the device,
-// records the receivers and advances a device-resident step clock.  The host synchronises once
-// per batch.
+// CUDA graph of eight steps; each step is 4 fused stage kernels + a diagnostics reduction +
+// a one-block verdict that applies the reference's acceptance rule on the device, records the
+// receivers and advances a device-resident step clock.  The host synchronises once per batch.
 #pragma once
 #include "../../include/swl_b200.h"
 #include "runtime.cuh"
@@ -194,24 +193,24 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         return p;
     }
     double dt_{};
-    // Enqueue one step: 4 stages; with `verdict`, stage 3 also reduces the diagnostics and its last
-    // CTA applies the acceptance rule, records the receivers and advances the clock.  Swaps roles.
+    // Enqueue one step: 4 stages (+ diagnostics and verdict when `verdict`).  Swaps roles.
     // `ev`, when given, receives 7 events: before stage 0, after each stage, after stats, after verdict.
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
         if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
         for (int s = 0; s < 4; ++s) {
             auto a = args(s);
-            if (s == 3 && verdict) { // diagnostics and the step verdict fused into stage 3
-                a.partials = partials_.as<k2::Partial>();
-                a.receivers = recIdx_.as<long long>(), a.traces = traces_.as<double>(), a.nrec = nrec_;
-            }
+            if (s == 3 && verdict) a.partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
             detail2::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 2), mech_, s, stageGrid_, stageBlock_, stream_, a);
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
         check(cudaGetLastError(), "2D stage launch");
-        if (verdict && ev) { // the verdict ran inside the last CTA of stage 3
-            check(cudaEventRecord(ev[5], stream_), "record event");
-            check(cudaEventRecord(ev[6], stream_), "record event");
+        if (verdict) {
+            Real *fresh = set_[a_];
+            if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
+            k2::verdict2d<Real><<<1, 1024, 0, stream_>>>(partials_.as<k2::Partial>(), int(stageGrid_.x * stageGrid_.y), fresh, count_,
+                                                         recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>(), 1);
+            if (ev) check(cudaEventRecord(ev[6], stream_), "record event");
+            check(cudaGetLastError(), "2D verdict launch");
         }
         std::swap(u_, a_);
     }
@@ -503,7 +502,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         }
         for (auto &e : ev) cudaEventDestroy(e);
         out.steps = hostClock_.accepted;
-        out.launches_per_step = 4;
+        out.launches_per_step = 5;
         out.bytes_per_step = bytesPerStep();
         const int accepted = hostClock_.accepted;
         u_ = (accepted % 2 == 0) ? u0 : 1 - u0;

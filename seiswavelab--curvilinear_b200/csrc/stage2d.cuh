@@ -55,7 +55,6 @@ struct Clock {
     int fault_step;  // the rejected step
     int trace_steps; // capacity of the trace table in steps
     int stalled;     // set by a stage kernel whose copy wait ran out (the host reports an error)
-    unsigned done;   // CTAs of the current stage-4 launch that have written their partial
     double peak_energy;
     double energy, max_velocity, traction;
     int finite;
@@ -86,14 +85,10 @@ template <class Real> struct StageArgs {
     const Real *pcin;
     Real *pcout;
     const Real *forcing; // 3 values per step of the batch: t, t+dt/2, t+dt
-    Clock *clock;
+    const Clock *clock;
     Real weight;         // dt/2, dt/2, dt for stages 0..2
     Real delta;          // dt
     Partial *partials;   // stage 3: per-CTA diagnostics of the new state (null: none)
-    // stage 3 with partials: the last CTA to finish applies the step's verdict (receivers below)
-    const long long *receivers;
-    double *traces;
-    int nrec;
     // Tensor maps of the streaming kernel (elastic only): the stage input as 40x8x5 boxes,
     // U, A and the compensation terms as 32x8x5 boxes, the model words as 32x8x5 (stages 0-2) or
     // 32x8x6 (stage 3, with J) boxes.
@@ -712,24 +707,7 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
         }
         return;
     }
-    if (withDiag) {
-        reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
-        // The last CTA to finish applies the step's verdict: every CTA publishes its partial, then
-        // takes a ticket; the CTA that draws the last ticket sees all partials and the whole new
-        // state (no waiting: the other CTAs have already finished).
-        __shared__ int lastCta;
-        const unsigned ctas = gridDim.x * gridDim.y;
-        if (tid == 0) {
-            __threadfence();
-            lastCta = atomicAdd(&p.clock->done, 1u) == ctas - 1;
-        }
-        __syncthreads();
-        if (lastCta) {
-            __threadfence();
-            verdictBody(p.partials, int(ctas), static_cast<const Real *>(p.acc), m.count, p.receivers, p.nrec, p.traces, p.clock, 1);
-            if (tid == 0) p.clock->done = 0;
-        }
-    }
+    if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
 }
 
 // The streaming stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.  DX/DZ:
@@ -813,43 +791,42 @@ __global__ void __launch_bounds__(256) stats2d(const Mesh<Real> m, const Real *_
 
 // Reduce the partials, apply the acceptance rule of Simulation::advance
 // (src/two_d/CurvilinearSolver2D.cpp:576-590), record the receivers of an accepted step and
-// advance the clock, with the `threads` threads of one block.  `w` is the new state; it and the
-// partials may have been written by other CTAs of the calling kernel, so they are read through
-// L2 (no read-only cache).
+// advance the clock.  One block.
 template <class Real>
-__device__ __forceinline__ void verdictBody(const Partial *parts, int nparts, const Real *w, long long count,
-                                            const long long *receivers, int nrec, double *traces, Clock *clk, int check) {
-    __shared__ Partial warpSum[32];
+__global__ void __launch_bounds__(1024) verdict2d(const Partial *__restrict__ parts, int nparts, const Real *__restrict__ w,
+                                                  long long count, const long long *__restrict__ receivers, int nrec,
+                                                  double *__restrict__ traces, Clock *clk, int check) {
+    __shared__ Partial sh[1024];
     __shared__ int accept;
-    const int threads = blockDim.x * blockDim.y * blockDim.z;
-    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int t = threadIdx.x;
+    if (clk->faulted) return;
     Partial s{0, 0, 0, 0, 0};
     if (check) {
-        for (int b = t; b < nparts; b += threads) {
-            s.energy += __ldcg(&parts[b].energy);
-            s.velocity = fmax(s.velocity, __ldcg(&parts[b].velocity));
-            s.traction = fmax(s.traction, __ldcg(&parts[b].traction));
-            s.bad |= __ldcg(&parts[b].bad);
+        for (int b = t; b < nparts; b += blockDim.x) {
+            const Partial y = parts[b];
+            s.energy += y.energy;
+            s.velocity = fmax(s.velocity, y.velocity);
+            s.traction = fmax(s.traction, y.traction);
+            s.bad |= y.bad;
         }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        s.energy += __shfl_down_sync(0xffffffffu, s.energy, o);
-        s.velocity = fmax(s.velocity, __shfl_down_sync(0xffffffffu, s.velocity, o));
-        s.traction = fmax(s.traction, __shfl_down_sync(0xffffffffu, s.traction, o));
-        s.bad |= __shfl_down_sync(0xffffffffu, s.bad, o);
-    }
-    if ((t & 31) == 0) warpSum[t >> 5] = s;
+    sh[t] = s;
     __syncthreads();
-    if (t == 0) {
-        for (int wp = 1; wp < threads / 32; ++wp) {
-            s.energy += warpSum[wp].energy;
-            s.velocity = fmax(s.velocity, warpSum[wp].velocity);
-            s.traction = fmax(s.traction, warpSum[wp].traction);
-            s.bad |= warpSum[wp].bad;
+    for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if (t < stride) {
+            Partial &x = sh[t];
+            const Partial y = sh[t + stride];
+            x.energy += y.energy;
+            x.velocity = fmax(x.velocity, y.velocity);
+            x.traction = fmax(x.traction, y.traction);
+            x.bad |= y.bad;
         }
+        __syncthreads();
+    }
+    if (t == 0) {
         int ok = 1;
         if (check) {
-            const Partial tot = s;
+            const Partial tot = sh[0];
             const bool finite = !tot.bad && isfinite(tot.energy);
             const bool growth = (clk->step + 1) * clk->dt > clk->growth_after && clk->peak_energy > 0 &&
                                 tot.energy > clk->peak_energy * 10000;
@@ -874,10 +851,10 @@ __device__ __forceinline__ void verdictBody(const Partial *parts, int nparts, co
     }
     const int row = clk->step - clk->first;
     if (row < clk->trace_steps)
-        for (int r = t; r < nrec; r += threads) {
+        for (int r = t; r < nrec; r += blockDim.x) {
             const long long qq = receivers[r];
-            traces[((long long)row * nrec + r) * 2] = double(__ldcg(w + qq));
-            traces[((long long)row * nrec + r) * 2 + 1] = double(__ldcg(w + count + qq));
+            traces[((long long)row * nrec + r) * 2] = double(w[qq]);
+            traces[((long long)row * nrec + r) * 2 + 1] = double(w[count + qq]);
         }
     __syncthreads();
     if (t == 0) {
@@ -885,7 +862,6 @@ __device__ __forceinline__ void verdictBody(const Partial *parts, int nparts, co
         clk->accepted += 1;
     }
 }
-
 
 // Gathers for sample / probes (CudaEngine2D.cu:79-89).
 template <class Real>
