@@ -139,15 +139,15 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
         if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
         for (int s = 0; s < 4; ++s) {
-            auto a = args(s);
-            if (s == 3 && verdict) a.partials = partials_.as<k3::Partial>(); // diagnostics fused into stage 3
             detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, grid_, block_,
-                                         stream_, a);
+                                         stream_, args(s));
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
         check(cudaGetLastError(), "3D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
+            k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, surfRate_.as<double>(), clock_.as<k2::Clock>(),
+                                                             partials_.as<k3::Partial>());
             if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
             k3::verdict3d<Real><<<1, 512, 0, stream_>>>(partials_.as<k3::Partial>(), nparts_, fresh, count_,
                                                          recIdx_.as<long long>(), nrec_, traces_.as<double>(), clock_.as<k2::Clock>());
@@ -362,7 +362,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         }
         for (auto &e : ev) cudaEventDestroy(e);
         out.steps = hostClock_.accepted;
-        out.launches_per_step = 5;
+        out.launches_per_step = 6;
         out.bytes_per_step = bytesPerStep();
         const int accepted = hostClock_.accepted;
         u_ = (accepted % 2 == 0) ? u0 : 1 - u0;

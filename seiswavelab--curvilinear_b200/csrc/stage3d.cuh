@@ -36,14 +36,6 @@ template <class Real> struct Mesh {
 
 using k2::Clock;
 
-// Per-CTA diagnostics of a state (CurvilinearSolver.cpp:214-250, CudaEngine3D.cu:36-55): energy,
-// peak |v|, the five peaks, the surface traction-rate residual and finiteness.
-struct Partial {
-    double energy, velocity, rateTraction, rateNorm;
-    double peak[5];
-    int bad, pad;
-};
-
 template <class Real> struct StageArgs {
     Mesh<Real> m;
     const Real *in;
@@ -57,7 +49,6 @@ template <class Real> struct StageArgs {
     double *surfRate;    // stage 3: |traction rate| and rate norm per surface node (2 x nx*ny)
     const Real *cin;     // FP32 only: Kahan compensation of U (read) and of the new state (written)
     Real *cout;
-    Partial *partials;   // stage 3: per-CTA diagnostics of the new state (null: none)
 };
 
 using k2::ld;
@@ -160,30 +151,8 @@ __device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__
 template <class Real> constexpr int minBlocks3() { return 4; }
 
 // RK combine, surface projection and stores of the nine rates of one node.
-// Diagnostics of one node of the new state (the per-node part of stats3d below).
-template <class Real> __device__ __forceinline__ void nodeDiag(const Mesh<Real> &m, const Real (&o)[9], long long q, Partial &s) {
-    double f[9];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) f[c] = double(o[c]), s.bad |= int(!isfinite(f[c]));
-    const double lam = m.mlambda ? double(ld(m.mlambda + q)) : double(m.lambda);
-    const double mu = m.mmu ? double(ld(m.mmu + q)) : double(m.mu);
-    const double rho = m.mdensity ? double(ld(m.mdensity + q)) : double(m.density);
-    const double v2 = f[0] * f[0] + f[1] * f[1] + f[2] * f[2];
-    s.velocity = sqrt(v2);
-    s.peak[0] = fabs(f[2]), s.peak[1] = fabs(f[0]), s.peak[2] = fabs(f[1]), s.peak[3] = sqrt(v2);
-    s.peak[4] = fabs((f[3] + f[4] + f[5]) / 3.0);
-    const double mean = (f[3] + f[4] + f[5]) / 3;
-    double dev = 0;
-    for (int c = 0; c < 3; ++c) dev += (f[c + 3] - mean) * (f[c + 3] - mean);
-    for (int c = 6; c < 9; ++c) dev += 2 * f[c] * f[c];
-    const double hh = double(m.h);
-    s.energy = (0.5 * rho * v2 + dev / (4 * mu) + mean * mean / (2 * (lam + 2 * mu / 3))) * double(ld(m.jac + q)) * hh * hh * hh;
-    s.bad |= int(!isfinite(s.energy));
-}
-
 template <class Real, int STAGE>
-__device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r)[9], long long q, int depth, long long sq,
-                                        Partial *diag) {
+__device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r)[9], long long q, int depth, long long sq) {
     const Mesh<Real> &m = p.m;
     const long long n = m.count;
     // FP64: A = U + dt/6 k1, A += dt/3 k2, A += dt/3 k3, new = A + dt/6 k4 (the reference's
@@ -236,13 +205,12 @@ __device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r
     if (STAGE == 3 && k2::kahan<Real>())
 #pragma unroll
         for (int f = 0; f < 9; ++f) p.cout[f * n + q] = comp[f];
-    if (STAGE == 3 && diag) nodeDiag(m, o, q, *diag);
 }
 
 // The general node: surface rows (traction-free derivative, traction-image momentum,
 // projection), sponge damping and the source.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
-__device__ __forceinline__ void stageBody3(const StageArgs<Real> &p, Partial *diag) {
+__device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -343,10 +311,9 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p, Partial *di
 #pragma unroll
         for (int f = 3; f < 9; ++f) norm2 += (f >= 6 ? 2.0 : 1.0) * double(r[f]) * double(r[f]);
         p.surfRate[sq] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-        if (diag) diag->rateTraction = p.surfRate[sq], diag->rateNorm = sqrt(norm2);
         p.surfRate[plane + sq] = sqrt(norm2);
     }
-    finish3<Real, STAGE>(p, r, q, depth, sq, diag);
+    finish3<Real, STAGE>(p, r, q, depth, sq);
 }
 
 // The interior node (below the surface rows, outside the sponge and the source support).  The
@@ -355,7 +322,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p, Partial *di
 // r1 = (gxy,x + gyy,y) + gyz,z, r2 = (gxz,x + gyz,y) + gzz,z (src/three_d/PointKernels3D.hpp:92-112),
 // so only a few gradients are live at a time.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
-__device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p, Partial *diag) {
+__device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -404,7 +371,7 @@ __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p, Partial
         r[1] = m1 / rho;
         r[2] = m2 / rho;
     }
-    finish3<Real, STAGE>(p, r, q, 4, i + nx * j, diag);
+    finish3<Real, STAGE>(p, r, q, 4, i + nx * j);
 }
 
 // One RK stage of a 3D shot: block 32x8 nodes of one z layer.  A CTA whose nodes are all below
@@ -419,47 +386,23 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __gri
     const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
     const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
     const bool interior = !(surface || source || sponge);
-    Partial s{};
-    const bool withDiag = STAGE == 3 && p.partials != nullptr;
-    Partial *d = withDiag ? &s : nullptr;
     if constexpr (sizeof(Real) == 4) {
-        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p, d);
-        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p, d);
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p);
     } else if (m.hinvExact) {
-        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p, d);
-        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p, d);
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, true>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, true>(p);
     } else {
-        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, false>(p, d);
-        else stageBody3<Real, DX, DY, DZ, STAGE, false>(p, d);
-    }
-    if (withDiag) { // one partial per CTA, in the layout stats3d writes (the verdict reduces them)
-        for (int o = 16; o > 0; o >>= 1) {
-            s.energy += __shfl_down_sync(0xffffffffu, s.energy, o);
-            s.velocity = fmax(s.velocity, __shfl_down_sync(0xffffffffu, s.velocity, o));
-            s.rateTraction = fmax(s.rateTraction, __shfl_down_sync(0xffffffffu, s.rateTraction, o));
-            s.rateNorm = fmax(s.rateNorm, __shfl_down_sync(0xffffffffu, s.rateNorm, o));
-#pragma unroll
-            for (int c = 0; c < 5; ++c) s.peak[c] = fmax(s.peak[c], __shfl_down_sync(0xffffffffu, s.peak[c], o));
-            s.bad |= __shfl_down_sync(0xffffffffu, s.bad, o);
-        }
-        __shared__ Partial warps[8];
-        const int t = threadIdx.x + blockDim.x * threadIdx.y;
-        if ((t & 31) == 0) warps[t >> 5] = s;
-        __syncthreads();
-        if (t == 0) {
-            Partial tot = warps[0];
-            for (int w = 1; w < 8; ++w) {
-                tot.energy += warps[w].energy;
-                tot.velocity = fmax(tot.velocity, warps[w].velocity);
-                tot.rateTraction = fmax(tot.rateTraction, warps[w].rateTraction);
-                tot.rateNorm = fmax(tot.rateNorm, warps[w].rateNorm);
-                for (int c = 0; c < 5; ++c) tot.peak[c] = fmax(tot.peak[c], warps[w].peak[c]);
-                tot.bad |= warps[w].bad;
-            }
-            p.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = tot;
-        }
+        if (interior) stageInterior3<Real, DX, DY, DZ, STAGE, false>(p);
+        else stageBody3<Real, DX, DY, DZ, STAGE, false>(p);
     }
 }
+
+struct Partial {
+    double energy, velocity, rateTraction, rateNorm;
+    double peak[5];
+    int bad, pad;
+};
 
 // Energy, peaks, finiteness and the traction-rate residual of a state
 // (src/three_d/CurvilinearSolver.cpp:214-250, CudaEngine3D.cu:36-55).
