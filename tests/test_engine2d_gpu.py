@@ -151,3 +151,18 @@ def test_diagnostics_report_energy_and_finiteness(swl):
     assert d["energy"] == pytest.approx(float(res["energy"]), rel=1e-9)
     assert d["max_velocity"] == pytest.approx(float(res["maxVelocity"]), rel=1e-12)
     assert d["resident_bytes"] > 0 and d["rhs_registers"] > 0
+
+
+@pytest.mark.parametrize("precision", ["SWL_FP32", "SWL_FP64"])
+def test_identical_engines_give_identical_results(precision, swl):
+    # The per-grid segment choice is kept per grid shape, so two engines of one shot use the same
+    # decomposition and agree bit for bit (FP32 rounding would otherwise depend on it).
+    case, res, mesh = load_2d("cpml_external_moment_layers")
+    dt, f, s = float(res["dt"]), mesh["frequency"], mesh["scale"]
+    out = []
+    for _ in range(2):
+        e = swl.Engine2D(mesh, receivers_2d(res), precision=getattr(swl, precision))
+        e.advance(0, 24, dt, f, s)
+        out.append((e.fields(), e.traces(0, 24)))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1][0], out[1][1][0])
