@@ -9,6 +9,8 @@
 #include <cmath>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace swl {
@@ -44,11 +46,12 @@ namespace detail3 {
 template <class Real> struct Launch {
     template <int DX, int DY, int DZ>
     static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
+        constexpr unsigned bytes = k3::streamBytes3<Real>();
         switch (stage) {
-        case 0: k3::stage3d<Real, DX, DY, DZ, 0><<<g, b, 0, s>>>(a); break;
-        case 1: k3::stage3d<Real, DX, DY, DZ, 1><<<g, b, 0, s>>>(a); break;
-        case 2: k3::stage3d<Real, DX, DY, DZ, 2><<<g, b, 0, s>>>(a); break;
-        default: k3::stage3d<Real, DX, DY, DZ, 3><<<g, b, 0, s>>>(a); break;
+        case 0: k3::stream3d<Real, DX, DY, DZ, 0><<<g, b, bytes, s>>>(a); break;
+        case 1: k3::stream3d<Real, DX, DY, DZ, 1><<<g, b, bytes, s>>>(a); break;
+        case 2: k3::stream3d<Real, DX, DY, DZ, 2><<<g, b, bytes, s>>>(a); break;
+        default: k3::stream3d<Real, DX, DY, DZ, 3><<<g, b, bytes, s>>>(a); break;
         }
     }
     static void stage(int dx, int dy, int dz, int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
@@ -63,6 +66,20 @@ template <class Real> struct Launch {
         default: st<1, 1, 1>(stage, g, b, s, a); break;
         }
     }
+    template <class K> static void allow(K kernel) {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k3::streamBytes3<Real>())),
+              "3D stage shared memory");
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)),
+              "3D stage shared-memory carveout");
+    }
+    template <int DX, int DY, int DZ> static void allowStages() {
+        allow(k3::stream3d<Real, DX, DY, DZ, 0>), allow(k3::stream3d<Real, DX, DY, DZ, 1>);
+        allow(k3::stream3d<Real, DX, DY, DZ, 2>), allow(k3::stream3d<Real, DX, DY, DZ, 3>);
+    }
+    static void prepare() {
+        allowStages<0, 0, 0>(), allowStages<0, 0, 1>(), allowStages<0, 1, 0>(), allowStages<0, 1, 1>();
+        allowStages<1, 0, 0>(), allowStages<1, 0, 1>(), allowStages<1, 1, 0>(), allowStages<1, 1, 1>();
+    }
 };
 } // namespace detail3
 
@@ -70,7 +87,10 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     int device_{};
     cudaStream_t stream_{}, ownStream_{};
     k3::Mesh<Real> m_{};
-    long long count_{};
+    long long count_{};         // nodes of one pitched field (px*ny*nz)
+    long long dense_{};         // nodes of one field in the API's dense layout (nx*ny*nz)
+    CUtensorMap inMap_[4]{};    // sets 0-3 as (x, y, z, field) tensors for the stage input
+    dim3 stageGrid_{};
     std::vector<DeviceBuffer> model_;
     DeviceBuffer sets_, recIdx_, traces_, forcing_, clock_, partials_, surfRate_;
     // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
@@ -102,13 +122,22 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             check(cudaMemcpy(model_.back().ptr, v.data(), v.size() * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
         return model_.back().template as<Real>();
     }
-    static std::vector<Real> conv(const double *src, std::size_t n, std::size_t stride = 1, std::size_t offset = 0) {
-        std::vector<Real> out(n);
-        for (std::size_t i = 0; i < n; ++i) {
-            out[i] = static_cast<Real>(src[i * stride + offset]);
-            if (!std::isfinite(double(out[i])))
-                throw Error(SWL_ERR_INVALID, "3D mesh value is not finite in the engine precision");
-        }
+    // Pitched position of dense node d = i + nx*(j + ny*k).
+    long long pitched(long long d) const {
+        const long long i = d % m_.nx, r = d / m_.nx;
+        return i + (long long)m_.px * r;
+    }
+    // A dense per-node array (value of node d at src[d*stride + offset]) in the engine precision,
+    // pitched; the pad columns hold zero.
+    std::vector<Real> conv(const double *src, std::size_t stride = 1, std::size_t offset = 0) const {
+        std::vector<Real> out(std::size_t(count_), Real(0));
+        const std::size_t nx = std::size_t(m_.nx), rows = std::size_t(m_.ny) * m_.nz;
+        for (std::size_t r = 0; r < rows; ++r)
+            for (std::size_t i = 0; i < nx; ++i) {
+                const Real v = static_cast<Real>(src[(i + nx * r) * stride + offset]);
+                if (!std::isfinite(double(v))) throw Error(SWL_ERR_INVALID, "3D mesh value is not finite in the engine precision");
+                out[i + std::size_t(m_.px) * r] = v;
+            }
         return out;
     }
     void dropGraphs() {
@@ -118,6 +147,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     k3::StageArgs<Real> args(int stage) const {
         k3::StageArgs<Real> p{};
         p.m = m_;
+        p.inMap = inMap_[stage == 0 ? u_ : stage == 2 ? 3 : 2];
         Real *U = set_[u_], *A = set_[a_], *S1 = set_[2], *S2 = set_[3];
         p.base = U;
         p.acc = A;
@@ -139,7 +169,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
         if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
         for (int s = 0; s < 4; ++s) {
-            detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, grid_, block_,
+            detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, stageGrid_, block_,
                                          stream_, args(s));
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
@@ -215,13 +245,15 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         if (nrec < 0 || (nrec && !rec)) throw Error(SWL_ERR_INVALID, "receiver list is invalid");
         check(cudaStreamCreateWithFlags(&ownStream_, cudaStreamNonBlocking), "create stream");
         stream_ = ownStream_;
-        const std::size_t n = std::size_t(g.count);
-        count_ = g.count;
+        m_.nx = g.nx, m_.ny = g.ny, m_.nz = g.nz;
+        m_.px = (g.nx + 3) / 4 * 4;
+        m_.plane = (long long)m_.px * g.ny;
+        m_.count = m_.plane * g.nz;
+        count_ = m_.count;
+        dense_ = g.count;
+        const std::size_t n = std::size_t(count_);
         nrec_ = nrec;
         hostDensity_ = g.density, hostH_ = g.h, amplitude_ = g.source_amplitude;
-        m_.nx = g.nx, m_.ny = g.ny, m_.nz = g.nz;
-        m_.count = g.count;
-        m_.plane = (long long)g.nx * g.ny;
         m_.h = static_cast<Real>(g.h);
         {
             // x/h equals x*(1/h) bit for bit when h is a power of two; otherwise the kernels form
@@ -233,18 +265,18 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
         }
         m_.lambda = static_cast<Real>(g.lambda), m_.mu = static_cast<Real>(g.mu), m_.density = static_cast<Real>(g.density);
-        for (int c = 0; c < 9; ++c) m_.metric[c] = upload(conv(g.metrics, n, 9, c));
-        m_.jac = upload(conv(g.jacobian, n));
-        const auto damping = conv(g.damping, n);
+        for (int c = 0; c < 9; ++c) m_.metric[c] = upload(conv(g.metrics, 9, c));
+        m_.jac = upload(conv(g.jacobian));
+        const auto damping = conv(g.damping);
         m_.damping = upload(damping);
-        const auto src = conv(g.source, n);
+        const auto src = conv(g.source);
         m_.source = upload(src);
         std::vector<Real> sg[3];
         const bool moment = g.source_gradient[0] != nullptr;
         for (int a = 0; a < 3; ++a) {
             if (moment) {
                 if (!g.source_gradient[a]) throw Error(SWL_ERR_INVALID, "moment source needs three gradient arrays");
-                sg[a] = conv(g.source_gradient[a], n);
+                sg[a] = conv(g.source_gradient[a]);
                 m_.sg[a] = upload(sg[a]);
             }
             m_.sdir[a] = static_cast<Real>(g.source_direction[a]);
@@ -252,15 +284,17 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         if (g.material_lambda || g.material_mu || g.material_density) {
             if (!g.material_lambda || !g.material_mu || !g.material_density)
                 throw Error(SWL_ERR_INVALID, "layered material needs lambda, mu and density arrays");
-            m_.mlambda = upload(conv(g.material_lambda, n));
-            m_.mmu = upload(conv(g.material_mu, n));
-            m_.mdensity = upload(conv(g.material_density, n));
+            m_.mlambda = upload(conv(g.material_lambda));
+            m_.mmu = upload(conv(g.material_mu));
+            m_.mdensity = upload(conv(g.material_density));
         }
         {
-            std::vector<Real> nrm(3 * std::size_t(m_.plane));
-            const std::size_t top = std::size_t(3) * m_.plane;
-            for (std::size_t s = 0; s < std::size_t(m_.plane); ++s)
-                for (int c = 0; c < 3; ++c) nrm[3 * s + c] = static_cast<Real>(g.normals[3 * (top + s) + c]);
+            std::vector<Real> nrm(3 * std::size_t(m_.plane), Real(0));
+            const std::size_t nx = std::size_t(g.nx), top = std::size_t(3) * nx * g.ny;
+            for (std::size_t j = 0; j < std::size_t(g.ny); ++j)
+                for (std::size_t i = 0; i < nx; ++i)
+                    for (int c = 0; c < 3; ++c)
+                        nrm[3 * (i + std::size_t(m_.px) * j) + c] = static_cast<Real>(g.normals[3 * (top + i + nx * j) + c]);
             m_.normals = upload(nrm);
         }
         // boxes of the source support and of the zero sponge rate
@@ -268,7 +302,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         for (int k = 0; k < g.nz; ++k)
             for (int j = 0; j < g.ny; ++j)
                 for (int i = 0; i < g.nx; ++i) {
-                    const std::size_t q = i + std::size_t(g.nx) * (j + std::size_t(g.ny) * k);
+                    const std::size_t q = i + std::size_t(m_.px) * (j + std::size_t(g.ny) * k);
                     const bool nz = moment ? (sg[0][q] != Real(0) || sg[1][q] != Real(0) || sg[2][q] != Real(0)) : src[q] != Real(0);
                     if (nz)
                         b[0] = std::min(b[0], i), b[1] = std::max(b[1], i + 1), b[2] = std::min(b[2], j), b[3] = std::max(b[3], j + 1),
@@ -276,7 +310,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
                 }
         m_.src_i0 = b[0], m_.src_i1 = b[1], m_.src_j0 = b[2], m_.src_j1 = b[3], m_.src_k0 = b[4], m_.src_k1 = b[5];
         {
-            auto D = [&](int i, int j, int k) { return damping[i + std::size_t(g.nx) * (j + std::size_t(g.ny) * k)]; };
+            auto D = [&](int i, int j, int k) { return damping[i + std::size_t(m_.px) * (j + std::size_t(g.ny) * k)]; };
             const int jm = g.ny / 2, im = g.nx / 2;
             int i0 = 3, i1 = g.nx - 3, j0 = 3, j1 = g.ny - 3, kk = 3;
             while (i0 < i1 && D(i0, jm, 3) != Real(0)) ++i0;
@@ -301,21 +335,75 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         std::vector<long long> idx(nrec);
         for (int r = 0; r < nrec; ++r) {
             if (rec[r] < 0 || rec[r] >= g.count) throw Error(SWL_ERR_INVALID, "receiver node outside the padded grid");
-            idx[r] = rec[r];
+            idx[r] = pitched(rec[r]);
         }
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + 31) / 32, (g.ny - 6 + 7) / 8, g.nz - 6);
         nparts_ = grid_.x * grid_.y * grid_.z;
         partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
+        {
+            const uint64_t dims[4] = {uint64_t(g.nx), uint64_t(g.ny), uint64_t(g.nz), 9};
+            const uint64_t strides[3] = {uint64_t(m_.px) * sizeof(Real), uint64_t(m_.plane) * sizeof(Real), uint64_t(n) * sizeof(Real)};
+            const uint32_t box[4] = {k3::BX, k3::BY, 1, 9};
+            for (int s = 0; s < 4; ++s) encodeTensorMap(&inMap_[s], sizeof(Real) == 8, set_[s], 4, dims, strides, box);
+        }
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
+        detail3::Launch<Real>::prepare();
         cudaFuncAttributes attr{};
-        check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
+        check(cudaFuncGetAttributes(&attr, k3::stream3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
         registers_ = attr.numRegs;
+        tune();
     }
+    // Stage-kernel segment: `seg` z planes per CTA.
+    void setSegment(int seg) {
+        m_.seg = seg;
+        stageGrid_ = dim3((m_.nx - 6 + k3::TX - 1) / k3::TX, (m_.ny - 6 + k3::TY - 1) / k3::TY, (m_.nz - 6 + seg - 1) / seg);
+        dropGraphs(); // the graphs hold the launch shape
+    }
+    // The segment length for this grid, picked by timing two steps per candidate on the fresh
+    // (zero) state: long segments copy fewer window planes per CTA (each segment starts by
+    // loading its five-plane window), short ones put more CTAs in flight, which a grid with few
+    // (x, y) tiles needs.  Candidates halve from the whole depth down to 4 planes; a shorter one
+    // is taken only when clearly faster.  The state and the clock are reset afterwards, and the
+    // choice is kept per grid shape for the life of the process.  Results do not depend on it:
+    // each node's arithmetic is fixed by its position alone.
+    void tune() {
+        static std::mutex mutex;
+        static std::map<std::tuple<int, int, int, int, int>, int> chosen;
+        const auto key = std::make_tuple(device_, m_.nx, m_.ny, m_.nz, m_.dmp_k1);
+        {
+            std::lock_guard<std::mutex> g(mutex);
+            const auto it = chosen.find(key);
+            if (it != chosen.end()) {
+                setSegment(it->second);
+                return;
+            }
+        }
+        const int planes = m_.nz - 6;
+        swl_profile prof{};
+        setSegment(planes);
+        profile(0, 1, 1e-6, 10.0, prof); // first launches (module load) outside the timing
+        int best = planes;
+        double bestMs = 0;
+        for (int seg = planes;; seg = (seg + 1) / 2) {
+            setSegment(seg);
+            profile(0, 2, 1e-6, 10.0, prof);
+            const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
+            if (seg == planes || ms < 0.97 * bestMs) best = seg, bestMs = ms;
+            if (seg <= 4) break;
+        }
+        {
+            std::lock_guard<std::mutex> g(mutex);
+            best = chosen.emplace(key, best).first->second; // a concurrent creation may have decided first
+        }
+        setSegment(best);
+        reset();
+    }
+    int segment() const { return m_.seg; }
     ~TypedEngine3D() override {
         if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
         if (stream_) cudaStreamSynchronize(stream_);
@@ -543,14 +631,19 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         std::vector<Real> tmp(count_);
         check(cudaMemcpy(tmp.data(), set_[u_] + std::size_t(field) * count_, count_ * sizeof(Real), cudaMemcpyDeviceToHost),
               "snapshot download");
-        for (long long i = 0; i < count_; ++i) out[i] = double(tmp[i]);
+        const long long rows = (long long)m_.ny * m_.nz;
+        for (long long r = 0; r < rows; ++r)
+            for (int i = 0; i < m_.nx; ++i) out[i + m_.nx * r] = double(tmp[i + m_.px * r]);
     }
     void load(int field, const double *in) override {
         settle();
         DeviceScope scope(device_);
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
         check(cudaStreamSynchronize(stream_), "load ordering");
-        std::vector<Real> tmp(in, in + count_);
+        std::vector<Real> tmp(count_, Real(0));
+        const long long rows = (long long)m_.ny * m_.nz;
+        for (long long r = 0; r < rows; ++r)
+            for (int i = 0; i < m_.nx; ++i) tmp[i + m_.px * r] = static_cast<Real>(in[i + m_.nx * r]);
         check(cudaMemcpy(set_[u_] + std::size_t(field) * count_, tmp.data(), count_ * sizeof(Real), cudaMemcpyHostToDevice),
               "field upload");
         if (k2::kahan<Real>()) // a loaded value starts without a compensation term

@@ -323,7 +323,8 @@ struct Session3D {
     }
     bool completed() const { return step >= model.total; }
     int64_t estimateBytes() const {
-        const double s = params.precision == SWL_FP32 ? 4 : 8, n = double(model.nx) * model.ny * model.nz;
+        // the engine pitches rows to a multiple of four nodes
+        const double s = params.precision == SWL_FP32 ? 4 : 8, n = double((model.nx + 3) / 4 * 4) * model.ny * model.nz;
         const double fields = (s == 4 ? 6 : 4) * 9; // state sets, with the FP32 compensation sets
         return int64_t(n * s * (fields + 9 + 2 + (model.materialLambda.empty() ? 0 : 3) + (model.sourceGradient[0].empty() ? 0 : 3))) + (64 << 20);
     }
