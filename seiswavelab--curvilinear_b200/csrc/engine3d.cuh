@@ -9,8 +9,6 @@
 #include <cmath>
 #include <map>
 #include <memory>
-#include <mutex>
-#include <tuple>
 #include <vector>
 
 namespace swl {
@@ -46,12 +44,11 @@ namespace detail3 {
 template <class Real> struct Launch {
     template <int DX, int DY, int DZ>
     static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
-        constexpr unsigned bytes = k3::streamBytes3<Real>();
         switch (stage) {
-        case 0: k3::stream3d<Real, DX, DY, DZ, 0><<<g, b, bytes, s>>>(a); break;
-        case 1: k3::stream3d<Real, DX, DY, DZ, 1><<<g, b, bytes, s>>>(a); break;
-        case 2: k3::stream3d<Real, DX, DY, DZ, 2><<<g, b, bytes, s>>>(a); break;
-        default: k3::stream3d<Real, DX, DY, DZ, 3><<<g, b, bytes, s>>>(a); break;
+        case 0: k3::stage3d<Real, DX, DY, DZ, 0><<<g, b, 0, s>>>(a); break;
+        case 1: k3::stage3d<Real, DX, DY, DZ, 1><<<g, b, 0, s>>>(a); break;
+        case 2: k3::stage3d<Real, DX, DY, DZ, 2><<<g, b, 0, s>>>(a); break;
+        default: k3::stage3d<Real, DX, DY, DZ, 3><<<g, b, 0, s>>>(a); break;
         }
     }
     static void stage(int dx, int dy, int dz, int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
@@ -66,20 +63,6 @@ template <class Real> struct Launch {
         default: st<1, 1, 1>(stage, g, b, s, a); break;
         }
     }
-    template <class K> static void allow(K kernel) {
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k3::streamBytes3<Real>())),
-              "3D stage shared memory");
-        check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)),
-              "3D stage shared-memory carveout");
-    }
-    template <int DX, int DY, int DZ> static void allowStages() {
-        allow(k3::stream3d<Real, DX, DY, DZ, 0>), allow(k3::stream3d<Real, DX, DY, DZ, 1>);
-        allow(k3::stream3d<Real, DX, DY, DZ, 2>), allow(k3::stream3d<Real, DX, DY, DZ, 3>);
-    }
-    static void prepare() {
-        allowStages<0, 0, 0>(), allowStages<0, 0, 1>(), allowStages<0, 1, 0>(), allowStages<0, 1, 1>();
-        allowStages<1, 0, 0>(), allowStages<1, 0, 1>(), allowStages<1, 1, 0>(), allowStages<1, 1, 1>();
-    }
 };
 } // namespace detail3
 
@@ -89,8 +72,6 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     k3::Mesh<Real> m_{};
     long long count_{};         // nodes of one pitched field (px*ny*nz)
     long long dense_{};         // nodes of one field in the API's dense layout (nx*ny*nz)
-    CUtensorMap inMap_[4]{};    // sets 0-3 as (x, y, z, field) tensors for the stage input
-    dim3 stageGrid_{};
     std::vector<DeviceBuffer> model_;
     DeviceBuffer sets_, recIdx_, traces_, forcing_, clock_, partials_, surfRate_;
     // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
@@ -147,7 +128,6 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     k3::StageArgs<Real> args(int stage) const {
         k3::StageArgs<Real> p{};
         p.m = m_;
-        p.inMap = inMap_[stage == 0 ? u_ : stage == 2 ? 3 : 2];
         Real *U = set_[u_], *A = set_[a_], *S1 = set_[2], *S2 = set_[3];
         p.base = U;
         p.acc = A;
@@ -169,7 +149,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
         if (ev) check(cudaEventRecord(ev[0], stream_), "record event");
         for (int s = 0; s < 4; ++s) {
-            detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, stageGrid_, block_,
+            detail3::Launch<Real>::stage(direction(step, s, 0), direction(step, s, 1), direction(step, s, 2), s, grid_, block_,
                                          stream_, args(s));
             if (ev) check(cudaEventRecord(ev[1 + s], stream_), "record event");
         }
@@ -342,68 +322,14 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         grid_ = dim3((g.nx - 6 + 31) / 32, (g.ny - 6 + 7) / 8, g.nz - 6);
         nparts_ = grid_.x * grid_.y * grid_.z;
         partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
-        {
-            const uint64_t dims[4] = {uint64_t(g.nx), uint64_t(g.ny), uint64_t(g.nz), 9};
-            const uint64_t strides[3] = {uint64_t(m_.px) * sizeof(Real), uint64_t(m_.plane) * sizeof(Real), uint64_t(n) * sizeof(Real)};
-            const uint32_t box[4] = {k3::BX, k3::BY, 1, 9};
-            for (int s = 0; s < 4; ++s) encodeTensorMap(&inMap_[s], sizeof(Real) == 8, set_[s], 4, dims, strides, box);
-        }
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
-        detail3::Launch<Real>::prepare();
         cudaFuncAttributes attr{};
-        check(cudaFuncGetAttributes(&attr, k3::stream3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
+        check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
         registers_ = attr.numRegs;
-        tune();
     }
-    // Stage-kernel segment: `seg` z planes per CTA.
-    void setSegment(int seg) {
-        m_.seg = seg;
-        stageGrid_ = dim3((m_.nx - 6 + k3::TX - 1) / k3::TX, (m_.ny - 6 + k3::TY - 1) / k3::TY, (m_.nz - 6 + seg - 1) / seg);
-        dropGraphs(); // the graphs hold the launch shape
-    }
-    // The segment length for this grid, picked by timing two steps per candidate on the fresh
-    // (zero) state: long segments copy fewer window planes per CTA (each segment starts by
-    // loading its five-plane window), short ones put more CTAs in flight, which a grid with few
-    // (x, y) tiles needs.  Candidates halve from the whole depth down to 4 planes; a shorter one
-    // is taken only when clearly faster.  The state and the clock are reset afterwards, and the
-    // choice is kept per grid shape for the life of the process.  Results do not depend on it:
-    // each node's arithmetic is fixed by its position alone.
-    void tune() {
-        static std::mutex mutex;
-        static std::map<std::tuple<int, int, int, int, int>, int> chosen;
-        const auto key = std::make_tuple(device_, m_.nx, m_.ny, m_.nz, m_.dmp_k1);
-        {
-            std::lock_guard<std::mutex> g(mutex);
-            const auto it = chosen.find(key);
-            if (it != chosen.end()) {
-                setSegment(it->second);
-                return;
-            }
-        }
-        const int planes = m_.nz - 6;
-        swl_profile prof{};
-        setSegment(planes);
-        profile(0, 1, 1e-6, 10.0, prof); // first launches (module load) outside the timing
-        int best = planes;
-        double bestMs = 0;
-        for (int seg = planes;; seg = (seg + 1) / 2) {
-            setSegment(seg);
-            profile(0, 2, 1e-6, 10.0, prof);
-            const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
-            if (seg == planes || ms < 0.97 * bestMs) best = seg, bestMs = ms;
-            if (seg <= 4) break;
-        }
-        {
-            std::lock_guard<std::mutex> g(mutex);
-            best = chosen.emplace(key, best).first->second; // a concurrent creation may have decided first
-        }
-        setSegment(best);
-        reset();
-    }
-    int segment() const { return m_.seg; }
     ~TypedEngine3D() override {
         if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
         if (stream_) cudaStreamSynchronize(stream_);

@@ -27,8 +27,8 @@ int selectDevice(int requested) {
     return requested >= 0 ? -1 : best;
 }
 
-void encodeTensorMap(CUtensorMap *map, bool fp64, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
-                     const uint32_t *box) {
+void encodeTensorMap3D(CUtensorMap *map, bool fp64, const void *base, const uint64_t dims[3], const uint64_t strides[2],
+                       const uint32_t box[3]) {
     using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
                                 const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -39,20 +39,12 @@ void encodeTensorMap(CUtensorMap *map, bool fp64, const void *base, int rank, co
         if (!fn || q != cudaDriverEntryPointSuccess) throw Error(-5, "the driver has no tensor-map encoder");
         return reinterpret_cast<Encode>(fn);
     }();
-    if (rank < 3 || rank > 5) throw Error(-5, "tensor-map rank must be 3..5");
-    cuuint64_t gdim[5], gstride[4];
-    cuuint32_t bdim[5], estride[5];
-    for (int d = 0; d < rank; ++d) gdim[d] = dims[d], bdim[d] = box[d], estride[d] = 1;
-    for (int d = 0; d + 1 < rank; ++d) gstride[d] = strides[d];
-    const CUresult r = encode(map, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, cuuint32_t(rank),
-                              const_cast<void *>(base), gdim, gstride, bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]}, gstride[2] = {strides[0], strides[1]};
+    const cuuint32_t bdim[3] = {box[0], box[1], box[2]}, estride[3] = {1, 1, 1};
+    const CUresult r = encode(map, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base),
+                              gdim, gstride, bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(-2, "CUDA encode tensor map: error " + std::to_string(int(r)));
-}
-
-void encodeTensorMap3D(CUtensorMap *map, bool fp64, const void *base, const uint64_t dims[3], const uint64_t strides[2],
-                       const uint32_t box[3]) {
-    encodeTensorMap(map, fp64, base, 3, dims, strides, box);
 }
 
 // src/two_d/CurvilinearSolver2D.cpp:31-34

@@ -119,8 +119,5 @@ double ricker(double t, double f);
 // runtime's entry-point query, so the library does not link libcuda.
 void encodeTensorMap3D(CUtensorMap *map, bool fp64, const void *base, const uint64_t dims[3], const uint64_t strides[2],
                        const uint32_t box[3]);
-// The same for a rank-`rank` tensor (3..5): dims[rank], strides[rank - 1], box[rank].
-void encodeTensorMap(CUtensorMap *map, bool fp64, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
-                     const uint32_t *box);
 
 } // namespace swl

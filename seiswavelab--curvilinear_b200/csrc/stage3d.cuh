@@ -1,25 +1,25 @@
 // 3D nine-field elastic device code: one fused kernel per classic-RK4 stage.
 //
-// Each node gets 27 MacCormack-DRP derivatives of the stage input, the metric transform to
-// physical gradients, the nine rates of src/three_d/PointKernels3D.hpp:92-112 (traction-image
-// momentum near the surface, traction-free surface derivative on the top row, sponge damping,
-// force or moment source), then its part of the RK combine and the tangential-stress
-// projection.  The 3D reference sums the RK stages as
+// Each thread owns one physical node: 27 MacCormack-DRP derivatives of the stage input, the
+// metric transform to physical gradients, the nine rates of src/three_d/PointKernels3D.hpp:92-112
+// (traction-image momentum near the surface, traction-free surface derivative on the top
+// row, sponge damping, force or moment source), then its part of the RK combine and the
+// tangential-stress projection.  The 3D reference sums the RK stages as
 // (((base + dt/6 k1) + dt/3 k2) + dt/3 k3) + dt/6 k4 (src/three_d/CurvilinearSolver.cpp:91-101),
 // so the accumulator here carries the partial state sum: A = U + dt/6 k1, A += dt/3 k2,
 // A += dt/3 k3, new state = A + dt/6 k4 written over A.
 //
 // Layout: every field is a pitched (x, y, z) array; node (i, j, k) sits at i + px*j + px*ny*k
 // with the row pitch px a multiple of four nodes, so that every row starts on a 16-byte
-// boundary and the nine fields of a state form one 4D tensor (x, y, z, field) for TMA.  Metrics
-// are nine separate arrays (structure of arrays) so that every point load of a warp is
-// coalesced; the surface normals and the traction-rate diagnostics only exist for the top row.
+// boundary.  Metrics are nine separate arrays (structure of arrays) so that every load of a
+// warp is coalesced; the surface normals and the traction-rate diagnostics only exist for the
+// top row.
 //
-// The stage kernel marches z: a CTA owns a 32 x 8 (x, y) tile and a segment of z planes.  One
-// thread issues a TMA copy of each plane's halo'd 40 x 12 tile of the nine input fields into a
-// ring of six plane slots; the five planes k-3..k+1 (backward z stencil) or k-1..k+3 (forward)
-// are resident while plane k is evaluated and plane k+2 (k+4) is in flight, so every stencil tap
-// is a shared-memory read and every input word crosses HBM once per stage.
+// The stencil taps are read through L1: a CTA of 32 x 8 nodes of one z layer re-reads its x/y
+// neighbours from L1 and the z layers above and below from L2.  A z-marching form that stages
+// halo'd planes in shared memory by TMA was measured slower: its ring of planes (207 KB FP64,
+// 104 KB FP32 per CTA) leaves 8 or 16 resident warps per SM, too few to hide the point loads
+// (metrics, material, base, accumulator) that every node still makes, while this form keeps 32.
 #pragma once
 #include "runtime.cuh"
 #include "stage2d.cuh"
@@ -30,7 +30,6 @@ namespace swl::k3 {
 template <class Real> struct Mesh {
     int nx, ny, nz;
     int px;                         // row pitch in nodes (multiple of 4, >= nx)
-    int seg;                        // z planes per CTA of the stage kernel
     long long count, plane;         // px*ny*nz, px*ny
     Real h, lambda, mu, density;    // uniform material (used when the material arrays are null)
     Real hinv;                      // RN(1/h)
@@ -47,7 +46,6 @@ template <class Real> struct Mesh {
 using k2::Clock;
 
 template <class Real> struct StageArgs {
-    CUtensorMap inMap;   // the nine fields of `in` as a (x, y, z, field) tensor; box 40 x 12 x 1 x 9
     Mesh<Real> m;
     const Real *in;
     Real *out;
@@ -63,16 +61,6 @@ template <class Real> struct StageArgs {
 };
 
 using k2::ld;
-
-// Tile of the stage kernel and its shared-memory ring.
-constexpr int TX = 32, TY = 8;                 // nodes of a CTA in x and y (one per thread)
-constexpr int BX = 40, BY = 12;                // halo'd plane tile: x from i0-3, y from j0-1 (j0-3)
-constexpr int FIELD_WORDS = BX * BY;           // one field of one slot
-constexpr int SLOT_WORDS = 9 * FIELD_WORDS;    // one z plane of the nine fields
-constexpr int SLOTS = 6;                       // five stencil planes and the one in flight
-template <class Real> constexpr unsigned streamBytes3() { return 256 + SLOTS * SLOT_WORDS * sizeof(Real); }
-// Resident CTAs per SM allowed by shared memory: 1 x 207.6 KB (FP64), 2 x 103.9 KB (FP32).
-template <class Real> constexpr int streamBlocks3() { return sizeof(Real) == 8 ? 1 : 2; }
 
 // x / h as the reference forms it: the product with 1/h when that is exact, else the correctly
 // rounded FMA quotient (both equal the IEEE division bit for bit).
@@ -127,18 +115,6 @@ template <class Real, int DIR, bool EXACT, class V> __device__ __forceinline__ R
     return overH<Real, EXACT>(m, r);
 }
 
-// The stage input around one node, read from the CTA's ring: plane k's slot for the centre and
-// the x / y taps, the slots of planes k-3..k+3 (those of the z window) for the z taps.
-template <class Real> struct Taps {
-    const Real *ring;
-    int local;   // word offset of the node's field 0 inside a slot
-    int slot[7]; // word offset of the slot holding plane k + o at index o + 3
-    __device__ __forceinline__ Real c(int f) const { return ring[slot[3] + f * FIELD_WORDS + local]; }
-    __device__ __forceinline__ Real x(int f, int o) const { return ring[slot[3] + f * FIELD_WORDS + local + o]; }
-    __device__ __forceinline__ Real y(int f, int o) const { return ring[slot[3] + f * FIELD_WORDS + local + o * BX]; }
-    __device__ __forceinline__ Real z(int f, int o) const { return ring[slot[o + 3] + f * FIELD_WORDS + local]; }
-};
-
 template <class Real>
 __device__ __forceinline__ Real tractionFlux(const Mesh<Real> &m, const Real *__restrict__ w, long long qq, int axis, int comp) {
     const int F[3][3] = {{3, 6, 7}, {6, 4, 8}, {7, 8, 5}};
@@ -175,23 +151,41 @@ __device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__
     return sum / (m.h * ld(m.jac + q) * rho);
 }
 
-// RK combine, surface projection and stores of the nine rates of one node.  Stage 0's base is
-// its input, so U comes from the ring there.
+// The same derivatives with their taps read from global memory along stride s around node q.
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real gd5(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    return d5<Real, DIR, EXACT>(m, [&](int o) { return ld(v + q + o * s); });
+}
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real gd2(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    return d2<Real, DIR, EXACT>(m, [&](int o) { return ld(v + q + o * s); });
+}
+template <class Real, int DIR, bool EXACT>
+__device__ __forceinline__ Real gd3(const Real *__restrict__ v, long long q, long long s, const Mesh<Real> &m) {
+    return d3<Real, DIR, EXACT>(m, [&](int o) { return ld(v + q + o * s); });
+}
+// Four CTAs of 256 threads per SM (64 registers).  The kernel waits on its L1/L2 loads, and the
+// extra resident warps hide more of that latency than the spills this bound costs: measured at
+// 400x288x200, the stages run 1.3x faster with three CTAs per SM than with two, and 1.09x faster
+// again with four.
+template <class Real> constexpr int minBlocks3() { return 4; }
+
+// RK combine, surface projection and stores of the nine rates of one node.  Every global load is
+// issued before the first store: the stores could alias the loaded arrays as far as the compiler
+// knows, and interleaving them serialised nine round trips per node (stages 1 and 2 ran 1.5x
+// longer than stage 0 that way).
 template <class Real, int STAGE>
-__device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Taps<Real> &t, const Real (&r)[9], long long q, int depth,
-                                        long long sq) {
+__device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r)[9], long long q, int depth, long long sq) {
     const Mesh<Real> &m = p.m;
     const long long n = m.count;
     // FP64: A = U + dt/6 k1, A += dt/3 k2, A += dt/3 k3, new = A + dt/6 k4 (the reference's
     // order).  FP32: A accumulates the increment alone (A = dt/6 k1, ...), and stage 3 adds
     // d = A + dt/6 k4 to U by Kahan's compensated summation (y = d - c, t = U + y,
     // c' = (t - U) - y).
-    // Every global load is issued before the first store: the stores could alias the loaded
-    // arrays as far as the compiler knows, and interleaving them would serialise nine round trips.
     Real u[9], a[9], c[9], o[9], na[9], comp[9];
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
-        u[f] = STAGE == 0 ? t.c(f) : (STAGE < 3 || k2::kahan<Real>()) ? ld(p.base + f * n + q) : Real(0);
+        u[f] = (STAGE < 3 || k2::kahan<Real>()) ? ld(p.base + f * n + q) : Real(0);
         a[f] = STAGE > 0 ? p.acc[f * n + q] : Real(0);
         c[f] = STAGE == 3 && k2::kahan<Real>() ? ld(p.cin + f * n + q) : Real(0);
     }
@@ -211,19 +205,22 @@ __device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Taps<Rea
             o[f] = a[f] + p.w6 * r[f];
         }
     }
+    if (STAGE < 3)
+#pragma unroll
+        for (int f = 0; f < 9; ++f) p.acc[f * n + q] = na[f];
     if (depth == 0) { // tangential stress projection (PointKernels3D.hpp:36-51)
         const Real nn[3] = {ld(m.normals + 3 * sq), ld(m.normals + 3 * sq + 1), ld(m.normals + 3 * sq + 2)};
         const Real s[9] = {o[3], o[6], o[7], o[6], o[4], o[8], o[7], o[8], o[5]};
-        Real tr[3] = {0, 0, 0}, x[9];
+        Real t[3] = {0, 0, 0}, x[9];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) tr[a] += s[3 * a + b] * nn[b];
-        const Real nnn = tr[0] * nn[0] + tr[1] * nn[1] + tr[2] * nn[2];
+            for (int b = 0; b < 3; ++b) t[a] += s[3 * a + b] * nn[b];
+        const Real nnn = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) x[3 * a + b] = s[3 * a + b] - nn[a] * tr[b] - tr[a] * nn[b] + nnn * nn[a] * nn[b];
+            for (int b = 0; b < 3; ++b) x[3 * a + b] = s[3 * a + b] - nn[a] * t[b] - t[a] * nn[b] + nnn * nn[a] * nn[b];
         o[3] = x[0];
         o[4] = x[4];
         o[5] = x[8];
@@ -231,9 +228,6 @@ __device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Taps<Rea
         o[7] = Real(0.5) * (x[2] + x[6]);
         o[8] = Real(0.5) * (x[5] + x[7]);
     }
-    if (STAGE < 3)
-#pragma unroll
-        for (int f = 0; f < 9; ++f) p.acc[f * n + q] = na[f];
     Real *dst = STAGE == 3 ? p.acc : p.out;
 #pragma unroll
     for (int f = 0; f < 9; ++f) dst[f * n + q] = o[f];
@@ -243,14 +237,19 @@ __device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Taps<Rea
 }
 
 // The general node: surface rows (traction-free derivative, traction-image momentum,
-// projection), sponge damping and the source.
+// projection) and the source support, with sponge damping where it applies.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
-__device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Taps<Real> &t, int i, int j, int k) {
+__device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    if (i >= m.nx - 3 || j >= m.ny - 3) return;
     const Clock *clk = p.clock;
-    const long long px = m.px, plane = m.plane;
-    const long long q = i + px * j + plane * k;
+    const long long n = m.count, nx = m.px, plane = m.plane;
+    const long long q = i + nx * j + plane * k;
     const int depth = k - 3;
+    const Real *__restrict__ w = p.in;
     const Real lam = m.mlambda ? ld(m.mlambda + q) : m.lambda;
     const Real mu = m.mmu ? ld(m.mmu + q) : m.mu;
     const Real rho = m.mdensity ? ld(m.mdensity + q) : m.density;
@@ -262,15 +261,15 @@ __device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Tap
     Real dv[3][2];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        dv[v][0] = d5<Real, DX, EXACT>(m, [&](int o) { return t.x(v, o); });
-        dv[v][1] = d5<Real, DY, EXACT>(m, [&](int o) { return t.y(v, o); });
+        dv[v][0] = gd5<Real, DX, EXACT>(w + v * n, q, 1, m);
+        dv[v][1] = gd5<Real, DY, EXACT>(w + v * n, q, nx, m);
     }
     Real dzs[3] = {0, 0, 0};
     if (depth == 0) { // src/three_d/PointKernels3D.hpp:52-66
         const Real c[3] = {M[6], M[7], M[8]};
         const Real c2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2], len = sqrt(c2);
         const Real nn[3] = {c[0] / len, c[1] / len, c[2] / len};
-        Real g[9], tr[3] = {0, 0, 0};
+        Real g[9], t[3] = {0, 0, 0};
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
@@ -279,27 +278,26 @@ __device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Tap
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) tr[a] += ((a == b ? lam * trace : Real(0)) + mu * (g[3 * a + b] + g[3 * b + a])) * c[b];
-        const Real normal = tr[0] * nn[0] + tr[1] * nn[1] + tr[2] * nn[2];
+            for (int b = 0; b < 3; ++b) t[a] += ((a == b ? lam * trace : Real(0)) + mu * (g[3 * a + b] + g[3 * b + a])) * c[b];
+        const Real normal = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) dzs[a] = -(tr[a] - nn[a] * normal) / (mu * c2) - nn[a] * normal / ((lam + 2 * mu) * c2);
+        for (int a = 0; a < 3; ++a) dzs[a] = -(t[a] - nn[a] * normal) / (mu * c2) - nn[a] * normal / ((lam + 2 * mu) * c2);
     }
     Real gr[9][3];
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
         Real dx, dy, dz;
-        auto zt = [&](int o) { return t.z(f, o); };
         if (f < 3) {
             dx = dv[f][0];
             dy = dv[f][1];
             if (depth == 0) dz = dzs[f];
-            else if (depth == 1) dz = d2<Real, DZ, EXACT>(m, zt);
-            else if (depth == 2) dz = d3<Real, DZ, EXACT>(m, zt);
-            else dz = d5<Real, DZ, EXACT>(m, zt);
+            else if (depth == 1) dz = gd2<Real, DZ, EXACT>(w + f * n, q, plane, m);
+            else if (depth == 2) dz = gd3<Real, DZ, EXACT>(w + f * n, q, plane, m);
+            else dz = gd5<Real, DZ, EXACT>(w + f * n, q, plane, m);
         } else {
-            dx = d5<Real, DX, EXACT>(m, [&](int o) { return t.x(f, o); });
-            dy = d5<Real, DY, EXACT>(m, [&](int o) { return t.y(f, o); });
-            dz = d5<Real, DZ, EXACT>(m, zt);
+            dx = gd5<Real, DX, EXACT>(w + f * n, q, 1, m);
+            dy = gd5<Real, DY, EXACT>(w + f * n, q, nx, m);
+            dz = gd5<Real, DZ, EXACT>(w + f * n, q, plane, m);
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) gr[f][a] = M[a] * dx + M[3 + a] * dy + M[6 + a] * dz;
@@ -307,7 +305,7 @@ __device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Tap
     Real r[9];
     if (depth <= (DZ ? 3 : 1)) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, p.in, q, a, depth, rho);
+        for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, a, depth, rho);
     } else {
         r[0] = (gr[3][0] + gr[6][1] + gr[7][2]) / rho;
         r[1] = (gr[6][0] + gr[4][1] + gr[8][2]) / rho;
@@ -329,10 +327,9 @@ __device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Tap
     if (!(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
         const Real d = ld(m.damping + q);
 #pragma unroll
-        for (int f = 0; f < 9; ++f) r[f] -= d * t.c(f);
+        for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
     }
-    const long long sq = i + px * j; // surface index
-    finish3<Real, STAGE>(p, t, r, q, depth, sq);
+    const long long sq = i + nx * j; // surface index
     if (STAGE == 3 && depth == 0 && p.surfRate) {
         // traction-rate residual of k4 (src/three_d/CurvilinearSolver.cpp:231-239)
         const double n0 = ld(m.normals + 3 * sq), n1 = ld(m.normals + 3 * sq + 1), n2 = ld(m.normals + 3 * sq + 2);
@@ -345,26 +342,33 @@ __device__ __forceinline__ void generalNode3(const StageArgs<Real> &p, const Tap
         p.surfRate[sq] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
         p.surfRate[plane + sq] = sqrt(norm2);
     }
+    finish3<Real, STAGE>(p, r, q, depth, sq);
 }
 
 // The interior node (below the surface rows, outside the source support), with the sponge's
 // damping term when DAMP.  The stress fields are differentiated one at a time and their physical
 // gradients folded into the momentum sums as they come, in the reference's order
 // r0 = (gxx,x + gxy,y) + gxz,z, r1 = (gxy,x + gyy,y) + gyz,z, r2 = (gxz,x + gyz,y) + gzz,z
-// (src/three_d/PointKernels3D.hpp:92-112), so only a few gradients are live at a time.
+// (src/three_d/PointKernels3D.hpp:92-112), so only a few gradients are live at a time.  The
+// damping term is subtracted after all nine rates, as in the general form.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool DAMP>
-__device__ __forceinline__ void interiorNode3(const StageArgs<Real> &p, const Taps<Real> &t, int i, int j, int k) {
+__device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
-    const long long px = m.px;
-    const long long q = i + px * j + m.plane * k;
+    const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    if (i >= m.nx - 3 || j >= m.ny - 3) return;
+    const long long n = m.count, nx = m.px, plane = m.plane;
+    const long long q = i + nx * j + plane * k;
+    const Real *__restrict__ w = p.in;
     Real M[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) M[c] = ld(m.metric[c] + q);
     // physical gradient component a of field f: ((M_a dxi + M_3+a deta) + M_6+a dzeta)
     auto grad = [&](int f, Real (&g)[3], bool x, bool y, bool z) {
-        const Real dx = d5<Real, DX, EXACT>(m, [&](int o) { return t.x(f, o); });
-        const Real dy = d5<Real, DY, EXACT>(m, [&](int o) { return t.y(f, o); });
-        const Real dz = d5<Real, DZ, EXACT>(m, [&](int o) { return t.z(f, o); });
+        const Real dx = gd5<Real, DX, EXACT>(w + f * n, q, 1, m);
+        const Real dy = gd5<Real, DY, EXACT>(w + f * n, q, nx, m);
+        const Real dz = gd5<Real, DZ, EXACT>(w + f * n, q, plane, m);
         if (x) g[0] = M[0] * dx + M[3] * dy + M[6] * dz;
         if (y) g[1] = M[1] * dx + M[4] * dy + M[7] * dz;
         if (z) g[2] = M[2] * dx + M[5] * dy + M[8] * dz;
@@ -400,100 +404,35 @@ __device__ __forceinline__ void interiorNode3(const StageArgs<Real> &p, const Ta
     if (DAMP && !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
         const Real d = ld(m.damping + q);
 #pragma unroll
-        for (int f = 0; f < 9; ++f) r[f] -= d * t.c(f);
+        for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
     }
-    finish3<Real, STAGE>(p, t, r, q, 4, i + px * j);
+    finish3<Real, STAGE>(p, r, q, 4, i + nx * j);
 }
 
-// 4D tiled tensor copy global -> shared (no multicast), completing on `bar`.
-__device__ __forceinline__ void tmaLoad4(void *dst, const CUtensorMap *map, int x, int y, int z, int f, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
-            k2::smemAddr(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(f), "r"(k2::smemAddr(bar))
-        : "memory");
-}
-
-// One CTA: the 32 x 8 tile at (i0, j0) over planes [k0, k1).  Plane z lives in slot
-// (z - zb) % SLOTS, zb = k0 - LO being the first plane of the first window, and its copy completes
-// on that slot's mbarrier in phase ((z - zb) / SLOTS) & 1.  Thread 0 issues the five planes of
-// the first window, then one plane per step of the march: plane k+HI+1 goes into the slot of
-// plane k-LO-1, which every thread released at the end of step k-1.  Waits are bounded: a wait
-// that runs out flags the clock (`stalled`), lets the copies still in flight land, and the CTA stops.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
-__device__ __forceinline__ void streamBody3(const StageArgs<Real> &p, uint64_t *bar, Real *ring) {
-    constexpr int LO = DZ ? 3 : 1, HI = DZ ? 1 : 3; // z window of plane k: k-LO .. k+HI
-    constexpr unsigned slotBytes = SLOT_WORDS * sizeof(Real);
-    const Mesh<Real> &m = p.m;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
-    const int i0 = 3 + blockIdx.x * TX, j0 = 3 + blockIdx.y * TY;
-    const int k0 = 3 + blockIdx.z * m.seg, k1 = min(k0 + m.seg, m.nz - 3);
-    const int zb = k0 - LO, yb = j0 - (DY ? 3 : 1);
-    const int i = i0 + tx, j = j0 + ty;
-    const bool active = i < m.nx - 3 && j < m.ny - 3;
-    __shared__ int stop;
-    auto issue = [&](int z) {
-        const int s = (z - zb) % SLOTS;
-        k2::mbarExpectTx(bar + s, slotBytes);
-        tmaLoad4(ring + s * SLOT_WORDS, &p.inMap, i0 - 3, yb, z, 0, bar + s);
-    };
-    auto landed = [&](int z) { return k2::mbarWait(bar + (z - zb) % SLOTS, unsigned((z - zb) / SLOTS) & 1); };
-    if (tid == 0) {
-        stop = 0;
-        for (int s = 0; s < SLOTS; ++s) k2::mbarInit(bar + s, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-    if (tid == 0)
-        for (int z = zb; z <= k0 + HI; ++z) issue(z);
-    // The tile lies inside the zero-damping box (x, y) / overlaps the source support (x, y).
-    const bool inner = i0 >= m.dmp_i0 && i0 + TX <= m.dmp_i1 && j0 >= m.dmp_j0 && j0 + TY <= m.dmp_j1;
-    const bool srcTile = i0 < m.src_i1 && i0 + TX > m.src_i0 && j0 < m.src_j1 && j0 + TY > m.src_j0;
-    Taps<Real> t;
-    t.ring = ring;
-    t.local = (ty + (DY ? 3 : 1)) * BX + tx + 3;
-    int waited = zb - 1, issued = k0 + HI; // planes up to `waited` have landed, up to `issued` were issued
-#pragma unroll 1
-    for (int k = k0; k < k1; ++k) {
-        if (k + 1 < k1) {
-            if (tid == 0) issue(k + HI + 1);
-            issued = k + HI + 1;
-        }
-        bool ok = true;
-        for (int z = waited + 1; z <= k + HI; ++z) ok = landed(z) && ok;
-        if (!ok) stop = 1;
-        __syncthreads();
-        if (stop) break;
-        waited = k + HI;
-#pragma unroll
-        for (int o = -LO; o <= HI; ++o) t.slot[o + 3] = ((k + o - zb) % SLOTS) * SLOT_WORDS;
-        if (active) {
-            // the general form for the surface rows and the source support; the interior form
-            // elsewhere, with the damping term where the tile-plane reaches into the sponge
-            if (k < 7 || (srcTile && k >= m.src_k0 && k < m.src_k1)) generalNode3<Real, DX, DY, DZ, STAGE, EXACT>(p, t, i, j, k);
-            else if (inner && k < m.dmp_k1) interiorNode3<Real, DX, DY, DZ, STAGE, EXACT, false>(p, t, i, j, k);
-            else interiorNode3<Real, DX, DY, DZ, STAGE, EXACT, true>(p, t, i, j, k);
-        }
-        __syncthreads(); // plane k-LO's slot is free
-    }
-    if (stop && tid == 0) { // a copy wait ran out: flag it and let the copies still in flight land
-        atomicExch(const_cast<int *>(&p.clock->stalled), 1);
-        for (int z = waited + 1; z <= issued; ++z) landed(z);
-    }
+__device__ __forceinline__ void stageNode3(const StageArgs<Real> &p, bool general, bool sponge) {
+    if (general) stageBody3<Real, DX, DY, DZ, STAGE, EXACT>(p);
+    else if (sponge) stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, true>(p);
+    else stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, false>(p);
 }
 
-// One RK stage of a 3D shot: grid (x tiles, y tiles, z segments), block 32 x 8.  DX/DY/DZ:
-// MacCormack directions of this (step, stage); STAGE: 0..3.
+// One RK stage of a 3D shot: block 32x8 nodes of one z layer.  CTAs on the surface rows or on
+// the source support run the general form; the others run the interior form, with the damping
+// term when the CTA reaches into the sponge (so the sponge costs nine multiply-adds, not the
+// general form).
 template <class Real, int DX, int DY, int DZ, int STAGE>
-__global__ void __launch_bounds__(TX *TY, (streamBlocks3<Real>())) stream3d(const __grid_constant__ StageArgs<Real> p) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    if (p.clock->faulted) return; // uniform across the grid
-    unsigned char *base = smemRaw + ((128 - (k2::smemAddr(smemRaw) & 127)) & 127);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(base);
-    Real *ring = reinterpret_cast<Real *>(base + 128);
-    if constexpr (sizeof(Real) == 4) streamBody3<Real, DX, DY, DZ, STAGE, true>(p, bar, ring);
-    else if (p.m.hinvExact) streamBody3<Real, DX, DY, DZ, STAGE, true>(p, bar, ring);
-    else streamBody3<Real, DX, DY, DZ, STAGE, false>(p, bar, ring);
+__global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __grid_constant__ StageArgs<Real> p) {
+    const Mesh<Real> &m = p.m;
+    if (p.clock->faulted) return;
+    const int i0 = 3 + blockIdx.x * blockDim.x, i1 = i0 + blockDim.x, j0 = 3 + blockIdx.y * blockDim.y, j1 = j0 + blockDim.y;
+    const int k = 3 + blockIdx.z;
+    const bool surface = k < 7;
+    const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
+    const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
+    const bool general = surface || source;
+    if constexpr (sizeof(Real) == 4) stageNode3<Real, DX, DY, DZ, STAGE, true>(p, general, sponge);
+    else if (m.hinvExact) stageNode3<Real, DX, DY, DZ, STAGE, true>(p, general, sponge);
+    else stageNode3<Real, DX, DY, DZ, STAGE, false>(p, general, sponge);
 }
 
 struct Partial {
