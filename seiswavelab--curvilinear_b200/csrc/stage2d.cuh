@@ -57,6 +57,7 @@ struct Clock {
     int stalled;     // set by a stage kernel whose copy wait ran out (the host reports an error)
     double peak_energy;
     double energy, max_velocity, traction;
+    double peaks[5]; // 3D: |Vz|, |Vx|, |Vy|, |V|, |mean stress| of the last accepted step
     int finite;
     int accepted;    // steps accepted in this batch
     double dt, growth_after; // energy-growth rule applies when (step+1)*dt > growth_after
@@ -424,6 +425,15 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
     Real r3 = lam * div + 2 * mu * dzv[1];
     Real r4 = mu * (dzv[0] + dxv[1]);
     if (MECH) {
+        // The accumulator words of the 4L memory fields and of Syy are loaded before the first
+        // store: a store could alias them as far as the compiler knows, so loading each after the
+        // previous field's store would serialise 4L+1 round trips per node.  (The other words are
+        // read-only loads, which the compiler may move.)
+        constexpr int NM = 4 * MECH + 1; // memory fields 6 .. 6+4L-1, then Syy (field 5)
+        Real am[NM];
+#pragma unroll
+        for (int j = 0; j < NM; ++j) am[j] = STAGE ? p.acc[(j < 4 * MECH ? 6 + j : 5) * n + q] : Real(0);
+        const Real w5 = damped ? ld(w + 5 * n + q) : Real(0);
         Real r5 = lam * div;
 #pragma unroll
         for (int l = 0; l < MECH; ++l) {
@@ -443,15 +453,15 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 if (damped) rm -= damp * wm[f];
                 const long long at = (mm + f) * n + q;
                 Real an;
-                const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), rm, KAHAN3 ? p.cin[at] : Real(0), an);
+                const Real o = combine<Real, STAGE>(p, am[4 * l + f], ld(p.base + at), rm, KAHAN3 ? ld(p.cin + at) : Real(0), an);
                 store<Real, STAGE>(p, at, o, an);
                 if (withDiag && !isfinite(o)) diag.bad = 1;
             }
         }
-        if (damped) r5 -= damp * ld(w + 5 * n + q);
+        if (damped) r5 -= damp * w5;
         const long long at = 5 * n + q;
         Real an;
-        const Real o = combine<Real, STAGE>(p, STAGE ? p.acc[at] : Real(0), ld(p.base + at), r5, KAHAN3 ? p.cin[at] : Real(0), an);
+        const Real o = combine<Real, STAGE>(p, am[NM - 1], ld(p.base + at), r5, KAHAN3 ? ld(p.cin + at) : Real(0), an);
         store<Real, STAGE>(p, at, o, an);
         if (withDiag && !isfinite(o)) diag.bad = 1;
     }
