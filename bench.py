@@ -19,11 +19,16 @@ nodes (absorber strips included, ghosts excluded) x steps / time.
 """
 from __future__ import annotations
 
+import os
+
+# More hardware work queues than the default 8, so that the serving leg's per-shot streams do not
+# share queues and serialise behind one another; it must be set before the CUDA context exists.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import argparse
 import ctypes as C
 import importlib.util
 import json
-import os
 import statistics
 import subprocess
 import sys
@@ -517,7 +522,7 @@ def main():
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")
     ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
     ap.add_argument("--serving-batch", type=int, default=64, help="steps per batch of a served shot")
-    ap.add_argument("--serving-active", type=int, default=16, help="shots built or running at once (0: memory-bound only)")
+    ap.add_argument("--serving-active", type=int, default=32, help="shots built or running at once (0: memory-bound only)")
     ap.add_argument("--serving-rate", type=float, default=0.0,
                     help="arrivals per second (0: 20/s of the full mix scaled by the work shrink factor)")
     args = ap.parse_args()

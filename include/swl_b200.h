@@ -117,6 +117,11 @@ swl_status swl2d_wait(swl2d_engine *engine, int32_t *accepted);
 swl_status swl2d_rollback(swl2d_engine *engine);    /* CudaEngine::rollback */
 swl_status swl2d_reset(swl2d_engine *engine);       /* CudaEngine::reset: zero fields, memories, traces */
 swl_status swl2d_diagnostics(swl2d_engine *engine, swl_diag2d *out); /* CudaEngine::diagnostics */
+/* The diagnostics of the last accepted step as the device-side acceptance verdict computed them
+ * (the energy, peak |v|, traction ratio and finiteness that CudaEngine2D.cu:155-162 reads back after
+ * every step), returned from the step clock that comes back with each batch: no kernel and no
+ * synchronisation.  Before the first batch (or after reset/load) it equals swl2d_diagnostics. */
+swl_status swl2d_step_diagnostics(swl2d_engine *engine, swl_diag2d *out);
 /* CudaEngine::sample: Vx, Vz of the current state at every receiver (FP64). */
 swl_status swl2d_sample(swl2d_engine *engine, double *vx, double *vz);
 /* Raw per-step receiver samples recorded by swl2d_advance for steps
@@ -248,6 +253,7 @@ swl_status swl3d_wait(swl3d_engine *engine, int32_t *accepted);
 swl_status swl3d_rollback(swl3d_engine *engine);
 swl_status swl3d_reset(swl3d_engine *engine);
 swl_status swl3d_diagnostics(swl3d_engine *engine, swl_diag3d *out);
+swl_status swl3d_step_diagnostics(swl3d_engine *engine, swl_diag3d *out); /* as swl2d_step_diagnostics */
 swl_status swl3d_sample(swl3d_engine *engine, double *vx, double *vy, double *vz);
 swl_status swl3d_traces(swl3d_engine *engine, int32_t first, int32_t count, double *vx, double *vy, double *vz);
 swl_status swl3d_snapshot(swl3d_engine *engine, int32_t field, double *out);

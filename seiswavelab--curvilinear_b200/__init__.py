@@ -111,6 +111,7 @@ def library() -> C.CDLL:
     L.swl2d_rollback.argtypes = [C.c_void_p]
     L.swl2d_reset.argtypes = [C.c_void_p]
     L.swl2d_diagnostics.argtypes = [C.c_void_p, C.POINTER(Diag2D)]
+    L.swl2d_step_diagnostics.argtypes = [C.c_void_p, C.POINTER(Diag2D)]
     L.swl2d_sample.argtypes = [C.c_void_p, _dp, _dp]
     L.swl2d_traces.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp]
     L.swl2d_snapshot.argtypes = [C.c_void_p, C.c_int32, _dp]
@@ -126,6 +127,7 @@ def library() -> C.CDLL:
     L.swl3d_rollback.argtypes = [C.c_void_p]
     L.swl3d_reset.argtypes = [C.c_void_p]
     L.swl3d_diagnostics.argtypes = [C.c_void_p, C.POINTER(Diag3D)]
+    L.swl3d_step_diagnostics.argtypes = [C.c_void_p, C.POINTER(Diag3D)]
     L.swl3d_sample.argtypes = [C.c_void_p, _dp, _dp, _dp]
     L.swl3d_traces.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp, _dp, _dp]
     L.swl3d_snapshot.argtypes = [C.c_void_p, C.c_int32, _dp]
@@ -260,6 +262,12 @@ class Engine2D:
         _check(library().swl2d_diagnostics(self._h, C.byref(d)))
         return {k: getattr(d, k) for k, _ in Diag2D._fields_}
 
+    def step_diagnostics(self) -> dict:
+        """The last accepted step's diagnostics as the device verdict computed them (no kernel)."""
+        d = Diag2D()
+        _check(library().swl2d_step_diagnostics(self._h, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in Diag2D._fields_}
+
     def sample(self):
         vx, vz = np.zeros(self.nrec), np.zeros(self.nrec)
         _check(library().swl2d_sample(self._h, vx.ctypes.data_as(_dp), vz.ctypes.data_as(_dp)))
@@ -366,6 +374,14 @@ class Engine3D:
     def diagnostics(self) -> dict:
         d = Diag3D()
         _check(library().swl3d_diagnostics(self._h, C.byref(d)))
+        out = {k: getattr(d, k) for k, _ in Diag3D._fields_}
+        out["peaks"] = list(d.peaks)
+        return out
+
+    def step_diagnostics(self) -> dict:
+        """The last accepted step's diagnostics as the device verdict computed them (no kernel)."""
+        d = Diag3D()
+        _check(library().swl3d_step_diagnostics(self._h, C.byref(d)))
         out = {k: getattr(d, k) for k, _ in Diag3D._fields_}
         out["peaks"] = list(d.peaks)
         return out

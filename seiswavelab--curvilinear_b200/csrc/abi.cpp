@@ -156,6 +156,13 @@ swl_status swl2d_diagnostics(swl2d_engine *e, swl_diag2d *out) {
         E.diagnostics(*out);
     });
 }
+swl_status swl2d_step_diagnostics(swl2d_engine *e, swl_diag2d *out) {
+    return guarded([&] {
+        ENGINE(e);
+        need(out, "out");
+        E.stepDiagnostics(*out);
+    });
+}
 swl_status swl2d_sample(swl2d_engine *e, double *vx, double *vz) {
     return guarded([&] {
         ENGINE(e);
@@ -284,6 +291,13 @@ swl_status swl3d_diagnostics(swl3d_engine *e, swl_diag3d *out) {
         ENGINE(e);
         need(out, "out");
         E.diagnostics(*out);
+    });
+}
+swl_status swl3d_step_diagnostics(swl3d_engine *e, swl_diag3d *out) {
+    return guarded([&] {
+        ENGINE(e);
+        need(out, "out");
+        E.stepDiagnostics(*out);
     });
 }
 swl_status swl3d_sample(swl3d_engine *e, double *vx, double *vy, double *vz) {

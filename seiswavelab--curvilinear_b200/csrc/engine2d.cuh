@@ -34,6 +34,9 @@ class Engine2D {
     virtual void rollback() = 0;
     virtual void reset() = 0;
     virtual void diagnostics(swl_diag2d &) = 0;
+    // Diagnostics of the last accepted step as the device verdict recorded them (read back with
+    // the batch): no kernel and no synchronisation.  Before any step, the same as diagnostics().
+    virtual void stepDiagnostics(swl_diag2d &) = 0;
     virtual void sample(double *vx, double *vz) = 0;
     virtual void traces(int first, int count, double *vx, double *vz) = 0;
     virtual void snapshot(int field, double *out) = 0;
@@ -130,7 +133,9 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     dim3 stageGrid_, stageBlock_{32, 8}; // strips of 32 columns x segments of 8*seg rows
     int nparts_{};
     k2::Clock hostClock_{};
-    PinnedBuffer pinnedForcing_, pinnedClock_;
+    PinnedBuffer pinnedForcing_, pinnedClock_, pinnedTraces_;
+    int pinnedRows_{0};     // trace rows of the last launched batch copied to pinnedTraces_ with it
+    bool clockStats_{false}; // the host clock holds a verdict's diagnostics
     std::map<int, cudaGraphExec_t> graphs_;
     bool faulted_{false};
     int registers_{};
@@ -235,6 +240,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             dropGraphs();
         }
         pinnedForcing_.reserve(std::size_t(steps) * 3 * sizeof(Real));
+        pinnedTraces_.reserve(std::max<std::size_t>(1, std::size_t(traceCap_) * nrec_ * 2) * sizeof(double));
     }
     void fillForcing(int first, int count, double dt, double frequency, double scale) {
         Real *f = pinnedForcing_.as<Real>();
@@ -476,6 +482,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         stream_ = s ? s : ownStream_;
     }
     void profile(int first, int count, double dt, double frequency, double scale, swl_profile &out) override {
+        pinnedRows_ = 0, clockStats_ = false;
         settle();
         DeviceScope scope(device_);
         if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
@@ -525,6 +532,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         fillForcing(step, 1, dt, frequency, scale);
         enqueueStep(step, false);
         previous_ = true;
+        pinnedRows_ = 0, clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "2D step completion");
     }
 
@@ -603,6 +611,13 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             done += 8; // eight role swaps: roles are back where they started
         }
         for (; done < count; ++done) enqueueStep(first + done, true);
+        // the batch's trace rows and clock come back with it, so that reading them needs no copy
+        if (nrec_)
+            check(cudaMemcpyAsync(pinnedTraces_.ptr, traces_.ptr, std::size_t(count) * nrec_ * 2 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "read traces");
+        pinnedRows_ = count;
+        clockStats_ = true;
         check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
         check(cudaEventRecord(done_, stream_), "record batch completion");
         batchU0_ = u0;
@@ -622,6 +637,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         check(cudaMemsetAsync(psets_.ptr, 0, psets_.bytes, stream_), "2D PML reset");
         if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "2D trace reset");
         hostClock_ = k2::Clock{};
+        pinnedRows_ = 0, clockStats_ = false;
         pushClock();
         check(cudaStreamSynchronize(stream_), "2D clear completion");
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
@@ -645,6 +661,16 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             d.finite &= !p.bad;
         }
         d.finite &= std::isfinite(d.energy) ? 1 : 0;
+        d.peak_energy = hostClock_.peak_energy;
+        d.rhs_registers = registers_;
+        d.rhs_local_bytes = localBytes_;
+        d.resident_bytes = residentBytes();
+    }
+    void stepDiagnostics(swl_diag2d &d) override {
+        settle();
+        if (!clockStats_) return diagnostics(d);
+        d.energy = hostClock_.energy, d.max_velocity = hostClock_.max_velocity, d.traction_relative = hostClock_.traction;
+        d.finite = hostClock_.finite;
         d.peak_energy = hostClock_.peak_energy;
         d.rhs_registers = registers_;
         d.rhs_local_bytes = localBytes_;
@@ -678,11 +704,16 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         const int row0 = first - hostClock_.first;
         if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
             throw Error(SWL_ERR_INVALID, "requested trace rows were not recorded by the last advance");
-        std::vector<double> buf(std::size_t(count) * nrec_ * 2);
-        if (!buf.empty())
-            check(cudaMemcpy(buf.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 2, buf.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost),
-                  "trace readback");
+        std::vector<double> copy;
+        const double *buf = pinnedTraces_.as<double>() + std::size_t(row0) * nrec_ * 2;
+        if (row0 + count > pinnedRows_) { // rows recorded outside an asynchronous batch
+            copy.resize(std::size_t(count) * nrec_ * 2);
+            if (!copy.empty())
+                check(cudaMemcpy(copy.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 2, copy.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost),
+                      "trace readback");
+            buf = copy.data();
+        }
         for (int r = 0; r < nrec_; ++r)
             for (int j = 0; j < count; ++j) {
                 vx[std::size_t(r) * count + j] = buf[(std::size_t(j) * nrec_ + r) * 2];
@@ -710,6 +741,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     void load(int field, const double *in) override {
         settle();
         DeviceScope scope(device_);
+        clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "load ordering");
         Real *dst;
         std::size_t len;

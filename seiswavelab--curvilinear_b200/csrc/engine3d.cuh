@@ -21,6 +21,9 @@ class Engine3D {
     virtual void rollback() = 0;
     virtual void reset() = 0;
     virtual void diagnostics(swl_diag3d &) = 0;
+    // Diagnostics of the last accepted step as the device verdict recorded them (read back with
+    // the batch): no kernel and no synchronisation.  Before any step, the same as diagnostics().
+    virtual void stepDiagnostics(swl_diag3d &) = 0;
     virtual void sample(double *vx, double *vy, double *vz) = 0;
     virtual void traces(int first, int count, double *vx, double *vy, double *vz) = 0;
     virtual void snapshot(int field, double *out) = 0;
@@ -84,7 +87,9 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     dim3 grid_, block_{32, 8, 1};
     int nparts_{};
     k2::Clock hostClock_{};
-    PinnedBuffer pinnedForcing_, pinnedClock_;
+    PinnedBuffer pinnedForcing_, pinnedClock_, pinnedTraces_;
+    int pinnedRows_{0};     // trace rows of the last launched batch copied to pinnedTraces_ with it
+    bool clockStats_{false}; // the host clock holds a verdict's diagnostics
     std::map<int, cudaGraphExec_t> graphs_;
     bool faulted_{false};
     int registers_{};
@@ -187,6 +192,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             dropGraphs();
         }
         pinnedForcing_.reserve(std::size_t(steps) * 3 * sizeof(Real));
+        pinnedTraces_.reserve(std::max<std::size_t>(1, std::size_t(traceCap_) * nrec_ * 3) * sizeof(double));
     }
     // src/three_d/CurvilinearSolver.cpp:75-77 (scale = amplitude / (rho0 h^3)).
     double source(double t, double f) const {
@@ -350,6 +356,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         stream_ = s ? s : ownStream_;
     }
     void profile(int first, int count, double dt, double frequency, swl_profile &out) override {
+        pinnedRows_ = 0, clockStats_ = false;
         settle();
         DeviceScope scope(device_);
         if (count <= 0) throw Error(SWL_ERR_INVALID, "profile needs count > 0");
@@ -397,6 +404,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         fillForcing(step, 1, dt, frequency);
         enqueueStep(step, false);
         previous_ = true;
+        pinnedRows_ = 0, clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "3D step completion");
     }
     int advance(int first, int count, double dt, double frequency, double growthAfter) override {
@@ -469,6 +477,13 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             done += 8;
         }
         for (; done < count; ++done) enqueueStep(first + done, true);
+        // the batch's trace rows and clock come back with it, so that reading them needs no copy
+        if (nrec_)
+            check(cudaMemcpyAsync(pinnedTraces_.ptr, traces_.ptr, std::size_t(count) * nrec_ * 3 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "read traces");
+        pinnedRows_ = count;
+        clockStats_ = true;
         check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
         check(cudaEventRecord(done_, stream_), "record batch completion");
         batchU0_ = u0;
@@ -488,6 +503,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "3D trace reset");
         check(cudaMemsetAsync(surfRate_.ptr, 0, surfRate_.bytes, stream_), "3D surface reset");
         hostClock_ = k2::Clock{};
+        pinnedRows_ = 0, clockStats_ = false;
         pushClock();
         check(cudaStreamSynchronize(stream_), "3D clear completion");
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
@@ -517,6 +533,17 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         d.rhs_registers = registers_;
         d.resident_bytes = residentBytes();
     }
+    void stepDiagnostics(swl_diag3d &d) override {
+        settle();
+        if (!clockStats_) return diagnostics(d);
+        d.energy = hostClock_.energy, d.max_velocity = hostClock_.max_velocity;
+        d.traction_rate_relative = hostClock_.traction;
+        for (int c = 0; c < 5; ++c) d.peaks[c] = hostClock_.peaks[c];
+        d.finite = hostClock_.finite;
+        d.peak_energy = hostClock_.peak_energy;
+        d.rhs_registers = registers_;
+        d.resident_bytes = residentBytes();
+    }
     void sample(double *vx, double *vy, double *vz) override {
         settle();
         DeviceScope scope(device_);
@@ -538,11 +565,16 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         const int row0 = first - hostClock_.first;
         if (count < 0 || row0 < 0 || row0 + count > hostClock_.accepted)
             throw Error(SWL_ERR_INVALID, "requested trace rows were not recorded by the last advance");
-        std::vector<double> buf(std::size_t(count) * nrec_ * 3);
-        if (!buf.empty())
-            check(cudaMemcpy(buf.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 3, buf.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost),
-                  "trace readback");
+        std::vector<double> copy;
+        const double *buf = pinnedTraces_.as<double>() + std::size_t(row0) * nrec_ * 3;
+        if (row0 + count > pinnedRows_) { // rows recorded outside an asynchronous batch
+            copy.resize(std::size_t(count) * nrec_ * 3);
+            if (!copy.empty())
+                check(cudaMemcpy(copy.data(), traces_.as<double>() + std::size_t(row0) * nrec_ * 3, copy.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost),
+                      "trace readback");
+            buf = copy.data();
+        }
         for (int r = 0; r < nrec_; ++r)
             for (int j = 0; j < count; ++j) {
                 const std::size_t at = (std::size_t(j) * nrec_ + r) * 3, to = std::size_t(r) * count + j;
@@ -565,6 +597,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         settle();
         DeviceScope scope(device_);
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
+        clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "load ordering");
         std::vector<Real> tmp(count_, Real(0));
         const long long rows = (long long)m_.ny * m_.nz;

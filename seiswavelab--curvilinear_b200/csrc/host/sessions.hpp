@@ -138,7 +138,7 @@ struct Session2D {
         lastMs = millis(batchStart) / std::max(1, accepted);
         totalMs += millis(batchStart);
         inflight = 0;
-        ok(swl2d_diagnostics(engine, &diag));
+        ok(swl2d_step_diagnostics(engine, &diag));
         if (st == SWL_ERR_FAULT) {
             fault = "2D step rejected: nonfinite fields or excessive late energy growth. Rebuild the session.";
             throw Failure(SWL_ERR_FAULT, fault);
@@ -302,7 +302,7 @@ struct Session3D {
         lastMs = millis(batchStart) / std::max(1, accepted);
         totalMs += millis(batchStart);
         inflight = 0;
-        ok(swl3d_diagnostics(engine, &diag));
+        ok(swl3d_step_diagnostics(engine, &diag));
         if (st == SWL_ERR_FAULT) {
             fault = "Non-finite RK4 step or energy growth above 10,000 times the source-window peak rejected. "
                     "Last accepted step retained; rebuild with smaller CFL or gentler terrain.";

@@ -552,6 +552,7 @@ __global__ void __launch_bounds__(512) verdict3d(const Partial *__restrict__ par
             clk->energy = tot.energy;
             clk->max_velocity = tot.velocity;
             clk->traction = ratio;
+            for (int c = 0; c < 5; ++c) clk->peaks[c] = tot.peak[c];
         }
         accept = ok;
     }

@@ -166,3 +166,21 @@ def test_identical_engines_give_identical_results(precision, swl):
         out.append((e.fields(), e.traces(0, 24)))
     np.testing.assert_array_equal(out[0][0], out[1][0])
     np.testing.assert_array_equal(out[0][1][0], out[1][1][0])
+
+
+@pytest.mark.parametrize("precision", ["SWL_FP32", "SWL_FP64"])
+def test_step_diagnostics_match_full_diagnostics(precision, swl):
+    # The verdict's per-step numbers (read back with the batch) agree with a full pass over the
+    # state; only the order of the energy sum differs.
+    case, res, mesh = load_2d("gsls3_cpml_surface_force")
+    dt, f, s = float(res["dt"]), mesh["frequency"], mesh["scale"]
+    e = swl.Engine2D(mesh, receivers_2d(res), precision=getattr(swl, precision))
+    before = e.step_diagnostics()
+    assert before["energy"] == e.diagnostics()["energy"]
+    e.advance(0, 20, dt, f, s)
+    quick, full = e.step_diagnostics(), e.diagnostics()
+    assert quick["finite"] == full["finite"] == 1
+    assert quick["energy"] == pytest.approx(full["energy"], rel=1e-12)
+    assert quick["max_velocity"] == pytest.approx(full["max_velocity"], rel=1e-14)
+    assert quick["traction_relative"] == pytest.approx(full["traction_relative"], rel=1e-14)
+    assert quick["peak_energy"] == full["peak_energy"]

@@ -75,3 +75,15 @@ def test_diagnostics(swl):
     assert d["finite"] == 1
     assert d["energy"] == pytest.approx(float(res["energy"]), rel=1e-9)
     assert d["max_velocity"] == pytest.approx(float(res["maxAbsVelocity"]), rel=1e-12)
+
+
+def test_step_diagnostics_match_full_diagnostics(swl):
+    # the verdict's per-step numbers, read back with the batch, agree with a full pass over the state
+    case, res, mesh = load_3d("force")
+    e, _ = run(swl, mesh, res, swl.SWL_FP64)
+    quick, full = e.step_diagnostics(), e.diagnostics()
+    assert quick["finite"] == full["finite"] == 1
+    assert quick["energy"] == pytest.approx(full["energy"], rel=1e-12)
+    assert quick["max_velocity"] == pytest.approx(full["max_velocity"], rel=1e-14)
+    assert quick["traction_rate_relative"] == pytest.approx(full["traction_rate_relative"], rel=1e-14)
+    assert quick["peaks"] == pytest.approx(full["peaks"], rel=1e-14)
