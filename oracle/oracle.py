@@ -263,6 +263,10 @@ def _load_dir(d: Path) -> dict:
     res = _meta(d / "meta.txt")
     for f in d.glob("*.bin"):
         res[f.stem] = np.fromfile(f, dtype=np.float64)
+    for f in d.glob("*.csv"):  # the reference's receiver CSV files, as text
+        res["csv:" + f.stem] = f.read_text()
+    for f in d.glob("*.sgy"):  # its SEG-Y exports of the session records, as bytes
+        res["sgy:" + f.stem] = f.read_bytes()
     return res
 
 

@@ -33,6 +33,7 @@
 #ifdef SEIS3D_HAS_OPENMP
 #include <omp.h>
 #endif
+#include "SeisCommon/SegyIo.hpp"
 #define private public
 #include "CurvilinearSolver2D.cpp"
 #undef private
@@ -225,6 +226,29 @@ int main(int argc, char **argv) {
         }
         write(out, "tracesVx.bin", vx);
         write(out, "tracesVz.bin", vz);
+        { // the reference's receiver CSV (writeReceivers, CurvilinearSolver2D.cpp:811-855)
+            std::string csvError;
+            if (!writeReceivers(sim, out / "receivers.csv", csvError)) std::ofstream(out / "csv_error.txt") << csvError << '\n';
+        }
+        { // the workbench's record view (src/two_d/ui/Workbench2D.cpp:251-268) through writeSegy
+            SeisWave::RecordDataView data;
+            data.dt = sim.recordDt();
+            data.components = {"Vz", "Vx"};
+            const auto &p = sim.parameters();
+            const auto src = sim.grid().coordinates[sim.grid().modelIndex(p.sourceX < 0 ? p.nx / 2 : p.sourceX, p.sourceZ)];
+            for (const auto &r : sim.receivers()) {
+                SeisWave::TraceView t;
+                t.position = {r.position[0], 0, r.position[1]};
+                t.source = {src[0], 0, src[1]};
+                t.channels[0] = r.vz;
+                t.channels[1] = r.vx;
+                data.traces.push_back(t);
+            }
+            std::string segyError;
+            if (!SeisWave::writeSegy(data, 0, out / "vz_ieee32.sgy", segyError, false) ||
+                !SeisWave::writeSegy(data, 1, out / "vx_ieee64.sgy", segyError, true))
+                std::ofstream(out / "segy_error.txt") << segyError << '\n';
+        }
         const auto &d = sim.diagnostics();
         std::ofstream meta(out / "meta.txt");
         meta.imbue(std::locale::classic());

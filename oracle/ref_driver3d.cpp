@@ -28,8 +28,10 @@
 #include <omp.h>
 #endif
 #include <unistd.h>
+#include "SeisCommon/SegyIo.hpp"
 #define private public
 #include "CurvilinearSolver.cpp"
+#include "Seis3D/ReceiverIo.hpp"
 #undef private
 
 using namespace Seis3D::Curvilinear;
@@ -195,6 +197,27 @@ int main(int argc, char **argv) {
         write(out, "tracesVx.bin", vx);
         write(out, "tracesVy.bin", vy);
         write(out, "tracesVz.bin", vz);
+        { // the reference's receiver CSV files (src/three_d/ReceiverIo.cpp): all components, and Vx+Vz
+            std::string csvError;
+            if (!writeReceiversCsv(sim, out / "receivers.csv", {true, true, true}, csvError) ||
+                !writeReceiversCsv(sim, out / "receivers_xz.csv", {true, false, true}, csvError))
+                std::ofstream(out / "csv_error.txt") << csvError << '\n';
+        }
+        { // the record view of src/three_d/ui/RecordView3D.cpp:5-6 through writeSegy
+            SeisWave::RecordDataView data;
+            data.dt = sim.dt();
+            data.components = {"Vz", "Vx", "Vy"};
+            for (const auto &trace : sim.receivers()) {
+                SeisWave::TraceView t;
+                t.position = trace.position;
+                t.channels = {trace.samples, trace.samplesVx, trace.samplesVy};
+                data.traces.push_back(t);
+            }
+            std::string segyError;
+            if (!SeisWave::writeSegy(data, 0, out / "vz_ieee32.sgy", segyError, false) ||
+                !SeisWave::writeSegy(data, 2, out / "vy_ieee64.sgy", segyError, true))
+                std::ofstream(out / "segy_error.txt") << segyError << '\n';
+        }
         const auto &d = sim.diagnostics();
         std::ofstream meta(out / "meta.txt");
         meta.imbue(std::locale::classic());

@@ -41,6 +41,7 @@ UNITS = {
     "host/model3d.cpp": [],
     "host/session.cpp": [],
     "host/server.cpp": [],
+    "host/records.cpp": [],
 }
 
 

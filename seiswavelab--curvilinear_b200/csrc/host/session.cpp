@@ -3,6 +3,12 @@
 // (one host synchronisation per batch, the acceptance rule applied on the device) and keeps the
 // receiver records exactly as the reference sessions do.
 #include "sessions.hpp"
+#include "records.hpp"
+#include "../../../include/swl_records.h"
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <locale>
 
 
 using swl::host::guard;
@@ -22,6 +28,64 @@ template <class S> swl_status modelArray(const S *s, const char *name, double *o
         *n = int64_t(v->size());
         if (out && !v->empty()) std::memcpy(out, v->data(), v->size() * sizeof(double));
     });
+}
+// include/SeisCommon/SourceMechanism.hpp:32-38: the unit force direction (zero for a moment)
+std::array<double, 3> unitDirection(int kind, const std::array<double, 3> &d) {
+    if (kind == 1) return {0, 0, 0};
+    const double norm = std::hypot(d[0], d[1], d[2]);
+    return {d[0] / norm, d[1] / norm, d[2] / norm};
+}
+const char *const kBackend = "swl_b200 CUDA sm_100a";
+
+// The record set of a 2D session as src/two_d/ui/Workbench2D.cpp:251-268 builds it: components Vz,
+// Vx; receivers at (x, 0, z); the source node's coordinates (x, 0, z); the record axis's dt.
+swl::records::RecordSet records2d(const swl::host::Session2D &s) {
+    const auto &m = s.model;
+    const auto &p = s.params;
+    swl::records::RecordSet rec;
+    rec.dt = m.recordDt;
+    rec.components = {"Vz", "Vx"};
+    rec.samples = s.vx.empty() ? 0 : s.vx.front().size();
+    const int sx = (p.sourceX < 0 ? p.nx / 2 : p.sourceX) + 3 + m.modelOffsetX, sz = p.sourceZ + 3; // Grid::modelIndex
+    const std::size_t node = std::size_t(sx) + std::size_t(m.nx) * std::size_t(sz);
+    const double srcX = m.coordinates[2 * node], srcZ = m.coordinates[2 * node + 1];
+    for (std::size_t r = 0; r < s.vx.size(); ++r) {
+        swl::records::Trace t;
+        t.position = {m.receiverPositions[r][0], 0, m.receiverPositions[r][1]};
+        t.source = {srcX, 0, srcZ};
+        t.channel = {s.vz[r].data(), s.vx[r].data(), nullptr};
+        rec.traces.push_back(t);
+    }
+    return rec;
+}
+// src/three_d/ui/RecordView3D.cpp:5-6: components Vz, Vx, Vy; the solver's dt.
+swl::records::RecordSet records3d(const swl::host::Session3D &s) {
+    swl::records::RecordSet rec;
+    rec.dt = s.model.dt;
+    rec.components = {"Vz", "Vx", "Vy"};
+    rec.samples = s.rec[2].empty() ? 0 : s.rec[2].front().size();
+    for (std::size_t r = 0; r < s.rec[2].size(); ++r) {
+        swl::records::Trace t;
+        t.position = s.model.receiverPositions[r];
+        t.channel = {s.rec[2][r].data(), s.rec[0][r].data(), s.rec[1][r].data()};
+        rec.traces.push_back(t);
+    }
+    return rec;
+}
+swl::records::SegyOptions segyOptions(const swl_segy_options *o) {
+    if (!o) throw swl::host::Failure(SWL_ERR_INVALID, "options are required");
+    return {o->profile, o->sample_gain, o->sample_interval_s};
+}
+std::ofstream csvFile(const char *path, const char *emptyName, const char *cannotCreate) {
+    if (!path) throw swl::host::Failure(SWL_ERR_INVALID, "path is null");
+    const std::filesystem::path file(path);
+    if (file.empty() || file.filename().empty()) throw swl::host::Failure(SWL_ERR_INVALID, emptyName);
+    if (!file.parent_path().empty()) std::filesystem::create_directories(file.parent_path());
+    std::ofstream out(file);
+    if (!out) throw swl::host::Failure(SWL_ERR_INVALID, cannotCreate);
+    out.imbue(std::locale::classic());
+    out << std::setprecision(17);
+    return out;
 }
 } // namespace
 
@@ -192,5 +256,102 @@ swl_status swl3d_session_snapshot(swl3d_session *s, int32_t field, double *out) 
 }
 swl_status swl3d_session_model(const swl3d_session *s, const char *name, double *out, int64_t *n) { return modelArray(s, name, out, n); }
 swl3d_engine *swl3d_session_engine(swl3d_session *s) { return s ? s->engine : nullptr; }
+
+
+// ------------------------------------------------------------------------- record output
+swl_status swl2d_session_write_segy(const swl2d_session *s, int32_t component, const char *path, const swl_segy_options *o) {
+    return guard([&] {
+        needSession(s);
+        if (!path) throw swl::host::Failure(SWL_ERR_INVALID, "path is null");
+        swl::records::writeSegy(records2d(*s), component, path, segyOptions(o));
+    });
+}
+swl_status swl3d_session_write_segy(const swl3d_session *s, int32_t component, const char *path, const swl_segy_options *o) {
+    return guard([&] {
+        needSession(s);
+        if (!path) throw swl::host::Failure(SWL_ERR_INVALID, "path is null");
+        swl::records::writeSegy(records3d(*s), component, path, segyOptions(o));
+    });
+}
+// writeReceivers (src/two_d/CurvilinearSolver2D.cpp:811-855): the run's metadata as comment lines,
+// then one row per receiver and record sample.
+swl_status swl2d_session_write_receivers(const swl2d_session *s, const char *path) {
+    return guard([&] {
+        needSession(s);
+        const auto &p = s->params;
+        const auto &m = s->model;
+        auto out = csvFile(path, "Choose a receiver CSV file name.", "Cannot create 2D receiver CSV.");
+        const char *precision = p.precision == SWL_FP32 ? "FP32" : "FP64";
+        const auto dir = unitDirection(p.sourceKind, p.sourceDirection);
+        const auto &q = p.attenuation;
+        out << "# P-SV plane strain; x,z in m; velocity in m/s; t=0 included\n# dt=" << m.recordDt << "\n# solver_dt=" << m.dt
+            << "\n# backend=" << kBackend;
+        out << "\n# calculation_precision=" << precision << "; model_precision=" << precision
+            << "; record_storage=Float64; values_sampled_from=" << precision;
+        out << "\n# external_absorption=" << p.externalAbsorption << "; computational_NXZ=" << m.nx - 6 << ',' << m.nz - 6;
+        out << "\n# absorption_enabled=" << p.absorbing << "; absorber=" << (p.absorber == 1 ? "CFS-PML_ADE" : "sponge")
+            << "; effective_width_XZ=" << std::min(p.spongeX, p.nx / 3) << ',' << std::min(p.spongeZ, p.nz / 3)
+            << "; PML_target_R=" << p.cpmlReflection << "; kappa=" << p.cpmlKappaMax
+            << "; PML_Hz=" << (p.cpmlFrequency > 0 ? p.cpmlFrequency : p.frequency);
+        out << "\n# GSLS=" << q.enabled << "; mechanisms=" << q.mechanisms << "; reference_Hz=" << q.referenceFrequency
+            << "; fit_band_Hz=" << q.minFrequency << ':' << q.maxFrequency;
+        if (p.layered) {
+            for (std::size_t i = 0; i < p.layers.size(); ++i) out << "\n# layer_" << i << "_Qp_Qs=" << p.layers[i].qp << ',' << p.layers[i].qs;
+        } else {
+            out << "; Qp=" << q.qp << "; Qs=" << q.qs;
+        }
+        out << "\n# source_kind=" << p.sourceKind << " (0=directional_force,1=isotropic_moment); force_per_length_N_per_m="
+            << p.forcePerLength << "; diagonal_moment_per_length_N=" << p.momentPerLength << "; direction_XZ=" << dir[0] << ','
+            << dir[2] << "; Ricker_f0_Hz=" << p.frequency << "\nreceiver,x_m,z_m,time_s,vx_m_s,vz_m_s\n";
+        for (std::size_t r = 0; r < s->vx.size(); ++r)
+            for (std::size_t t = 0; t < s->vx[r].size(); ++t)
+                out << r << ',' << m.receiverPositions[r][0] << ',' << m.receiverPositions[r][1] << ',' << t * m.recordDt << ','
+                    << s->vx[r][t] << ',' << s->vz[r][t] << '\n';
+        if (!out) throw swl::host::Failure(SWL_ERR_INVALID, "2D receiver write failed.");
+    });
+}
+// writeReceiversCsv (src/three_d/ReceiverIo.cpp): header comments, then one row per time sample with
+// the selected components of every receiver.
+swl_status swl3d_session_write_receivers(const swl3d_session *s, const char *path, const int32_t selected[3]) {
+    return guard([&] {
+        needSession(s);
+        if (!selected || !(selected[0] || selected[1] || selected[2]))
+            throw swl::host::Failure(SWL_ERR_INVALID, "Select at least one receiver component.");
+        const auto &p = s->params;
+        const auto &m = s->model;
+        auto out = csvFile(path, "Could not open receiver CSV.", "Could not open receiver CSV.");
+        static const char *const names[3] = {"Vx", "Vy", "Vz"};
+        out << "# ";
+        bool comma = false;
+        for (int c = 0; c < 3; ++c)
+            if (selected[c]) out << (comma ? "," : "") << names[c], comma = true;
+        out << " in m/s; time in seconds; coordinates in metres; depth positive down\n";
+        const auto dir = unitDirection(p.sourceKind, p.sourceDirection);
+        out << "# source_kind=" << p.sourceKind << " (0=directional_force,1=isotropic_moment); force_N=" << p.sourceForce
+            << "; diagonal_moment_Nm=" << p.sourceMoment << "; direction=" << dir[0] << ',' << dir[1] << ',' << dir[2]
+            << "; Ricker_f0_Hz=" << p.frequency << '\n';
+        const int si = p.sourceX < 0 ? p.nx / 2 : p.sourceX, sj = p.sourceY < 0 ? p.ny / 2 : p.sourceY, sk = p.sourceZ;
+        const std::size_t node = std::size_t(si + 3) + std::size_t(m.nx) * (std::size_t(sj + 3) + std::size_t(m.ny) * std::size_t(sk + 3));
+        out << "# source XYZ (m): " << m.coordinates[3 * node] << ',' << m.coordinates[3 * node + 1] << ',' << m.coordinates[3 * node + 2]
+            << "; grid IJK (zero-based): " << si << ',' << sj << ',' << sk << '\n';
+        const std::size_t R = m.receiverPositions.size();
+        for (std::size_t r = 0; r < R; ++r)
+            out << "# receiver " << r + 1 << ": " << m.receiverPositions[r][0] << ',' << m.receiverPositions[r][1] << ','
+                << m.receiverPositions[r][2] << '\n';
+        out << "time_s";
+        for (std::size_t r = 0; r < R; ++r)
+            for (int c = 0; c < 3; ++c)
+                if (selected[c]) out << ",receiver_" << r + 1 << '_' << names[c];
+        out << '\n';
+        for (int t = 0; t <= s->step; ++t) {
+            out << t * m.dt;
+            for (std::size_t r = 0; r < R; ++r)
+                for (int c = 0; c < 3; ++c)
+                    if (selected[c]) out << ',' << s->rec[c][r].at(std::size_t(t));
+            out << '\n';
+        }
+        if (!out.good()) throw swl::host::Failure(SWL_ERR_INVALID, "Receiver CSV write failed.");
+    });
+}
 
 } // extern "C"

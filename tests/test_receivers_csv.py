@@ -1,0 +1,125 @@
+"""Receiver CSV files of the sessions against the reference's own writers.
+
+tests/golden/receivers_csv.json (made by tests/golden/make_csv.py) holds the files that
+writeReceivers (src/two_d/CurvilinearSolver2D.cpp:811-855) and writeReceiversCsv
+(src/three_d/ReceiverIo.cpp) wrote for the cases of tests/cases.py.  After zero steps (a model-only
+session, no GPU) the files must be identical but for the backend line, which names the device;
+after the cases' steps (GPU) the header is identical and the samples equal the reference's records.
+"""
+import importlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cases import CASES_2D, CASES_3D
+from conftest import rel_l2
+from helpers import load_2d, load_3d, records_2d, records_3d
+
+GOLDEN = json.loads((Path(__file__).resolve().parent / "golden" / "receivers_csv.json").read_text())
+MODEL_ONLY = -2
+
+
+@pytest.fixture(scope="module")
+def S(swl):
+    return importlib.import_module("swl_b200.session")
+
+
+@pytest.fixture(scope="module")
+def R(swl):
+    return importlib.import_module("swl_b200.records")
+
+
+def same_but_backend(got: str, want: str):
+    g, w = got.splitlines(), want.splitlines()
+    assert len(g) == len(w)
+    for a, b in zip(g, w):
+        if b.startswith("# backend="):
+            assert a.startswith("# backend=")
+        else:
+            assert a == b
+
+
+@pytest.mark.parametrize("name", list(CASES_2D))
+def test_2d_csv_after_zero_steps_matches_reference(name, S, R, tmp_path):
+    sim = S.Simulation2D(CASES_2D[name], device=MODEL_ONLY)
+    R.session_write_receivers(sim, tmp_path / "r.csv")
+    same_but_backend((tmp_path / "r.csv").read_text(), GOLDEN[f"2/{name}/receivers/0"])
+
+
+@pytest.mark.parametrize("name", list(CASES_3D))
+@pytest.mark.parametrize("which,selected", [("receivers", (1, 1, 1)), ("receivers_xz", (1, 0, 1))])
+def test_3d_csv_after_zero_steps_matches_reference(name, which, selected, S, R, tmp_path):
+    sim = S.Simulation3D(CASES_3D[name], device=MODEL_ONLY)
+    R.session_write_receivers(sim, tmp_path / "r.csv", selected)
+    assert (tmp_path / "r.csv").read_text() == GOLDEN[f"3/{name}/{which}/0"]
+
+
+def test_3d_csv_needs_a_component(S, R, swl, tmp_path):
+    sim = S.Simulation3D(CASES_3D["force"], device=MODEL_ONLY)
+    with pytest.raises(swl.SwlError, match="Select at least one receiver component."):
+        R.session_write_receivers(sim, tmp_path / "r.csv", (0, 0, 0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES_2D))
+def test_2d_csv_after_steps_matches_reference(name, S, R, tmp_path):
+    case, res, _ = load_2d(name)
+    want = GOLDEN[f"2/{name}/receivers/n"]
+    sim = S.Simulation2D(case, device=0)
+    sim.advance(want["steps"])
+    R.session_write_receivers(sim, tmp_path / "r.csv")
+    lines = (tmp_path / "r.csv").read_text().splitlines()
+    head = len(want["header"])
+    same_but_backend("\n".join(lines[:head]), "\n".join(want["header"]))
+    rows = [line.split(",") for line in lines[head:]]
+    rvx, rvz = records_2d(res)
+    n = rvx.shape[1]
+    assert len(rows) == rvx.shape[0] * n
+    vx = np.array([float(r[4]) for r in rows]).reshape(rvx.shape)
+    vz = np.array([float(r[5]) for r in rows]).reshape(rvz.shape)
+    assert [int(r[0]) for r in rows[::n]] == list(range(rvx.shape[0]))
+    assert rel_l2(vx, rvx) <= 1e-11 and rel_l2(vz, rvz) <= 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES_3D))
+def test_3d_csv_after_steps_matches_reference(name, S, R, tmp_path):
+    case, res, _ = load_3d(name)
+    want = GOLDEN[f"3/{name}/receivers/n"]
+    sim = S.Simulation3D(case, device=0)
+    sim.advance(want["steps"])
+    R.session_write_receivers(sim, tmp_path / "r.csv", (1, 1, 1))
+    lines = (tmp_path / "r.csv").read_text().splitlines()
+    head = len(want["header"])
+    assert lines[:head] == want["header"]
+    values = np.array([[float(v) for v in line.split(",")] for line in lines[head:]])
+    rx, ry, rz = records_3d(res)
+    assert values.shape == (rx.shape[1], 1 + 3 * rx.shape[0])
+    for c, rec in enumerate((rx, ry, rz)):
+        np.testing.assert_array_equal(values[:, 1 + c::3].T, rec)
+
+
+SEGY = np.load(Path(__file__).resolve().parent / "golden" / "session_segy.npz")
+# (component, profile) of each file: Vz as IEEE32; Vx (2D, component 1) / Vy (3D, component 2) as IEEE64
+SEGY_FILES = {2: [("vz_ieee32", 0, 0), ("vx_ieee64", 1, 1)], 3: [("vz_ieee32", 0, 0), ("vy_ieee64", 2, 1)]}
+
+
+@pytest.mark.parametrize("dim,name", [(2, n) for n in CASES_2D] + [(3, n) for n in CASES_3D])
+def test_session_segy_after_zero_steps_matches_reference(dim, name, S, R, tmp_path):
+    sim = (S.Simulation2D if dim == 2 else S.Simulation3D)((CASES_2D if dim == 2 else CASES_3D)[name], device=MODEL_ONLY)
+    for f, comp, profile in SEGY_FILES[dim]:
+        R.session_write_segy(sim, comp, tmp_path / f"{f}.sgy", profile=profile)
+        assert (tmp_path / f"{f}.sgy").read_bytes() == bytes(SEGY[f"{dim}/{name}/{f}/0"]), f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,name", [(2, n) for n in CASES_2D] + [(3, n) for n in CASES_3D])
+def test_session_segy_after_steps_matches_reference(dim, name, S, R, tmp_path):
+    # the FP64 session records equal the reference's, so the exported files are identical
+    sim = (S.Simulation2D if dim == 2 else S.Simulation3D)((CASES_2D if dim == 2 else CASES_3D)[name], device=0)
+    sim.advance(GOLDEN[f"{dim}/{name}/receivers/n"]["steps"])
+    for f, comp, profile in SEGY_FILES[dim]:
+        R.session_write_segy(sim, comp, tmp_path / f"{f}.sgy", profile=profile)
+        assert (tmp_path / f"{f}.sgy").read_bytes() == bytes(SEGY[f"{dim}/{name}/{f}/n"]), f
