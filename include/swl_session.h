@@ -74,6 +74,13 @@ swl_status swl2d_session_snapshot(swl2d_session *s, int32_t field, double *out);
  * "deltaP0".."deltaS2"); *n receives the length (out may be null to query it). */
 swl_status swl2d_session_model(const swl2d_session *s, const char *name, double *out, int64_t *n);
 swl2d_engine *swl2d_session_engine(swl2d_session *s);
+/* writeSnapshot (src/two_d/CurvilinearSolver2D.cpp:725-810): the current wavefield as a VTK
+ * structured grid (.vts, ASCII) of the logical model, byte for byte the reference's file.
+ * components: Vx, Vz, velocity magnitude, pressure, Sxx, Szz, Sxz (SnapshotExportOptions); the
+ * reference's default is {1, 1, 0, 0, 1, 1, 1} with the material. */
+swl_status swl2d_session_write_snapshot(swl2d_session *s, const char *path, const int32_t components[7], int32_t include_material);
+/* Simulation::readProbes (:710-724): Vx, Vz, Sxx, Szz, Sxz at logical nodes (i, k), 5 per node. */
+swl_status swl2d_session_read_probes(swl2d_session *s, const int32_t *nodes_ik, int32_t n, double *out5);
 
 typedef struct swl_layer3d {
     double thickness, vp, vs, density;
@@ -123,6 +130,12 @@ swl_status swl3d_session_snapshot(swl3d_session *s, int32_t field, double *out);
  * "materialLambda", "materialMu", "materialDensity". */
 swl_status swl3d_session_model(const swl3d_session *s, const char *name, double *out, int64_t *n);
 swl3d_engine *swl3d_session_engine(swl3d_session *s);
+/* writeVts (src/three_d/VtsWriter.cpp) of the current state: the physical nodes as a VTK
+ * structured grid (.vts, ASCII), byte for byte the reference's file.  fields: Vx, Vy, Vz, |V|,
+ * mean normal stress, Sxx, Syy, Szz, Sxy, Sxz, Syz (VtsExportOptions3D; default all, with the
+ * material and the velocity vector). */
+swl_status swl3d_session_write_snapshot(swl3d_session *s, const char *path, const int32_t fields[11], int32_t include_material,
+                                        int32_t include_velocity_vector);
 
 #ifdef __cplusplus
 }

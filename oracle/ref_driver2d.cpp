@@ -230,6 +230,24 @@ int main(int argc, char **argv) {
             std::string csvError;
             if (!writeReceivers(sim, out / "receivers.csv", csvError)) std::ofstream(out / "csv_error.txt") << csvError << '\n';
         }
+        { // writeSnapshot (CurvilinearSolver2D.cpp:725-810) with the default options and with every component
+            std::string vtsError;
+            SnapshotExportOptions all;
+            all.components = {true, true, true, true, true, true, true};
+            if (!writeSnapshot(sim, out / "snapshot.vts", vtsError, SnapshotExportOptions{}) ||
+                !writeSnapshot(sim, out / "snapshot_all.vts", vtsError, all))
+                std::ofstream(out / "vts_error.txt") << vtsError << '\n';
+            // readProbes at a few logical nodes
+            const auto &pp = sim.parameters();
+            std::vector<std::array<int, 2>> nodes{{0, 0}, {pp.nx / 2, pp.nz / 3}, {pp.nx - 1, pp.nz - 1}, {pp.nx / 3, 0}};
+            std::vector<std::array<double, 5>> probes;
+            std::string probeError;
+            if (sim.readProbes(nodes, probes, probeError)) {
+                std::vector<double> flat;
+                for (const auto &v : probes) flat.insert(flat.end(), v.begin(), v.end());
+                write(out, "probes.bin", flat);
+            }
+        }
         { // the workbench's record view (src/two_d/ui/Workbench2D.cpp:251-268) through writeSegy
             SeisWave::RecordDataView data;
             data.dt = sim.recordDt();

@@ -32,6 +32,7 @@
 #define private public
 #include "CurvilinearSolver.cpp"
 #include "Seis3D/ReceiverIo.hpp"
+#include "Seis3D/VtsWriter.hpp"
 #undef private
 
 using namespace Seis3D::Curvilinear;
@@ -202,6 +203,17 @@ int main(int argc, char **argv) {
             if (!writeReceiversCsv(sim, out / "receivers.csv", {true, true, true}, csvError) ||
                 !writeReceiversCsv(sim, out / "receivers_xz.csv", {true, false, true}, csvError))
                 std::ofstream(out / "csv_error.txt") << csvError << '\n';
+        }
+        { // writeVts (src/three_d/VtsWriter.cpp) of the snapshot, default options and a reduced set
+            std::string vtsError;
+            VtsExportOptions3D some;
+            some.fields = {false, false, true, false, true, false, false, false, true, false, false};
+            some.includeMaterial = false;
+            some.includeVelocityVector = false;
+            const auto snap = sim.snapshot();
+            if (!writeVts(snap, out / "snapshot.vts", VtsExportOptions3D{}, vtsError) ||
+                !writeVts(snap, out / "snapshot_some.vts", some, vtsError))
+                std::ofstream(out / "vts_error.txt") << vtsError << '\n';
         }
         { // the record view of src/three_d/ui/RecordView3D.cpp:5-6 through writeSegy
             SeisWave::RecordDataView data;

@@ -354,4 +354,260 @@ swl_status swl3d_session_write_receivers(const swl3d_session *s, const char *pat
     });
 }
 
+
+// -------------------------------------------------------------------- snapshots and probes
+// writeSnapshot (src/two_d/CurvilinearSolver2D.cpp:725-810): a VTK structured grid of the logical
+// model with the run's metadata as field data, the selected wavefield components (and material)
+// as point data in the session precision, and the node coordinates.
+swl_status swl2d_session_write_snapshot(swl2d_session *s, const char *path, const int32_t components[7], int32_t include_material) {
+    return guard([&] {
+        needSession(s);
+        if (!components || std::none_of(components, components + 7, [](int32_t v) { return v != 0; }))
+            throw swl::host::Failure(SWL_ERR_INVALID, "Select at least one wavefield export component.");
+        if (!path) throw swl::host::Failure(SWL_ERR_INVALID, "path is null");
+        const auto &p = s->params;
+        const auto &m = s->model;
+        const std::size_t count = std::size_t(m.nx) * m.nz;
+        // the current state (zero before the first step, and without an engine)
+        std::vector<double> fields[6];
+        const int nf = m.mechanisms ? 6 : 5;
+        for (int f = 0; f < nf; ++f) {
+            fields[f].assign(count, 0.0);
+            if (s->engine) swl::host::ok(swl2d_snapshot(s->engine, f, fields[f].data()));
+        }
+        std::ofstream out(path);
+        if (!out) throw swl::host::Failure(SWL_ERR_INVALID, "Cannot create 2D VTS file.");
+        out.imbue(std::locale::classic());
+        const bool fp32 = p.precision == SWL_FP32;
+        const char *pointType = fp32 ? "Float32" : "Float64";
+        out << std::setprecision(17) << "<?xml version=\"1.0\"?>\n<VTKFile type=\"StructuredGrid\" version=\"0.1\" "
+               "byte_order=\"LittleEndian\"><StructuredGrid WholeExtent=\"0 " << p.nx - 1 << " 0 0 0 " << p.nz - 1 << "\">\n";
+        const auto dir = unitDirection(p.sourceKind, p.sourceDirection);
+        out << "<FieldData>";
+        const auto scalar = [&](const char *name, double value) {
+            out << "<DataArray type=\"Float64\" Name=\"" << name << "\" NumberOfTuples=\"1\" format=\"ascii\">" << value << "</DataArray>";
+        };
+        const auto &q = p.attenuation;
+        scalar("CalculationPrecisionBits", fp32 ? 32 : 64);
+        scalar("ExternalAbsorption", p.externalAbsorption);
+        scalar("ComputationalNodesX", m.nx - 6);
+        scalar("ComputationalNodesZ", m.nz - 6);
+        scalar("LogicalModelOffsetXCells", m.modelOffsetX);
+        scalar("AbsorptionEnabled", p.absorbing);
+        scalar("AbsorberKind", p.absorber);
+        scalar("AbsorberWidthXCells", std::min(p.spongeX, p.nx / 3));
+        scalar("AbsorberWidthZCells", std::min(p.spongeZ, p.nz / 3));
+        scalar("CfsPmlTargetReflection", p.cpmlReflection);
+        scalar("CfsPmlKappaMax", p.cpmlKappaMax);
+        scalar("CfsPmlFrequencyHz", p.cpmlFrequency > 0 ? p.cpmlFrequency : p.frequency);
+        scalar("SourceKind", p.sourceKind);
+        scalar("SourceForcePerLengthNPerM", p.forcePerLength);
+        scalar("SourceMomentPerLengthN", p.momentPerLength);
+        scalar("SourceFrequencyHz", p.frequency);
+        scalar("SourceDirectionX", dir[0]);
+        scalar("SourceDirectionZ", dir[2]);
+        scalar("SimulationDt", m.dt);
+        scalar("RecordIntervalSeconds", m.recordDt);
+        scalar("SimulationStep", s->step);
+        scalar("TIME_VALUE", s->step * m.dt);
+        scalar("AttenuationGSLS", q.enabled);
+        scalar("QReferenceFrequencyHz", q.referenceFrequency);
+        scalar("QBandMinHz", q.minFrequency);
+        scalar("QBandMaxHz", q.maxFrequency);
+        scalar("RelaxationMechanisms", q.enabled ? q.mechanisms : 0);
+        static const char *const names[10] = {"Vx", "Vz", "VelocityMagnitude", "Pressure", "Sxx", "Szz", "Sxz", "Vp", "Vs", "Density"};
+        const int first = int(std::find_if(components, components + 7, [](int32_t v) { return v != 0; }) - components);
+        out << "</FieldData><Piece Extent=\"0 " << p.nx - 1 << " 0 0 0 " << p.nz - 1 << "\"><PointData Scalars=\"" << names[first] << "\">\n";
+        const auto node = [&](int i, int k) { return std::size_t(i + 3 + m.modelOffsetX) + std::size_t(m.nx) * std::size_t(k + 3); };
+        for (int f = 0; f < 10; ++f) {
+            if (f < 7 ? !components[f] : !include_material) continue;
+            out << "<DataArray type=\"" << pointType << "\" Name=\"" << names[f] << "\" format=\"ascii\">\n";
+            for (int k = 0; k < p.nz; ++k)
+                for (int i = 0; i < p.nx; ++i) {
+                    const std::size_t n = node(i, k);
+                    double v;
+                    if (f < 2) v = fields[f][n];
+                    else if (f == 2) v = std::sqrt(fields[0][n] * fields[0][n] + fields[1][n] * fields[1][n]);
+                    else if (f == 3) { // pressure -tr(S)/3; plane strain Syy = lambda (Sxx + Szz) / (2 (lambda + mu)) without GSLS
+                        const double mu = m.density[n] * m.vs[n] * m.vs[n];
+                        const double lambda = m.density[n] * m.vp[n] * m.vp[n] - 2 * mu;
+                        v = q.enabled ? -(fields[2][n] + fields[3][n] + fields[5][n]) / 3
+                                      : -(1 + lambda / (2 * (lambda + mu))) * (fields[2][n] + fields[3][n]) / 3;
+                    } else if (f < 7) v = fields[f - 2][n];
+                    else v = f == 7 ? m.vp[n] : f == 8 ? m.vs[n] : m.density[n];
+                    out << (fp32 ? double(static_cast<float>(v)) : v) << ' ';
+                }
+            out << "\n</DataArray>\n";
+        }
+        if (q.enabled) {
+            const auto array = [&](const char *name, const std::vector<double> &values) {
+                out << "<DataArray type=\"" << pointType << "\" Name=\"" << name << "\" format=\"ascii\">\n";
+                for (int k = 0; k < p.nz; ++k)
+                    for (int i = 0; i < p.nx; ++i) out << values[node(i, k)] << ' ';
+                out << "\n</DataArray>\n";
+            };
+            if (include_material) array("Qp", m.qp), array("Qs", m.qs);
+            if (components[3] || components[4] || components[5]) array("Syy", fields[5]);
+        }
+        out << "</PointData><Points><DataArray type=\"" << pointType << "\" NumberOfComponents=\"3\" format=\"ascii\">\n";
+        for (int k = 0; k < p.nz; ++k)
+            for (int i = 0; i < p.nx; ++i) {
+                const std::size_t n = node(i, k);
+                out << m.coordinates[2 * n] << " 0 " << m.coordinates[2 * n + 1] << ' ';
+            }
+        out << "</DataArray></Points></Piece></StructuredGrid></VTKFile>\n";
+        if (!out) throw swl::host::Failure(SWL_ERR_INVALID, "2D VTS write failed.");
+    });
+}
+// Simulation::readProbes (src/two_d/CurvilinearSolver2D.cpp:710-724): Vx, Vz, Sxx, Szz, Sxz at
+// logical model nodes (i, k), 5 values per node, read on the device.
+swl_status swl2d_session_read_probes(swl2d_session *s, const int32_t *nodes_ik, int32_t n, double *out5) {
+    return guard([&] {
+        if (!s) throw swl::host::Failure(SWL_ERR_INVALID, "Initialize before probe readback.");
+        if (n > 1000000) throw swl::host::Failure(SWL_ERR_INVALID, "Too many probe nodes.");
+        if (n < 0 || (n && (!nodes_ik || !out5))) throw swl::host::Failure(SWL_ERR_INVALID, "nodes and out are required");
+        if (!s->engine) throw swl::host::Failure(SWL_ERR_STATE, "no engine (model-only session)");
+        const auto &m = s->model;
+        std::vector<int64_t> idx(static_cast<std::size_t>(n));
+        for (int32_t r = 0; r < n; ++r) {
+            const int i = nodes_ik[2 * r], k = nodes_ik[2 * r + 1];
+            if (i < 0 || i >= m.logicalNx || k < 0 || k >= m.logicalNz) throw swl::host::Failure(SWL_ERR_INVALID, "Probe outside logical model.");
+            idx[std::size_t(r)] = int64_t(i + 3 + m.modelOffsetX) + int64_t(m.nx) * int64_t(k + 3);
+        }
+        if (n) swl::host::ok(swl2d_probes(s->engine, idx.data(), n, out5));
+    });
+}
+
+
+// writeVts (src/three_d/VtsWriter.cpp) of the session's current state (CpuSimulation3D::snapshot,
+// src/three_d/CurvilinearSolver.cpp:648-687): the physical nodes as a VTK structured grid with the
+// run's metadata, the selected fields, the material (and layer ids) and the velocity vector.
+// fields: Vx, Vy, Vz, |V|, mean normal stress, Sxx, Syy, Szz, Sxy, Sxz, Syz.
+swl_status swl3d_session_write_snapshot(swl3d_session *s, const char *path, const int32_t fields[11], int32_t include_material,
+                                        int32_t include_velocity_vector) {
+    return guard([&] {
+        needSession(s);
+        if (!path || !fields) throw swl::host::Failure(SWL_ERR_INVALID, "path and fields are required");
+        if (!include_velocity_vector && std::none_of(fields, fields + 11, [](int32_t v) { return v != 0; }))
+            throw swl::host::Failure(SWL_ERR_INVALID, "Select at least one wavefield component.");
+        const auto &p = s->params;
+        const auto &m = s->model;
+        const int nx = m.nx - 6, ny = m.ny - 6, nz = m.nz - 6;
+        const std::size_t count = std::size_t(m.nx) * m.ny * m.nz, plane = std::size_t(m.nx) * m.ny;
+        std::vector<double> f[9];
+        for (int c = 0; c < 9; ++c) {
+            f[c].assign(count, 0.0);
+            if (s->engine) swl::host::ok(swl3d_snapshot(s->engine, c, f[c].data()));
+        }
+        bool finite = true;
+        if (s->engine) {
+            swl_diag3d d{};
+            swl::host::ok(swl3d_diagnostics(s->engine, &d));
+            finite = d.finite != 0;
+        }
+        if (!finite) throw swl::host::Failure(SWL_ERR_INVALID, "Refusing to export non-finite simulation fields.");
+        const bool layered = !m.materialLambda.empty();
+        std::vector<double> vp, vs;
+        std::vector<int> layer;
+        if (layered) {
+            vp.resize(count), vs.resize(count), layer.resize(count);
+            for (std::size_t q = 0; q < count; ++q) {
+                vp[q] = std::sqrt((m.materialLambda[q] + 2 * m.materialMu[q]) / m.materialDensity[q]);
+                vs[q] = std::sqrt(m.materialMu[q] / m.materialDensity[q]);
+                // materialDepth3D / materialLayerAtDepth3D (include/Seis3D/MaterialModels3D.hpp:19-31)
+                double depth;
+                if (p.layerDepthMode == 0) depth = (static_cast<int>(q / plane) - 3) * m.h;
+                else if (p.layerDepthMode == 2) depth = m.coordinates[3 * q + 2];
+                else depth = m.coordinates[3 * q + 2] - m.coordinates[3 * (3 * plane + q % plane) + 2];
+                double bottom = 0;
+                int id = static_cast<int>(p.layers.size()) - 1;
+                for (std::size_t i = 0; i + 1 < p.layers.size(); ++i) {
+                    bottom += p.layers[i].thickness;
+                    if (depth < bottom) {
+                        id = static_cast<int>(i);
+                        break;
+                    }
+                }
+                layer[q] = id;
+            }
+        }
+        const int si = p.sourceX < 0 ? p.nx / 2 : p.sourceX, sj = p.sourceY < 0 ? p.ny / 2 : p.sourceY, sk = p.sourceZ;
+        const std::size_t sq = std::size_t(si + 3) + std::size_t(m.nx) * (std::size_t(sj + 3) + std::size_t(m.ny) * std::size_t(sk + 3));
+        const double *source = &m.coordinates[3 * sq];
+        const auto dir = unitDirection(p.sourceKind, p.sourceDirection);
+        const std::filesystem::path file(path);
+        if (!file.parent_path().empty()) std::filesystem::create_directories(file.parent_path());
+        std::ofstream out(file, std::ios::binary);
+        if (!out) throw swl::host::Failure(SWL_ERR_INVALID, std::string("Could not open VTS output file: ") + file.string());
+        out.imbue(std::locale::classic());
+        out << std::setprecision(17);
+        const auto meta = [&](const char *type, const char *name, auto value) {
+            out << "<DataArray type=\"" << type << "\" Name=\"" << name << "\" NumberOfTuples=\"1\" format=\"ascii\">" << value << "</DataArray>";
+        };
+        out << "<?xml version=\"1.0\"?>\n<VTKFile type=\"StructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\">\n"
+            << "  <StructuredGrid WholeExtent=\"0 " << nx - 1 << " 0 " << ny - 1 << " 0 " << nz - 1 << "\">\n    <FieldData>";
+        meta("Float64", "TIME_VALUE", s->step * m.dt);
+        meta("Float64", "SimulationDt", m.dt);
+        meta("Int32", "SimulationStep", s->step);
+        meta("Float64", "SourceX", source[0]);
+        meta("Float64", "SourceY", source[1]);
+        meta("Float64", "SourceZ", source[2]);
+        meta("Int32", "SourceKind", p.sourceKind);
+        meta("Float64", "SourceForceN", p.sourceForce);
+        meta("Float64", "SourceMomentNm", p.sourceMoment);
+        meta("Float64", "SourceFrequencyHz", p.frequency);
+        meta("Float64", "SourceDirectionX", dir[0]);
+        meta("Float64", "SourceDirectionY", dir[1]);
+        meta("Float64", "SourceDirectionZ", dir[2]);
+        meta("Float64", "GridSpacing", m.h);
+        meta("Float64", "TerrainTransitionDepth", m.flattenDepth);
+        out << "</FieldData>\n    <Piece Extent=\"0 " << nx - 1 << " 0 " << ny - 1 << " 0 " << nz - 1 << "\">\n      <PointData";
+        static const char *const names[11] = {"Vx", "Vy", "Vz", "VelocityMagnitude", "MeanNormalStress", "Sxx", "Syy", "Szz", "Sxy", "Sxz", "Syz"};
+        for (int c = 0; c < 11; ++c)
+            if (fields[c]) {
+                out << " Scalars=\"" << names[c] << "\"";
+                break;
+            }
+        if (include_velocity_vector) out << " Vectors=\"Velocity\"";
+        out << ">\n";
+        // physical nodes, x fastest; `perLine` values and then a line break
+        const auto each = [&](int perLine, auto &&write) {
+            std::size_t written = 0;
+            for (int k = 3; k < m.nz - 3; ++k)
+                for (int j = 3; j < m.ny - 3; ++j)
+                    for (int i = 3; i < m.nx - 3; ++i) {
+                        write(std::size_t(i) + std::size_t(m.nx) * (std::size_t(j) + std::size_t(m.ny) * std::size_t(k)));
+                        if (++written % perLine == 0) out << "\n          ";
+                    }
+        };
+        const auto scalar = [&](const char *name, auto valueAt) {
+            out << "        <DataArray type=\"Float64\" Name=\"" << name << "\" format=\"ascii\">\n          ";
+            each(6, [&](std::size_t q) { out << valueAt(q) << ' '; });
+            out << "\n        </DataArray>\n";
+        };
+        for (int c = 0; c < 3; ++c)
+            if (fields[c]) scalar(names[c], [&](std::size_t q) { return f[c][q]; });
+        if (include_material) {
+            scalar("Vp", [&](std::size_t q) { return layered ? vp[q] : p.vp; });
+            scalar("Vs", [&](std::size_t q) { return layered ? vs[q] : p.vs; });
+            scalar("Density", [&](std::size_t q) { return layered ? m.materialDensity[q] : p.density; });
+            if (layered) scalar("LayerId", [&](std::size_t q) { return layer[q]; });
+        }
+        if (fields[3]) scalar(names[3], [&](std::size_t q) { return std::hypot(f[0][q], f[1][q], f[2][q]); });
+        if (fields[4]) scalar(names[4], [&](std::size_t q) { return -(f[3][q] + f[4][q] + f[5][q]) / 3.; });
+        for (int c = 0; c < 6; ++c)
+            if (fields[5 + c]) scalar(names[5 + c], [&](std::size_t q) { return f[3 + c][q]; });
+        if (include_velocity_vector) {
+            out << "        <DataArray type=\"Float64\" Name=\"Velocity\" NumberOfComponents=\"3\" format=\"ascii\">\n          ";
+            each(2, [&](std::size_t q) { out << f[0][q] << ' ' << f[1][q] << ' ' << f[2][q] << ' '; });
+            out << "\n        </DataArray>\n";
+        }
+        out << "      </PointData>\n      <CellData/>\n      <Points>\n"
+            << "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n          ";
+        each(2, [&](std::size_t q) { out << m.coordinates[3 * q] << ' ' << m.coordinates[3 * q + 1] << ' ' << m.coordinates[3 * q + 2] << ' '; });
+        out << "\n        </DataArray>\n      </Points>\n    </Piece>\n  </StructuredGrid>\n</VTKFile>\n";
+        if (!out.good()) throw swl::host::Failure(SWL_ERR_INVALID, std::string("Failed while writing VTS output: ") + file.string());
+    });
+}
+
 } // extern "C"

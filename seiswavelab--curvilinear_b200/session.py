@@ -108,6 +108,8 @@ def _bind():
     L.swl2d_session_model.argtypes = [vp, C.c_char_p, _dp, C.POINTER(C.c_int64)]
     L.swl2d_session_engine.argtypes = [vp]
     L.swl2d_session_engine.restype = vp
+    L.swl2d_session_write_snapshot.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int32), C.c_int32]
+    L.swl2d_session_read_probes.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32, _dp]
     L.swl3d_params_default.argtypes = [C.POINTER(Params3D)]
     L.swl3d_session_create.argtypes = [C.POINTER(Params3D), C.c_int32, C.POINTER(vp)]
     L.swl3d_session_destroy.argtypes = [vp]
@@ -119,6 +121,7 @@ def _bind():
     L.swl3d_session_model.argtypes = [vp, C.c_char_p, _dp, C.POINTER(C.c_int64)]
     L.swl3d_session_engine.argtypes = [vp]
     L.swl3d_session_engine.restype = vp
+    L.swl3d_session_write_snapshot.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int32), C.c_int32, C.c_int32]
     _bound = True
     return L
 
@@ -272,6 +275,19 @@ class Simulation2D:
     def engine_handle(self) -> int:
         return library().swl2d_session_engine(self._h)
 
+    def write_snapshot(self, path, components=(1, 1, 0, 0, 1, 1, 1), include_material=True):
+        """writeSnapshot: the wavefield as a .vts file (Vx, Vz, |V|, pressure, Sxx, Szz, Sxz)."""
+        comp = (C.c_int32 * 7)(*[int(bool(c)) for c in components])
+        _check(library().swl2d_session_write_snapshot(self._h, str(path).encode(), comp, int(bool(include_material))))
+
+    def read_probes(self, nodes) -> np.ndarray:
+        """Simulation::readProbes: Vx, Vz, Sxx, Szz, Sxz at logical nodes (i, k)."""
+        ik = np.ascontiguousarray(np.asarray(nodes, dtype=np.int32).reshape(-1, 2))
+        out = np.zeros((ik.shape[0], 5))
+        _check(library().swl2d_session_read_probes(self._h, ik.ctypes.data_as(C.POINTER(C.c_int32)), ik.shape[0],
+                                                   out.ctypes.data_as(_dp)))
+        return out
+
 
 class Simulation3D:
     """Seis3D::Curvilinear::ISimulationBackend3D on the B200 engine."""
@@ -323,3 +339,9 @@ class Simulation3D:
 
     def engine_handle(self) -> int:
         return library().swl3d_session_engine(self._h)
+
+    def write_snapshot(self, path, fields=(1,) * 11, include_material=True, include_velocity_vector=True):
+        """writeVts: Vx, Vy, Vz, |V|, mean normal stress, Sxx, Syy, Szz, Sxy, Sxz, Syz as a .vts file."""
+        sel = (C.c_int32 * 11)(*[int(bool(c)) for c in fields])
+        _check(library().swl3d_session_write_snapshot(self._h, str(path).encode(), sel, int(bool(include_material)),
+                                                      int(bool(include_velocity_vector))))

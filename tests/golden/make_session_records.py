@@ -12,10 +12,18 @@ src/three_d/ui/RecordView3D.cpp:5-6) with writeSegy (src/common/SegyIo.cpp): Vz 
 Vx (2D) / Vy (3D) as IEEE64, after zero and after n steps; their bytes go to
 tests/golden/session_segy.npz as "<dim>/<case>/<file>/<0|n>".
 
+The 2D drivers also call writeSnapshot (src/two_d/CurvilinearSolver2D.cpp:725-810) with the
+default options and with every component, and readProbes (:710-724) at four logical nodes; the
+snapshots are stored as their SHA-256, size and header (through "<PointData"), the probes as values,
+in receivers_csv.json under "2/<case>/snapshot[_all]/<0|n>" and "2/<case>/probes/n".  The 3D
+drivers call writeVts (src/three_d/VtsWriter.cpp) with the default options and with a reduced set
+("3/<case>/snapshot[_some]/<0|n>").
+
 Usage: python tests/golden/make_session_records.py   (needs oracle/_ref/ref2d and ref3d: make -C oracle ref)
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import sys
 
@@ -50,6 +58,14 @@ def main():
             for f in ("vz_ieee32", "vx_ieee64" if dim == 2 else "vy_ieee64"):
                 segy[f"{dim}/{name}/{f}/0"] = np.frombuffer(zero["sgy:" + f], dtype=np.uint8)
                 segy[f"{dim}/{name}/{f}/n"] = np.frombuffer(full["sgy:" + f], dtype=np.uint8)
+            for f in (("snapshot", "snapshot_all") if dim == 2 else ("snapshot", "snapshot_some")):
+                for tag, res in (("0", zero), ("n", full)):
+                    text = res["vts:" + f]
+                    out[f"{dim}/{name}/{f}/{tag}"] = {"sha256": hashlib.sha256(text.encode()).hexdigest(),
+                                                      "size": len(text.encode()),
+                                                      "head": text[:text.index("<PointData")]}
+            if dim == 2:
+                out[f"2/{name}/probes/n"] = [repr(float(v)) for v in full["probes"]]
             print(dim, name, "ok")
     (HERE / "receivers_csv.json").write_text(json.dumps(out, indent=0))
     np.savez_compressed(HERE / "session_segy.npz", **segy)

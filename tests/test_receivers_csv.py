@@ -123,3 +123,71 @@ def test_session_segy_after_steps_matches_reference(dim, name, S, R, tmp_path):
     for f, comp, profile in SEGY_FILES[dim]:
         R.session_write_segy(sim, comp, tmp_path / f"{f}.sgy", profile=profile)
         assert (tmp_path / f"{f}.sgy").read_bytes() == bytes(SEGY[f"{dim}/{name}/{f}/n"]), f
+
+
+def check_snapshot(text: str, want: dict):
+    got = text.encode()
+    head = text[:text.index("<PointData")] if "<PointData" in text else text[:2000]
+    assert head == want["head"]
+    assert len(got) == want["size"]
+    import hashlib
+    assert hashlib.sha256(got).hexdigest() == want["sha256"]
+
+
+ALL = (1, 1, 1, 1, 1, 1, 1)
+
+
+@pytest.mark.parametrize("name", list(CASES_2D))
+def test_2d_snapshot_after_zero_steps_matches_reference(name, S, tmp_path):
+    sim = S.Simulation2D(CASES_2D[name], device=MODEL_ONLY)
+    sim.write_snapshot(tmp_path / "s.vts")
+    check_snapshot((tmp_path / "s.vts").read_text(), GOLDEN[f"2/{name}/snapshot/0"])
+    sim.write_snapshot(tmp_path / "a.vts", ALL)
+    check_snapshot((tmp_path / "a.vts").read_text(), GOLDEN[f"2/{name}/snapshot_all/0"])
+
+
+def test_2d_snapshot_needs_a_component(S, swl, tmp_path):
+    sim = S.Simulation2D(CASES_2D["sponge_force"], device=MODEL_ONLY)
+    with pytest.raises(swl.SwlError, match="Select at least one wavefield export component."):
+        sim.write_snapshot(tmp_path / "s.vts", (0,) * 7)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES_2D))
+def test_2d_snapshot_and_probes_after_steps_match_reference(name, S, swl, tmp_path):
+    case = CASES_2D[name]
+    sim = S.Simulation2D(case, device=0)
+    sim.advance(GOLDEN[f"2/{name}/receivers/n"]["steps"])
+    sim.write_snapshot(tmp_path / "s.vts")
+    check_snapshot((tmp_path / "s.vts").read_text(), GOLDEN[f"2/{name}/snapshot/n"])
+    sim.write_snapshot(tmp_path / "a.vts", ALL)
+    check_snapshot((tmp_path / "a.vts").read_text(), GOLDEN[f"2/{name}/snapshot_all/n"])
+    nx, nz = int(case["nx"]), int(case["nz"])
+    got = sim.read_probes([(0, 0), (nx // 2, nz // 3), (nx - 1, nz - 1), (nx // 3, 0)])
+    want = np.array([float(v) for v in GOLDEN[f"2/{name}/probes/n"]]).reshape(4, 5)
+    np.testing.assert_array_equal(got, want)
+    with pytest.raises(swl.SwlError, match="Probe outside logical model."):
+        sim.read_probes([(nx, 0)])
+
+
+SOME3D = (0, 0, 1, 0, 1, 0, 0, 0, 1, 0, 0)
+
+
+@pytest.mark.parametrize("name", list(CASES_3D))
+def test_3d_snapshot_after_zero_steps_matches_reference(name, S, tmp_path):
+    sim = S.Simulation3D(CASES_3D[name], device=MODEL_ONLY)
+    sim.write_snapshot(tmp_path / "s.vts")
+    check_snapshot((tmp_path / "s.vts").read_text(), GOLDEN[f"3/{name}/snapshot/0"])
+    sim.write_snapshot(tmp_path / "t.vts", SOME3D, include_material=False, include_velocity_vector=False)
+    check_snapshot((tmp_path / "t.vts").read_text(), GOLDEN[f"3/{name}/snapshot_some/0"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES_3D))
+def test_3d_snapshot_after_steps_matches_reference(name, S, tmp_path):
+    sim = S.Simulation3D(CASES_3D[name], device=0)
+    sim.advance(GOLDEN[f"3/{name}/receivers/n"]["steps"])
+    sim.write_snapshot(tmp_path / "s.vts")
+    check_snapshot((tmp_path / "s.vts").read_text(), GOLDEN[f"3/{name}/snapshot/n"])
+    sim.write_snapshot(tmp_path / "t.vts", SOME3D, include_material=False, include_velocity_vector=False)
+    check_snapshot((tmp_path / "t.vts").read_text(), GOLDEN[f"3/{name}/snapshot_some/n"])
