@@ -267,7 +267,7 @@ def _load_dir(d: Path) -> dict:
         res["csv:" + f.stem] = f.read_text()
     for f in d.glob("*.sgy"):  # its SEG-Y exports of the session records, as bytes
         res["sgy:" + f.stem] = f.read_bytes()
-    for f in d.glob("*.vts"):  # its wavefield snapshots, as text
+    for f in d.glob("*.vts"):  # its wavefield snapshots and model files, as text
         res["vts:" + f.stem] = f.read_text()
     return res
 

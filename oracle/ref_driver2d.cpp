@@ -37,6 +37,7 @@
 #define private public
 #include "CurvilinearSolver2D.cpp"
 #undef private
+#include "Seis2D/ModelIo2D.hpp"
 
 using namespace Seis2D::Curvilinear;
 
@@ -229,6 +230,11 @@ int main(int argc, char **argv) {
         { // the reference's receiver CSV (writeReceivers, CurvilinearSolver2D.cpp:811-855)
             std::string csvError;
             if (!writeReceivers(sim, out / "receivers.csv", csvError)) std::ofstream(out / "csv_error.txt") << csvError << '\n';
+        }
+        { // writeModelVts (src/two_d/ModelIo2D.cpp:75-145) with this run's compute settings
+            std::string modelError;
+            if (!writeModelVts(sim, out / "model.vts", ComputeSettings3D{threads, -1}, modelError))
+                std::ofstream(out / "model_error.txt") << modelError << '\n';
         }
         { // writeSnapshot (CurvilinearSolver2D.cpp:725-810) with the default options and with every component
             std::string vtsError;

@@ -42,6 +42,7 @@ UNITS = {
     "host/session.cpp": [],
     "host/server.cpp": [],
     "host/records.cpp": [],
+    "host/modelio.cpp": [],
 }
 
 

@@ -12,8 +12,6 @@
 
 
 using swl::host::guard;
-struct swl2d_session : swl::host::Session2D {};
-struct swl3d_session : swl::host::Session3D {};
 
 namespace {
 void needSession(const void *s) {

@@ -378,3 +378,7 @@ inline Params3D toParams(const swl_params3d &c) {
 }
 
 } // namespace swl::host
+
+// The C-ABI session handles (include/swl_session.h) are the session classes themselves.
+struct swl2d_session : swl::host::Session2D {};
+struct swl3d_session : swl::host::Session3D {};

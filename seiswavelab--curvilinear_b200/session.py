@@ -90,6 +90,10 @@ class Info3D(C.Structure):
 _bound = False
 
 
+class ModelCompute(C.Structure):
+    _fields_ = [("backend", C.c_int32), ("cpu_threads", C.c_int32), ("cuda_device", C.c_int32)]
+
+
 def _bind():
     global _bound
     L = library()
@@ -109,6 +113,10 @@ def _bind():
     L.swl2d_session_engine.argtypes = [vp]
     L.swl2d_session_engine.restype = vp
     L.swl2d_session_write_snapshot.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int32), C.c_int32]
+    L.swl2d_session_write_model.argtypes = [vp, C.c_char_p, C.POINTER(ModelCompute)]
+    L.swl2d_read_model.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.swl2d_model_document_params.argtypes = [vp, C.POINTER(Params2D), C.POINTER(ModelCompute), _dp]
+    L.swl2d_model_document_free.argtypes = [vp]
     L.swl2d_session_read_probes.argtypes = [vp, C.POINTER(C.c_int32), C.c_int32, _dp]
     L.swl3d_params_default.argtypes = [C.POINTER(Params3D)]
     L.swl3d_session_create.argtypes = [C.POINTER(Params3D), C.c_int32, C.POINTER(vp)]
@@ -280,6 +288,11 @@ class Simulation2D:
         comp = (C.c_int32 * 7)(*[int(bool(c)) for c in components])
         _check(library().swl2d_session_write_snapshot(self._h, str(path).encode(), comp, int(bool(include_material))))
 
+    def write_model(self, path, backend=1, cpu_threads=0, cuda_device=-1):
+        """writeModelVts: the session's model as the reference's versioned model file."""
+        c = ModelCompute(int(backend), int(cpu_threads), int(cuda_device))
+        _check(library().swl2d_session_write_model(self._h, str(path).encode(), C.byref(c)))
+
     def read_probes(self, nodes) -> np.ndarray:
         """Simulation::readProbes: Vx, Vz, Sxx, Szz, Sxz at logical nodes (i, k)."""
         ik = np.ascontiguousarray(np.asarray(nodes, dtype=np.int32).reshape(-1, 2))
@@ -287,6 +300,27 @@ class Simulation2D:
         _check(library().swl2d_session_read_probes(self._h, ik.ctypes.data_as(C.POINTER(C.c_int32)), ik.shape[0],
                                                    out.ctypes.data_as(_dp)))
         return out
+
+
+def read_model(path):
+    """readModelVts: (parameters with the reference's names, compute settings, planned dt) of a 2D
+    model file; the parameters build a Simulation2D."""
+    L = _bind()
+    h = C.c_void_p()
+    _check(L.swl2d_read_model(str(path).encode(), C.byref(h)))
+    try:
+        p, c, dt = Params2D(), ModelCompute(), C.c_double()
+        _check(L.swl2d_model_document_params(h, C.byref(p), C.byref(c), C.byref(dt)))
+        out = {k: getattr(p, f) for k, f in _MAP2D.items() if k not in ("deviceGeometry",)}
+        out["sourceDirection"] = list(p.source_direction)
+        out["layers"] = [[p.layers[i].thickness, p.layers[i].vp, p.layers[i].vs, p.layers[i].density, p.layers[i].qp,
+                          p.layers[i].qs] for i in range(p.n_layers)]
+        if p.n_surface:
+            out["surface"] = [[p.surface_xz[2 * i], p.surface_xz[2 * i + 1]] for i in range(p.n_surface)]
+        compute = {"backend": c.backend, "cpuThreads": c.cpu_threads, "cudaDevice": c.cuda_device}
+        return out, compute, dt.value
+    finally:
+        L.swl2d_model_document_free(h)
 
 
 class Simulation3D:

@@ -191,3 +191,35 @@ def test_3d_snapshot_after_steps_matches_reference(name, S, tmp_path):
     check_snapshot((tmp_path / "s.vts").read_text(), GOLDEN[f"3/{name}/snapshot/n"])
     sim.write_snapshot(tmp_path / "t.vts", SOME3D, include_material=False, include_velocity_vector=False)
     check_snapshot((tmp_path / "t.vts").read_text(), GOLDEN[f"3/{name}/snapshot_some/n"])
+
+
+# ---------------------------------------------------------------- model files (writeModelVts)
+REF_COMPUTE = dict(backend=0, cpu_threads=1, cuda_device=-1)  # the reference runs' settings
+
+
+@pytest.mark.parametrize("name", list(CASES_2D))
+def test_2d_model_file_matches_reference_and_reads_back(name, S, tmp_path):
+    sim = S.Simulation2D(CASES_2D[name], device=MODEL_ONLY)
+    sim.write_model(tmp_path / "m.vts", **REF_COMPUTE)
+    check_snapshot((tmp_path / "m.vts").read_text(), GOLDEN[f"2/{name}/model"])
+    params, compute, dt = S.read_model(tmp_path / "m.vts")
+    assert compute == {"backend": 0, "cpuThreads": 1, "cudaDevice": -1}
+    assert dt == sim.info()["dt"]
+    again = S.Simulation2D(params, device=MODEL_ONLY)  # the file's parameters rebuild the same model
+    again.write_model(tmp_path / "m2.vts", **REF_COMPUTE)
+    assert (tmp_path / "m2.vts").read_bytes() == (tmp_path / "m.vts").read_bytes()
+
+
+def test_2d_model_file_rejects_damage(S, swl, tmp_path):
+    sim = S.Simulation2D(CASES_2D["gsls3_cpml_surface_force"], device=MODEL_ONLY)
+    sim.write_model(tmp_path / "m.vts", **REF_COMPUTE)
+    text = (tmp_path / "m.vts").read_text()
+    i = text.index('Name="Vp"')
+    j = text.index("\n", i) + 1  # first Vp value
+    k = text.index(" ", j)
+    (tmp_path / "bad.vts").write_text(text[:j] + repr(float(text[j:k]) + 1.0) + text[k:])
+    with pytest.raises(swl.SwlError, match="Model checksum mismatch"):
+        S.read_model(tmp_path / "bad.vts")
+    (tmp_path / "cut.vts").write_text(text[: len(text) // 2])
+    with pytest.raises(swl.SwlError):
+        S.read_model(tmp_path / "cut.vts")
