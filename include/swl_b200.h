@@ -66,6 +66,8 @@ typedef struct swl_mesh2d {
     double rates[3];
     const void *delta_p[3], *delta_s[3];
     int32_t precision, array_precision;
+    int32_t segment_rule; /* 0: time the candidate stage-kernel segment lengths at creation; 1: choose by
+                           * occupancy, without running steps (for engines built while others run) */
 } swl_mesh2d;
 
 /* Per-step diagnostics, mirror of the GPU-relevant part of Diagnostics

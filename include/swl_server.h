@@ -27,6 +27,8 @@ typedef struct swl_server_config {
     int32_t max_active;    /* shots building or running at once; 0: only the budget limits */
     int32_t batch_steps;   /* RK4 steps per engine batch (default 64) */
     int32_t build_threads; /* host threads building models (default 4) */
+    int32_t scheduler_threads; /* host threads driving the running shots' batches (default 4); each
+                                * owns the shots it started: polls, records and relaunches them */
 } swl_server_config;
 
 enum { SWL_SHOT_QUEUED = 0, SWL_SHOT_BUILDING = 1, SWL_SHOT_RUNNING = 2, SWL_SHOT_DONE = 3, SWL_SHOT_FAILED = 4 };

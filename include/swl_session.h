@@ -40,6 +40,8 @@ typedef struct swl_params2d {
     double surface_datum;
     const double *surface_xz; /* n_surface pairs (x, elevation) */
     int32_t device_geometry;  /* 1: build the FP64 node geometry on the session's GPU (swl2d_build_geometry) */
+    int32_t segment_rule;     /* 1: the engine's segment length by occupancy rule, without timing runs (the
+                               * server's choice for every shot); 0: timed at creation */
 } swl_params2d;
 
 typedef struct swl_info2d {

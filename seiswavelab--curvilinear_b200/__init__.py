@@ -47,7 +47,7 @@ class Mesh2D(C.Structure):
         ("mechanisms", C.c_int32), ("field_count", C.c_int32), ("cpml_x", _vp), ("cpml_z", _vp),
         ("cpml_width_x", C.c_int32), ("cpml_width_z", C.c_int32), ("cpml_count", C.c_int64),
         ("rates", C.c_double * 3), ("delta_p", _vp * 3), ("delta_s", _vp * 3),
-        ("precision", C.c_int32), ("array_precision", C.c_int32),
+        ("precision", C.c_int32), ("array_precision", C.c_int32), ("segment_rule", C.c_int32),
     ]
 
 

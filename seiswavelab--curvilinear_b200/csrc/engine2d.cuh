@@ -113,6 +113,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     cudaStream_t stream_{}, ownStream_{};
     k2::Mesh<Real> m_{};
     int mech_{}, fc_{};
+    bool segmentRule_{false}; // choose the segment by occupancy instead of timing
     long long count_{}, pcount_{};
     bool cpml_{};
     std::vector<DeviceBuffer> model_;
@@ -286,6 +287,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         count_ = (long long)pitch_ * g.nz;
         const std::size_t n = std::size_t(count_), nu = std::size_t(g.count); // device and caller node counts
         mech_ = g.mechanisms;
+        segmentRule_ = g.segment_rule != 0;
         fc_ = g.field_count;
         nrec_ = nrec;
         const int ap = g.array_precision;
@@ -426,17 +428,18 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         stageGrid_ = dim3((nx_ - 6 + k2::SW - 1) / k2::SW, (nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg));
         dropGraphs(); // the graphs hold the launch shape
     }
-    // The segment length for this grid, picked by timing a few steps per candidate on the fresh
-    // (zero, unforced) state: long segments stream more rows per CTA and re-read fewer halo rows;
-    // short ones put more CTAs in flight and shorten each CTA's chain of row blocks, which is
-    // what a small grid needs.  The state and the clock are reset afterwards.  The choice is kept
+    // The segment length for this grid.  By default it is picked by timing a few steps per
+    // candidate on the fresh (zero, unforced) state: long segments stream more rows per CTA and
+    // re-read fewer halo rows; short ones put more CTAs in flight and shorten each CTA's chain of
+    // row blocks, which is what a small grid needs.  The state and the clock are reset afterwards.
+    // With segment_rule set it follows an occupancy rule instead (see below).  The choice is kept
     // per grid shape for the life of the process, so that identical shots always run the same
     // decomposition (FP32 rounding differs slightly between the interior and the boundary forms
     // of a node, which the decomposition decides).
     void tune() {
         static std::mutex mutex;
-        static std::map<std::tuple<int, int, int, int, int, int, int>, int> chosen;
-        const auto key = std::make_tuple(device_, nx_, nz_, mech_, m_.wx, m_.wz, m_.dmp_k1);
+        static std::map<std::tuple<int, int, int, int, int, int, int, bool>, int> chosen;
+        const auto key = std::make_tuple(device_, nx_, nz_, mech_, m_.wx, m_.wz, m_.dmp_k1, segmentRule_);
         {
             std::lock_guard<std::mutex> g(mutex);
             const auto it = chosen.find(key);
@@ -445,22 +448,36 @@ template <class Real> class TypedEngine2D final : public Engine2D {
                 return;
             }
         }
-        swl_profile prof{};
-        profile(0, 1, 1e-6, 10.0, 0.0, prof); // first launches (module load) outside the timing
         int best = k2::MAX_SEG;
-        double bestMs = 0;
-        for (int seg = k2::MAX_SEG; seg >= 1; seg /= 2) {
-            setSegment(seg);
-            profile(0, 3, 1e-6, 10.0, 0.0, prof);
-            const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
-            if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
+        const bool timed = !segmentRule_;
+        if (!timed) {
+            // An engine built while others run (a server's shots) cannot time fairly and should not
+            // stall for it: take the longest segment that still fills one wave of resident CTAs,
+            // else one-block segments.
+            int sms = 0;
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "query SM count");
+            const long long wave = (long long)sms * k2::streamBlocks<Real>();
+            for (best = k2::MAX_SEG; best > 1; best /= 2) {
+                setSegment(best);
+                if ((long long)stageGrid_.x * stageGrid_.y >= wave) break;
+            }
+        } else {
+            swl_profile prof{};
+            profile(0, 1, 1e-6, 10.0, 0.0, prof); // first launches (module load) outside the timing
+            double bestMs = 0;
+            for (int seg = k2::MAX_SEG; seg >= 1; seg /= 2) {
+                setSegment(seg);
+                profile(0, 3, 1e-6, 10.0, 0.0, prof);
+                const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
+                if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
+            }
         }
         {
             std::lock_guard<std::mutex> g(mutex);
             best = chosen.emplace(key, best).first->second; // a concurrent creation may have decided first
         }
         setSegment(best);
-        reset();
+        if (timed) reset();
     }
     ~TypedEngine2D() override {
         if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);

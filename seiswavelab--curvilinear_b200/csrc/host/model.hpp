@@ -66,6 +66,8 @@ struct Params2D {
     // (-1: the largest) instead of on the host; not part of the reference's Parameters.
     bool deviceGeometry{false};
     int geometryDevice{-1};
+    // the engine's stage-kernel segment by occupancy rule instead of timing runs (a server's shots)
+    bool segmentRule{false};
     std::vector<Layer2D> layers{{20, 1500, 700, 2050, 100, 60}, {50, 2500, 1300, 2250, 100, 60}, {0, 4000, 2300, 2650, 100, 60}};
 };
 

@@ -53,6 +53,7 @@ class Server {
         if (device_ < 0) throw Failure(SWL_ERR_UNAVAILABLE, "no usable sm_100 CUDA device for the server");
         if (cfg_.batch_steps <= 0) cfg_.batch_steps = 64;
         if (cfg_.build_threads <= 0) cfg_.build_threads = 4;
+        if (cfg_.scheduler_threads <= 0) cfg_.scheduler_threads = 4;
         budget_ = cfg_.memory_budget;
         if (budget_ <= 0) {
             DeviceScope scope(device_);
@@ -61,7 +62,7 @@ class Server {
             budget_ = int64_t(0.85 * double(freeB));
         }
         for (int t = 0; t < cfg_.build_threads; ++t) builders_.emplace_back([this] { buildLoop(); });
-        loop_ = std::thread([this] { schedule(); });
+        for (int t = 0; t < cfg_.scheduler_threads; ++t) loops_.emplace_back([this] { schedule(); });
         reaper_ = std::thread([this] { reapLoop(); });
     }
     ~Server() {
@@ -74,7 +75,7 @@ class Server {
         cvDone_.notify_all();
         cvReap_.notify_all();
         for (auto &t : builders_) t.join();
-        loop_.join();
+        for (auto &t : loops_) t.join();
         reaper_.join();
     }
     int64_t submit(std::shared_ptr<Shot> s) {
@@ -156,10 +157,10 @@ class Server {
     std::deque<std::shared_ptr<Shot>> toBuild_, built_;
     std::map<int64_t, std::shared_ptr<Shot>> shots_;
     int64_t nextId_{}, finished_{}, building_{};
-    int peakRunning_{};
+    int running_{}, peakRunning_{};
     bool stop_{false};
     std::vector<std::thread> builders_;
-    std::thread loop_;
+    std::vector<std::thread> loops_;
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
     int64_t submittedCount() const { return nextId_; }
@@ -196,6 +197,7 @@ class Server {
                 if (s->dim == 2) {
                     auto x = std::make_unique<Session2D>();
                     x->params = s->p2;
+                    x->params.segmentRule = true; // built while other shots run: no timing runs
                     x->create(device_);
                     s->s2 = std::move(x);
                 } else {
@@ -263,20 +265,23 @@ class Server {
             cvBuild_.notify_one();
         }
     }
+    // One scheduler thread: it takes built shots (one per pass, so the shots spread over the
+    // threads) and drives the ones it took -- poll, record, relaunch -- until they finish.
     void schedule() {
         std::vector<std::shared_ptr<Shot>> running;
         for (;;) {
             {
                 std::unique_lock<std::mutex> g(mu_);
                 if (stop_) break;
-                while (!built_.empty()) {
+                if (!built_.empty()) {
                     built_.front()->state = SWL_SHOT_RUNNING;
                     built_.front()->run = now();
                     running.push_back(built_.front());
                     built_.pop_front();
+                    ++running_;
                 }
-                peakRunning_ = std::max(peakRunning_, int(running.size()));
-                admit(int(running.size()));
+                peakRunning_ = std::max(peakRunning_, running_);
+                admit(running_);
             }
             bool progressed = false;
             for (std::size_t i = 0; i < running.size();) {
@@ -312,6 +317,7 @@ class Server {
                     // freeing device memory waits for the whole device, which would stall the other
                     // shots' batches if this loop did it.
                     std::lock_guard<std::mutex> g(mu_);
+                    --running_;
                     finishShot(s, error.empty() ? SWL_SHOT_DONE : SWL_SHOT_FAILED, error, false);
                     reap_.push_back(s);
                     cvReap_.notify_one();
@@ -344,6 +350,7 @@ void swl_server_config_default(swl_server_config *c) {
     if (!c) return;
     *c = swl_server_config{};
     c->device = -1, c->memory_budget = 0, c->max_active = 0, c->batch_steps = 64, c->build_threads = 4;
+    c->scheduler_threads = 4;
 }
 swl_status swl_server_create(const swl_server_config *c, swl_server **out) {
     return swl::host::guard([&] {

@@ -104,6 +104,7 @@ struct Session2D {
             for (int l = 0; l < model.mechanisms; ++l)
                 m.rates[l] = model.rates[l], m.delta_p[l] = model.deltaP[l].data(), m.delta_s[l] = model.deltaS[l].data();
             m.precision = params.precision, m.array_precision = SWL_FP64;
+            m.segment_rule = params.segmentRule ? 1 : 0;
             ok(swl2d_create(&m, model.receiverNodes.data(), int32_t(model.receiverNodes.size()), device, &engine));
             ok(swl2d_reserve(engine, std::min(model.total, maxBatch))); // batch tables sized once, at creation
             ok(swl2d_diagnostics(engine, &diag));
@@ -222,6 +223,7 @@ inline Params2D toParams(const swl_params2d &c) {
     if (c.n_surface < 0 || (c.n_surface && !c.surface_xz)) throw std::runtime_error("Invalid surface sample list.");
     for (int i = 0; i < c.n_surface; ++i) p.surfaceSamples.push_back({c.surface_xz[2 * i], c.surface_xz[2 * i + 1]});
     p.deviceGeometry = c.device_geometry != 0;
+    p.segmentRule = c.segment_rule != 0;
     return p;
 }
 

@@ -39,7 +39,7 @@ class Params2D(C.Structure):
         ("attenuation", C.c_int32), ("mechanisms", C.c_int32),
         *[(k, C.c_double) for k in ("q_min_frequency", "q_max_frequency", "q_reference_frequency", "qp", "qs")],
         ("imported_surface", C.c_int32), ("n_surface", C.c_int32), ("surface_datum", C.c_double),
-        ("surface_xz", _dp), ("device_geometry", C.c_int32),
+        ("surface_xz", _dp), ("device_geometry", C.c_int32), ("segment_rule", C.c_int32),
     ]
 
 
@@ -149,7 +149,7 @@ _MAP2D = {
     "attenuation": "attenuation", "mechanisms": "mechanisms", "qMinFrequency": "q_min_frequency",
     "qMaxFrequency": "q_max_frequency", "qReferenceFrequency": "q_reference_frequency", "qp": "qp", "qs": "qs",
     "importedSurface": "imported_surface", "surfaceDatum": "surface_datum",
-    "deviceGeometry": "device_geometry",
+    "deviceGeometry": "device_geometry", "segmentRule": "segment_rule",
 }
 _MAP3D = {
     "precision": "precision", "nx": "nx", "ny": "ny", "nz": "nz", "spacing": "spacing", "vp": "vp", "vs": "vs",
@@ -311,7 +311,7 @@ def read_model(path):
     try:
         p, c, dt = Params2D(), ModelCompute(), C.c_double()
         _check(L.swl2d_model_document_params(h, C.byref(p), C.byref(c), C.byref(dt)))
-        out = {k: getattr(p, f) for k, f in _MAP2D.items() if k not in ("deviceGeometry",)}
+        out = {k: getattr(p, f) for k, f in _MAP2D.items() if k not in ("deviceGeometry", "segmentRule")}
         out["sourceDirection"] = list(p.source_direction)
         out["layers"] = [[p.layers[i].thickness, p.layers[i].vp, p.layers[i].vs, p.layers[i].density, p.layers[i].qp,
                           p.layers[i].qs] for i in range(p.n_layers)]

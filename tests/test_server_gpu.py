@@ -37,7 +37,9 @@ def mix():
 
 
 def alone(S, dim, params):
-    sim = (S.Simulation2D if dim == 2 else S.Simulation3D)(params, device=0)
+    # the same shot in the same form, alone: the server picks 2D stage segments by rule (no timing
+    # runs while other shots run), and so does this session
+    sim = (S.Simulation2D(dict(params, segmentRule=1), device=0) if dim == 2 else S.Simulation3D(params, device=0))
     sim.advance(sim.info()["total_steps"])
     return sim.records()
 
