@@ -428,7 +428,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         stageGrid_ = dim3((nx_ - 6 + k2::SW - 1) / k2::SW, (nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg));
         dropGraphs(); // the graphs hold the launch shape
     }
-    // The segment length for this grid.  By default it is picked by timing a few steps per
+    // The segment length for this grid.  By default it is picked by timing an 8-step graph per
     // candidate on the fresh (zero, unforced) state: long segments stream more rows per CTA and
     // re-read fewer halo rows; short ones put more CTAs in flight and shorten each CTA's chain of
     // row blocks, which is what a small grid needs.  The state and the clock are reset afterwards.
@@ -452,25 +452,38 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         const bool timed = !segmentRule_;
         if (!timed) {
             // An engine built while others run (a server's shots) cannot time fairly and should not
-            // stall for it: take the longest segment that still fills one wave of resident CTAs,
-            // else one-block segments.
+            // stall for it: the shortest segment that keeps the grid within eight waves of resident
+            // CTAs.  Short segments shorten each CTA's chain of row blocks, which bounds a small
+            // grid's step; past a few waves, longer ones save re-read halo rows.
             int sms = 0;
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "query SM count");
-            const long long wave = (long long)sms * k2::streamBlocks<Real>();
-            for (best = k2::MAX_SEG; best > 1; best /= 2) {
+            const long long waves8 = 8LL * sms * k2::streamBlocks<Real>();
+            for (best = 1;; best *= 2) {
                 setSegment(best);
-                if ((long long)stageGrid_.x * stageGrid_.y >= wave) break;
+                if ((long long)stageGrid_.x * stageGrid_.y <= waves8 || best == k2::MAX_SEG) break;
             }
         } else {
-            swl_profile prof{};
-            profile(0, 1, 1e-6, 10.0, 0.0, prof); // first launches (module load) outside the timing
+            // Each candidate is timed as an 8-step CUDA graph, the form a batch runs in: timing eager
+            // steps would measure the host's launch gaps, which dominate a small grid's step.
+            cudaEvent_t e0{}, e1{};
+            check(cudaEventCreate(&e0), "create event");
+            check(cudaEventCreate(&e1), "create event");
             double bestMs = 0;
             for (int seg = k2::MAX_SEG; seg >= 1; seg /= 2) {
                 setSegment(seg);
-                profile(0, 3, 1e-6, 10.0, 0.0, prof);
-                const double ms = prof.stage_ms[0] + prof.stage_ms[1] + prof.stage_ms[2] + prof.stage_ms[3];
+                launch(0, 8, 1e-6, 10.0, 0.0, 0.3); // records this segment's graph (and loads modules)
+                finish();
+                check(cudaEventRecord(e0, stream_), "record event");
+                launch(0, 8, 1e-6, 10.0, 0.0, 0.3);
+                check(cudaEventRecord(e1, stream_), "record event");
+                finish();
+                check(cudaEventSynchronize(e1), "tuning completion");
+                float ms = 0;
+                check(cudaEventElapsedTime(&ms, e0, e1), "event time");
                 if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
             }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
         }
         {
             std::lock_guard<std::mutex> g(mutex);

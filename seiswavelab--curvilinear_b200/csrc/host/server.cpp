@@ -29,21 +29,29 @@ struct Shot {
     int total() const { return dim == 2 ? (s2 ? s2->model.total : 0) : (s3 ? s3->model.total : 0); }
 };
 
-// Device bytes of a request before its model exists (src/two_d/MemoryBudget2D.hpp:12-38 style:
-// four state sets, the model arrays, ADE memories, plus a fixed allowance).
+// Device bytes of a request before its model exists (src/two_d/MemoryBudget2D.hpp:12-38 style), an
+// upper bound of what its engine will hold: the state sets (six in FP32, with the compensation),
+// the model arrays, the ADE memories, the trace table of the largest batch, and an allowance.
 int64_t estimate(const Shot &s) {
+    constexpr double allowance = double(64ll << 20);
     if (s.dim == 2) {
         const auto &p = s.p2;
         const int wx = std::clamp(p.spongeX, 1, std::max(1, p.nx / 3)), wz = std::clamp(p.spongeZ, 1, std::max(1, p.nz / 3));
         const bool ext = p.absorbing && p.externalAbsorption;
-        const double n = double(p.nx + 6 + (ext ? 2 * wx : 0)) * (p.nz + 6 + (ext ? wz : 0));
+        const int nxp = p.nx + 6 + (ext ? 2 * wx : 0), nzp = p.nz + 6 + (ext ? wz : 0);
+        const double n = double((nxp + 1 + 7) / 8 * 8) * nzp; // pitched rows
         const int L = p.attenuation.enabled ? p.attenuation.mechanisms : 0, fc = L ? 6 + 4 * L : 5;
-        const double s = p.precision == SWL_FP32 ? 4 : 8;
-        return int64_t(n * s * (4 * fc + 14 + 2 * L)) + (64ll << 20);
+        const double b = p.precision == SWL_FP32 ? 4 : 8, sets = p.precision == SWL_FP32 ? 6 : 4;
+        const double cpml = p.absorbing && p.absorber == 1 ? 4.0 * (2.0 * wx * nzp + double(wz) * nxp) : 0;
+        const double traces = double(std::max(1, p.receiverCount)) * std::min(p.maxSteps, host::maxBatch) * 2 * 8;
+        return int64_t(n * b * (sets * fc + 14 + 2 * L) + sets * b * cpml + traces + allowance);
     }
     const auto &p = s.p3;
-    const double n = double(p.nx + 6) * (p.ny + 6) * (p.nz + 6), bytes = p.precision == SWL_FP32 ? 4 : 8;
-    return int64_t(n * bytes * (36 + 9 + 5 + (p.layered ? 3 : 0) + (p.sourceKind == 1 ? 3 : 0))) + (64ll << 20);
+    const double n = double((p.nx + 6 + 3) / 4 * 4) * (p.ny + 6) * (p.nz + 6); // pitched rows
+    const double b = p.precision == SWL_FP32 ? 4 : 8, sets = p.precision == SWL_FP32 ? 6 : 4;
+    const double receivers = double(std::max(1, p.receiverCountX)) * std::max(1, p.receiverCountY);
+    const double traces = receivers * std::min(p.maxSteps, host::maxBatch) * 3 * 8;
+    return int64_t(n * b * (sets * 9 + 9 + 5 + (p.layered ? 3 : 0) + (p.sourceKind == 1 ? 3 : 0)) + traces + allowance);
 }
 
 class Server {

@@ -1,11 +1,52 @@
 // Device inventory and shared host math.
 #include "runtime.cuh"
+#include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 
 namespace swl {
 
 // Device selection in the manner of selectCudaDevice3D (src/common/ComputeDevices.cpp:16-40):
 // an explicit index must be a usable sm_100 device; -1 picks the one with the most memory.
+namespace {
+constexpr std::size_t kPinnedCacheBytes = std::size_t(1) << 30;
+std::mutex pinnedMutex;
+std::multimap<std::size_t, void *> pinnedIdle; // size -> block
+std::size_t pinnedIdleBytes = 0;
+} // namespace
+
+void *pinnedTake(std::size_t n, std::size_t &got) {
+    {
+        std::lock_guard<std::mutex> g(pinnedMutex);
+        const auto it = pinnedIdle.lower_bound(n);
+        if (it != pinnedIdle.end() && it->first <= 4 * n + 4096) { // first fit, not far larger
+            void *p = it->second;
+            got = it->first;
+            pinnedIdleBytes -= it->first;
+            pinnedIdle.erase(it);
+            return p;
+        }
+    }
+    const std::size_t size = std::max<std::size_t>(n, 4096);
+    void *p = nullptr;
+    check(cudaMallocHost(&p, size), "allocate pinned host buffer");
+    got = size;
+    return p;
+}
+
+void pinnedGive(void *p, std::size_t n) {
+    {
+        std::lock_guard<std::mutex> g(pinnedMutex);
+        if (pinnedIdleBytes + n <= kPinnedCacheBytes) {
+            pinnedIdle.emplace(n, p);
+            pinnedIdleBytes += n;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+}
+
 int selectDevice(int requested) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) {

@@ -36,20 +36,28 @@ struct DeviceScope {
     DeviceScope &operator=(const DeviceScope &) = delete;
 };
 
-// Owning device allocation (zeroed on allocation).
+// Owning device allocation (zeroed on allocation), from the device's stream-ordered memory pool.
+// cudaMalloc / cudaFree synchronise the whole device, which stalls every other shot a server
+// runs; an allocation here is made and cleared on the calling thread's stream and waited for, so
+// it is usable on any stream, and a release returns the memory to the pool without a device-wide
+// synchronisation.  The owner must have finished its own work on the buffer before releasing it
+// (the engines synchronise their stream first).
 struct DeviceBuffer {
     void *ptr{};
     std::size_t bytes{};
+    int device{-1};
     DeviceBuffer() = default;
     explicit DeviceBuffer(std::size_t n) { allocate(n); }
     DeviceBuffer(const DeviceBuffer &) = delete;
     DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(std::exchange(o.ptr, nullptr)), bytes(std::exchange(o.bytes, 0)) {}
+    DeviceBuffer(DeviceBuffer &&o) noexcept
+        : ptr(std::exchange(o.ptr, nullptr)), bytes(std::exchange(o.bytes, 0)), device(std::exchange(o.device, -1)) {}
     DeviceBuffer &operator=(DeviceBuffer &&o) noexcept {
         if (this != &o) {
             release();
             ptr = std::exchange(o.ptr, nullptr);
             bytes = std::exchange(o.bytes, 0);
+            device = std::exchange(o.device, -1);
         }
         return *this;
     }
@@ -57,22 +65,36 @@ struct DeviceBuffer {
     void allocate(std::size_t n) {
         release();
         if (!n) return;
-        cudaError_t e = cudaMalloc(&ptr, n);
+        check(cudaGetDevice(&device), "query current device");
+        cudaError_t e = cudaMallocAsync(&ptr, n, cudaStreamPerThread);
         if (e != cudaSuccess) {
             ptr = nullptr;
             cudaGetLastError();
             throw Error(-3, std::string("CUDA allocate ") + std::to_string(n) + " bytes: " + cudaGetErrorString(e));
         }
         bytes = n;
-        check(cudaMemset(ptr, 0, n), "clear allocation");
+        check(cudaMemsetAsync(ptr, 0, n, cudaStreamPerThread), "clear allocation");
+        check(cudaStreamSynchronize(cudaStreamPerThread), "allocation");
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            int current = -1;
+            cudaGetDevice(&current);
+            if (current != device) cudaSetDevice(device);
+            cudaFreeAsync(ptr, cudaStreamPerThread);
+            if (current != device && current >= 0) cudaSetDevice(current);
+        }
         ptr = nullptr;
         bytes = 0;
     }
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
+
+// Page-locked host blocks are kept for reuse instead of being freed: cudaFreeHost synchronises the
+// device (stalling every running shot), and cudaMallocHost is slow.  Blocks are handed out first
+// fit by size; at most `kPinnedCacheBytes` are kept idle.
+void *pinnedTake(std::size_t n, std::size_t &got);
+void pinnedGive(void *p, std::size_t n);
 
 // Owning pinned host allocation for asynchronous copies.
 struct PinnedBuffer {
@@ -85,11 +107,10 @@ struct PinnedBuffer {
     void reserve(std::size_t n) {
         if (n <= bytes) return;
         release();
-        check(cudaMallocHost(&ptr, n), "allocate pinned host buffer");
-        bytes = n;
+        ptr = pinnedTake(n, bytes);
     }
     void release() {
-        if (ptr) cudaFreeHost(ptr);
+        if (ptr) pinnedGive(ptr, bytes);
         ptr = nullptr;
         bytes = 0;
     }
