@@ -274,7 +274,7 @@ def _load_dir(d: Path) -> dict:
 
 def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_mesh: bool = True,
                   workdir: Path | None = None, timeout: float | None = None, warmup: int = 0,
-                  backend: str = "cpu") -> dict:
+                  backend: str = "cpu", files: bool = False) -> dict:
     """Run the reference solver built from its sources: its CPU loops, or (2D, backend="cuda")
     its own CUDA engine."""
     exe = REF2D_CUDA if backend == "cuda" else REF2D if dim == 2 else REF3D
@@ -289,7 +289,8 @@ def run_reference(dim: int, case: dict, steps: int = -1, threads: int = 1, dump_
     write_case(case, workdir / "case.txt")
     out = workdir / "out"
     proc = subprocess.run([str(exe), str(workdir / "case.txt"), str(out), str(steps), str(threads),
-                           "1" if dump_mesh else "0", str(int(warmup)), backend], capture_output=True, text=True,
+                           "1" if dump_mesh else "0", str(int(warmup)), backend] + (["files"] if files else []),
+                          capture_output=True, text=True,
                           timeout=timeout)
     if proc.returncode != 0:
         raise RuntimeError(f"reference {dim}D run failed ({proc.returncode}): {proc.stderr.strip()}")

@@ -4,7 +4,8 @@
 // float64 files.  Nothing in the product links or runs this program; tests use it as
 // the parity truth and bench.py times it as the reference CPU arm.
 //
-// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps] [cpu|cuda]
+// Usage: ref2d <case.txt> <outdir> [steps] [threads] [dump_mesh 0|1] [warmup steps] [cpu|cuda] [files]
+//   files  : also write the reference's receiver CSV, SEG-Y, snapshot and model files (small cases only)
 //   steps  : accepted RK4 steps to run (default: the session's total)
 //   threads: ComputeSettings3D::cpuThreads (0 = reference default)
 //
@@ -227,16 +228,17 @@ int main(int argc, char **argv) {
         }
         write(out, "tracesVx.bin", vx);
         write(out, "tracesVz.bin", vz);
-        { // the reference's receiver CSV (writeReceivers, CurvilinearSolver2D.cpp:811-855)
+        const bool files = argc > 8 && std::string(argv[8]) == "files";
+        if (files) { // the reference's receiver CSV (writeReceivers, CurvilinearSolver2D.cpp:811-855)
             std::string csvError;
             if (!writeReceivers(sim, out / "receivers.csv", csvError)) std::ofstream(out / "csv_error.txt") << csvError << '\n';
         }
-        { // writeModelVts (src/two_d/ModelIo2D.cpp:75-145) with this run's compute settings
+        if (files) { // writeModelVts (src/two_d/ModelIo2D.cpp:75-145) with this run's compute settings
             std::string modelError;
             if (!writeModelVts(sim, out / "model.vts", ComputeSettings3D{threads, -1}, modelError))
                 std::ofstream(out / "model_error.txt") << modelError << '\n';
         }
-        { // writeSnapshot (CurvilinearSolver2D.cpp:725-810) with the default options and with every component
+        if (files) { // writeSnapshot (CurvilinearSolver2D.cpp:725-810) with the default options and with every component
             std::string vtsError;
             SnapshotExportOptions all;
             all.components = {true, true, true, true, true, true, true};
@@ -254,7 +256,7 @@ int main(int argc, char **argv) {
                 write(out, "probes.bin", flat);
             }
         }
-        { // the workbench's record view (src/two_d/ui/Workbench2D.cpp:251-268) through writeSegy
+        if (files) { // the workbench's record view (src/two_d/ui/Workbench2D.cpp:251-268) through writeSegy
             SeisWave::RecordDataView data;
             data.dt = sim.recordDt();
             data.components = {"Vz", "Vx"};

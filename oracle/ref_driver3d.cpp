@@ -198,13 +198,14 @@ int main(int argc, char **argv) {
         write(out, "tracesVx.bin", vx);
         write(out, "tracesVy.bin", vy);
         write(out, "tracesVz.bin", vz);
-        { // the reference's receiver CSV files (src/three_d/ReceiverIo.cpp): all components, and Vx+Vz
+        const bool files = argc > 8 && std::string(argv[8]) == "files";
+        if (files) { // the reference's receiver CSV files (src/three_d/ReceiverIo.cpp): all components, and Vx+Vz
             std::string csvError;
             if (!writeReceiversCsv(sim, out / "receivers.csv", {true, true, true}, csvError) ||
                 !writeReceiversCsv(sim, out / "receivers_xz.csv", {true, false, true}, csvError))
                 std::ofstream(out / "csv_error.txt") << csvError << '\n';
         }
-        { // writeVts (src/three_d/VtsWriter.cpp) of the snapshot, default options and a reduced set
+        if (files) { // writeVts (src/three_d/VtsWriter.cpp) of the snapshot, default options and a reduced set
             std::string vtsError;
             VtsExportOptions3D some;
             some.fields = {false, false, true, false, true, false, false, false, true, false, false};
@@ -215,7 +216,7 @@ int main(int argc, char **argv) {
                 !writeVts(snap, out / "snapshot_some.vts", some, vtsError))
                 std::ofstream(out / "vts_error.txt") << vtsError << '\n';
         }
-        { // the record view of src/three_d/ui/RecordView3D.cpp:5-6 through writeSegy
+        if (files) { // the record view of src/three_d/ui/RecordView3D.cpp:5-6 through writeSegy
             SeisWave::RecordDataView data;
             data.dt = sim.dt();
             data.components = {"Vz", "Vx", "Vy"};

@@ -50,8 +50,8 @@ def main():
     out, segy = {}, {}
     for dim, cases, run in ((2, CASES_2D, O.run_reference_2d), (3, CASES_3D, O.run_reference_3d)):
         for name, case in cases.items():
-            zero = run(case, steps=0, dump_mesh=False)
-            full = run(case, steps=int(case["maxSteps"]), dump_mesh=False)
+            zero = run(case, steps=0, dump_mesh=False, files=True)
+            full = run(case, steps=int(case["maxSteps"]), dump_mesh=False, files=True)
             files = ["receivers"] if dim == 2 else ["receivers", "receivers_xz"]
             for f in files:
                 out[f"{dim}/{name}/{f}/0"] = zero["csv:" + f]
