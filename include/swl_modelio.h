@@ -1,4 +1,4 @@
-/* swl_b200 model files: a 2D session's model as the reference's versioned ASCII VTS model
+/* swl_b200 model files: a 2D or 3D session's model as the reference's versioned ASCII VTS model
  * document, and the reader that turns such a file back into session parameters, so that shot
  * requests can be specified by the reference's own model files.
  *
@@ -32,6 +32,15 @@ swl_status swl2d_read_model(const char *path, swl2d_model_document **out);
 swl_status swl2d_model_document_params(const swl2d_model_document *d, swl_params2d *params, swl_model_compute *compute,
                                        double *reference_dt);
 void swl2d_model_document_free(swl2d_model_document *d);
+
+/* The same for 3D: writeModelVts3D / readModelVts3D (include/Seis3D/ModelIo3D.hpp,
+ * src/three_d/ModelIo3D.cpp), schema 1 (analytic terrain) or 2 (embedded DEM), layer names kept. */
+swl_status swl3d_session_write_model(const swl3d_session *s, const char *path, const swl_model_compute *compute);
+typedef struct swl3d_model_document swl3d_model_document;
+swl_status swl3d_read_model(const char *path, swl3d_model_document **out);
+swl_status swl3d_model_document_params(const swl3d_model_document *d, swl_params3d *params, swl_model_compute *compute,
+                                       double *reference_dt);
+void swl3d_model_document_free(swl3d_model_document *d);
 
 #ifdef __cplusplus
 }

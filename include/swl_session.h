@@ -107,6 +107,7 @@ typedef struct swl_params3d {
     int32_t absorbing, absorbing_cells[3];
     double absorbing_strength;
     int32_t device_geometry; /* 1: build the FP64 node geometry on the session's GPU (swl3d_build_geometry) */
+    const char *const *layer_names; /* n_layers UTF-8 names (MaterialLayer3D::name), or null: unnamed */
 } swl_params3d;
 
 typedef struct swl_info3d {

@@ -34,6 +34,7 @@
 #include "Seis3D/ReceiverIo.hpp"
 #include "Seis3D/VtsWriter.hpp"
 #undef private
+#include "Seis3D/ModelIo3D.hpp"
 
 using namespace Seis3D::Curvilinear;
 
@@ -204,6 +205,11 @@ int main(int argc, char **argv) {
             if (!writeReceiversCsv(sim, out / "receivers.csv", {true, true, true}, csvError) ||
                 !writeReceiversCsv(sim, out / "receivers_xz.csv", {true, false, true}, csvError))
                 std::ofstream(out / "csv_error.txt") << csvError << '\n';
+        }
+        if (files) { // writeModelVts3D (src/three_d/ModelIo3D.cpp:87-170) with this run's compute settings
+            std::string modelError;
+            if (!writeModelVts3D(sim, out / "model.vts", ComputeSettings3D{threads, -1}, modelError))
+                std::ofstream(out / "model_error.txt") << modelError << '\n';
         }
         if (files) { // writeVts (src/three_d/VtsWriter.cpp) of the snapshot, default options and a reduced set
             std::string vtsError;

@@ -144,6 +144,7 @@ struct Params3D {
     // FP64 node geometry built on this CUDA device (-1: the largest) instead of on the host
     bool deviceGeometry{false};
     int geometryDevice{-1};
+    std::vector<std::string> layerNames; // MaterialLayer3D::name per layer (may be shorter: unnamed)
 };
 struct Model3D {
     int nx{}, ny{}, nz{};

@@ -376,6 +376,8 @@ inline Params3D toParams(const swl_params3d &c) {
     for (int a = 0; a < 3; ++a) p.absorbingCells[a] = c.absorbing_cells[a];
     p.absorbingStrength = c.absorbing_strength;
     p.deviceGeometry = c.device_geometry != 0;
+    if (c.layer_names)
+        for (int l = 0; l < c.n_layers; ++l) p.layerNames.push_back(c.layer_names[l] ? c.layer_names[l] : "");
     return p;
 }
 

@@ -74,7 +74,7 @@ class Params3D(C.Structure):
                                    "receiver_count_x", "receiver_count_y", "receiver_stride_x", "receiver_stride_y",
                                    "receiver_limit")],
         ("absorbing", C.c_int32), ("absorbing_cells", C.c_int32 * 3), ("absorbing_strength", C.c_double),
-        ("device_geometry", C.c_int32),
+        ("device_geometry", C.c_int32), ("layer_names", C.POINTER(C.c_char_p)),
     ]
 
 
@@ -130,6 +130,10 @@ def _bind():
     L.swl3d_session_engine.argtypes = [vp]
     L.swl3d_session_engine.restype = vp
     L.swl3d_session_write_snapshot.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int32), C.c_int32, C.c_int32]
+    L.swl3d_session_write_model.argtypes = [vp, C.c_char_p, C.POINTER(ModelCompute)]
+    L.swl3d_read_model.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.swl3d_model_document_params.argtypes = [vp, C.POINTER(Params3D), C.POINTER(ModelCompute), _dp]
+    L.swl3d_model_document_free.argtypes = [vp]
     _bound = True
     return L
 
@@ -208,6 +212,10 @@ def params3d(params: dict):
         arr = (Layer3D * len(rows))(*[Layer3D(*r) for r in rows])
         keep.append(arr)
         p.layers, p.n_layers = arr, len(rows)
+    if "layerNames" in params:
+        names = (C.c_char_p * len(params["layerNames"]))(*[n.encode() for n in params["layerNames"]])
+        keep.append(names)
+        p.layer_names = C.cast(names, C.POINTER(C.c_char_p))
     if "receiverArray" in params:  # kind startX startY z countX countY strideX strideY
         r = [int(x) for x in params["receiverArray"]]
         (p.receiver_kind, p.receiver_start_x, p.receiver_start_y, p.receiver_z, p.receiver_count_x,
@@ -379,3 +387,35 @@ class Simulation3D:
         sel = (C.c_int32 * 11)(*[int(bool(c)) for c in fields])
         _check(library().swl3d_session_write_snapshot(self._h, str(path).encode(), sel, int(bool(include_material)),
                                                       int(bool(include_velocity_vector))))
+
+    def write_model(self, path, backend=1, cpu_threads=0, cuda_device=-1):
+        """writeModelVts3D: the session's model as the reference's versioned 3D model file."""
+        c = ModelCompute(int(backend), int(cpu_threads), int(cuda_device))
+        _check(library().swl3d_session_write_model(self._h, str(path).encode(), C.byref(c)))
+
+
+def read_model3d(path):
+    """readModelVts3D: (parameters with the reference's names, compute settings, planned dt) of a 3D
+    model file; the parameters build a Simulation3D."""
+    L = _bind()
+    h = C.c_void_p()
+    _check(L.swl3d_read_model(str(path).encode(), C.byref(h)))
+    try:
+        p, c, dt = Params3D(), ModelCompute(), C.c_double()
+        _check(L.swl3d_model_document_params(h, C.byref(p), C.byref(c), C.byref(dt)))
+        out = {k: getattr(p, f) for k, f in _MAP3D.items() if k not in ("deviceGeometry", "precision", "receiverLimit")}
+        out["sourceDirection"] = list(p.source_direction)
+        out["layers"] = [[p.layers[i].thickness, p.layers[i].vp, p.layers[i].vs, p.layers[i].density]
+                         for i in range(p.n_layers)]
+        if p.n_layers:
+            out["layerNames"] = [p.layer_names[i].decode() for i in range(p.n_layers)]
+        out["receiverArray"] = [p.receiver_kind, p.receiver_start_x, p.receiver_start_y, p.receiver_z,
+                                p.receiver_count_x, p.receiver_count_y, p.receiver_stride_x, p.receiver_stride_y]
+        out["absorbingCells"] = list(p.absorbing_cells)
+        if p.dem_nx:
+            out["demShape"] = [p.dem_nx, p.dem_ny, p.dem_spacing, p.dem_origin_x, p.dem_origin_y, p.dem_datum]
+            out["demElevations"] = np.ctypeslib.as_array(p.dem_elevations, shape=(p.dem_nx * p.dem_ny,)).copy()
+        compute = {"backend": c.backend, "cpuThreads": c.cpu_threads, "cudaDevice": c.cuda_device}
+        return out, compute, dt.value
+    finally:
+        L.swl3d_model_document_free(h)

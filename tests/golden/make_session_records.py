@@ -17,8 +17,9 @@ default options and with every component, and readProbes (:710-724) at four logi
 snapshots are stored as their SHA-256, size and header (through "<PointData"), the probes as values,
 in receivers_csv.json under "2/<case>/snapshot[_all]/<0|n>" and "2/<case>/probes/n".  The 3D
 drivers call writeVts (src/three_d/VtsWriter.cpp) with the default options and with a reduced set
-("3/<case>/snapshot[_some]/<0|n>").  The 2D drivers also save the model with writeModelVts
-(src/two_d/ModelIo2D.cpp:75-145) as a CPU run with one thread ("2/<case>/model").
+("3/<case>/snapshot[_some]/<0|n>").  The drivers also save the model with writeModelVts
+(src/two_d/ModelIo2D.cpp:75-145) and writeModelVts3D (src/three_d/ModelIo3D.cpp:87-170) as a CPU
+run with one thread ("<dim>/<case>/model"); the 3D driver names its layers "layer0", "layer1", ...
 
 Usage: python tests/golden/make_session_records.py   (needs oracle/_ref/ref2d and ref3d: make -C oracle ref)
 """
@@ -67,8 +68,8 @@ def main():
                                                       "head": text[:text.index("<PointData")]}
             if dim == 2:
                 out[f"2/{name}/probes/n"] = [repr(float(v)) for v in full["probes"]]
-                text = zero["vts:model"]  # writeModelVts (src/two_d/ModelIo2D.cpp), compute settings {1 thread, -1}
-                out[f"2/{name}/model"] = {"sha256": hashlib.sha256(text.encode()).hexdigest(), "size": len(text.encode()),
+            text = zero["vts:model"]  # writeModelVts / writeModelVts3D, compute settings {1 thread, -1}
+            out[f"{dim}/{name}/model"] = {"sha256": hashlib.sha256(text.encode()).hexdigest(), "size": len(text.encode()),
                                           "head": text[:text.index("<PointData")]}
             print(dim, name, "ok")
     (HERE / "receivers_csv.json").write_text(json.dumps(out, indent=0))

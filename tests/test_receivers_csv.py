@@ -223,3 +223,64 @@ def test_2d_model_file_rejects_damage(S, swl, tmp_path):
     (tmp_path / "cut.vts").write_text(text[: len(text) // 2])
     with pytest.raises(swl.SwlError):
         S.read_model(tmp_path / "cut.vts")
+
+
+def named_layers(case: dict) -> dict:
+    """The 3D reference driver names its layers "layer0", "layer1", ... (MaterialLayer3D::name)."""
+    p = dict(case)
+    if "layers" in p:
+        p["layerNames"] = [f"layer{i}" for i in range(len(p["layers"]) // 4)]
+    return p
+
+
+@pytest.mark.parametrize("name", list(CASES_3D))
+def test_3d_model_file_matches_reference_and_reads_back(name, S, tmp_path):
+    sim = S.Simulation3D(named_layers(CASES_3D[name]), device=MODEL_ONLY)
+    sim.write_model(tmp_path / "m.vts", **REF_COMPUTE)
+    check_snapshot((tmp_path / "m.vts").read_text(), GOLDEN[f"3/{name}/model"])
+    params, compute, dt = S.read_model3d(tmp_path / "m.vts")
+    assert compute == {"backend": 0, "cpuThreads": 1, "cudaDevice": -1}
+    assert dt == sim.info()["dt"]
+    if "layers" in CASES_3D[name]:
+        assert params["layerNames"] == [f"layer{i}" for i in range(3)]
+    again = S.Simulation3D(params, device=MODEL_ONLY)  # the file's parameters rebuild the same model
+    again.write_model(tmp_path / "m2.vts", **REF_COMPUTE)
+    assert (tmp_path / "m2.vts").read_bytes() == (tmp_path / "m.vts").read_bytes()
+
+
+def test_3d_model_file_with_dem_round_trips(S, tmp_path):
+    """Schema 2: the embedded DEM (SurfaceGridGeometry / SurfaceGridElevations) survives a round trip."""
+    nx, ny = 7, 6
+    y, x = np.mgrid[0:ny, 0:nx]
+    elev = 100.0 + 4.0 * np.sin(0.7 * x) * np.cos(0.5 * y)
+    case = dict(CASES_3D["force"], demShape=[nx, ny, 60.0, -30.0, -30.0, 104.0], demElevations=elev.ravel())
+    sim = S.Simulation3D(case, device=MODEL_ONLY)
+    sim.write_model(tmp_path / "m.vts", **REF_COMPUTE)
+    text = (tmp_path / "m.vts").read_text()
+    assert 'Name="SeisWaveModel3DVersion" NumberOfComponents="1" NumberOfTuples="1" format="ascii">2 ' in text
+    params, _, _ = S.read_model3d(tmp_path / "m.vts")
+    assert params["demShape"] == [nx, ny, 60.0, -30.0, -30.0, 104.0]
+    np.testing.assert_array_equal(params["demElevations"], elev.ravel())
+    again = S.Simulation3D(params, device=MODEL_ONLY)
+    again.write_model(tmp_path / "m2.vts", **REF_COMPUTE)
+    assert (tmp_path / "m2.vts").read_bytes() == (tmp_path / "m.vts").read_bytes()
+
+
+def test_3d_model_file_rejects_damage(S, swl, tmp_path):
+    sim = S.Simulation3D(named_layers(CASES_3D["moment_layered"]), device=MODEL_ONLY)
+    sim.write_model(tmp_path / "m.vts", **REF_COMPUTE)
+    text = (tmp_path / "m.vts").read_text()
+    i = text.index('Name="Jacobian"')
+    j = text.index("\n", i) + 1  # first Jacobian value
+    k = text.index(" ", j)
+    (tmp_path / "bad.vts").write_text(text[:j] + repr(float(text[j:k]) * 1.5) + text[k:])
+    with pytest.raises(swl.SwlError, match="Model checksum mismatch"):
+        S.read_model3d(tmp_path / "bad.vts")
+    (tmp_path / "cut.vts").write_text(text[: len(text) // 2])
+    with pytest.raises(swl.SwlError):
+        S.read_model3d(tmp_path / "cut.vts")
+    (tmp_path / "two.vts").write_text(text.replace('type="StructuredGrid"', 'type="UnstructuredGrid"', 1))
+    with pytest.raises(swl.SwlError, match="Expected a 3D StructuredGrid model VTS."):
+        S.read_model3d(tmp_path / "two.vts")
+    with pytest.raises(swl.SwlError, match="Cannot open 3D model VTS."):
+        S.read_model3d(tmp_path / "missing.vts")
