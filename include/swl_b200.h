@@ -116,6 +116,25 @@ swl_status swl2d_launch(swl2d_engine *engine, int32_t first, int32_t count, doub
 swl_status swl2d_query(swl2d_engine *engine, int32_t *done, int32_t *accepted);
 swl_status swl2d_wait(swl2d_engine *engine, int32_t *accepted);
 
+/* Persistent multi-shot launches: the batches of n engines (one precision, one GSLS mechanism
+ * count, one device) advance together in ONE kernel launch driven by a (shot, tile, stage) work
+ * queue.  Each CTA takes the next item of a fixed global order, waits (bounded) until its shot has
+ * finished the previous phase, and runs the same tile, verdict and receiver record that the
+ * engine's own batch would, so every engine's results equal those of swl2d_launch with the same
+ * arguments.  Each engine's uploads and read-backs stay on its own stream, ordered with the launch
+ * (on the queue's stream) by events; after the launch each engine's batch is completed with
+ * swl2d_query / swl2d_wait / swl2d_traces as after swl2d_launch.
+ * swl2d_queue_query / swl2d_queue_wait report the launch itself: SWL_ERR_CUDA if a wait in it ran
+ * out.  No counterpart in the reference, which steps one simulation per engine. */
+typedef struct swl2d_queue swl2d_queue;
+swl_status swl2d_queue_create(int32_t device, int32_t precision, swl2d_queue **out);
+void swl2d_queue_destroy(swl2d_queue *queue);
+swl_status swl2d_queue_launch(swl2d_queue *queue, swl2d_engine *const *engines, int32_t n, const int32_t *first,
+                              const int32_t *count, const double *dt, const double *frequency, const double *scale,
+                              const double *check_growth_after);
+swl_status swl2d_queue_query(swl2d_queue *queue, int32_t *done);
+swl_status swl2d_queue_wait(swl2d_queue *queue);
+
 swl_status swl2d_rollback(swl2d_engine *engine);    /* CudaEngine::rollback */
 swl_status swl2d_reset(swl2d_engine *engine);       /* CudaEngine::reset: zero fields, memories, traces */
 swl_status swl2d_diagnostics(swl2d_engine *engine, swl_diag2d *out); /* CudaEngine::diagnostics */

@@ -144,6 +144,13 @@ def library() -> C.CDLL:
     L.swl2d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
     L.swl2d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.swl2d_wait.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+    L.swl2d_queue_create.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.swl2d_queue_destroy.argtypes = [C.c_void_p]
+    L.swl2d_queue_launch.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.swl2d_queue_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+    L.swl2d_queue_wait.argtypes = [C.c_void_p]
     L.swl3d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double]
     L.swl3d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.swl3d_wait.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
@@ -162,6 +169,44 @@ def device_count() -> int:
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Queue2D:
+    """Persistent multi-shot launches (swl2d_queue_*): the batches of several Engine2D of one
+    precision and GSLS mechanism count advance together in one kernel launch."""
+
+    def __init__(self, precision: int = SWL_FP32, device: int = -1):
+        h = C.c_void_p()
+        _check(library().swl2d_queue_create(int(device), int(precision), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            library().swl2d_queue_destroy(self._h)
+            self._h = C.c_void_p()
+
+    __del__ = close
+
+    def launch(self, engines, first, count, dt, frequency, scale, growth_after=None):
+        """One launch for batches (first[i], count[i], dt[i], ...) of engines[i]; scalars broadcast."""
+        n = len(engines)
+
+        def vec(v, ctype, default=None):
+            v = default if v is None else v
+            v = [v] * n if np.isscalar(v) else list(v)
+            return (ctype * n)(*v)
+        hs = (C.c_void_p * n)(*[e._h.value for e in engines])
+        _check(library().swl2d_queue_launch(self._h, hs, n, vec(first, C.c_int32), vec(count, C.c_int32),
+                                            vec(dt, C.c_double), vec(frequency, C.c_double), vec(scale, C.c_double),
+                                            vec(growth_after, C.c_double, np.inf)))
+
+    def query(self) -> bool:
+        done = C.c_int32()
+        _check(library().swl2d_queue_query(self._h, C.byref(done)))
+        return bool(done.value)
+
+    def wait(self):
+        _check(library().swl2d_queue_wait(self._h))
 
 
 class Engine2D:

@@ -30,6 +30,10 @@ UNITS = {
     **{f"stages2d.cu@{r}{m}": (["--fmad=false"] if r == "f64" else []) +
        [f"-DSWL_STAGE_REAL={'double' if r == 'f64' else 'float'}", f"-DSWL_STAGE_MECH={m}"]
        for r in ("f64", "f32") for m in range(4)},
+    # the persistent multi-shot 2D kernel, one unit per (precision, GSLS mechanism count)
+    **{f"queue2d.cu@{r}{m}": (["--fmad=false"] if r == "f64" else []) +
+       [f"-DSWL_STAGE_REAL={'double' if r == 'f64' else 'float'}", f"-DSWL_STAGE_MECH={m}", "-DSWL_STAGE_COHERENT=1"]
+       for r in ("f64", "f32") for m in range(4)},
     "engine3d_f64.cu": ["--fmad=false"],
     "engine3d_f32.cu": [],
     "abi.cpp": ["-x", "cu"],

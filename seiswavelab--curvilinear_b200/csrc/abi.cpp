@@ -5,6 +5,7 @@
 #include "engine3d.cuh"
 #include <cstring>
 #include <string>
+#include <vector>
 
 namespace swl {
 std::string &lastErrorRef() {
@@ -53,6 +54,9 @@ struct swl2d_engine {
 };
 struct swl3d_engine {
     std::unique_ptr<swl::Engine3D> impl;
+};
+struct swl2d_queue {
+    std::unique_ptr<swl::Queue2D> impl;
 };
 
 extern "C" {
@@ -145,6 +149,54 @@ swl_status swl2d_wait(swl2d_engine *e, int32_t *accepted) {
         if (accepted) *accepted = acc;
         if (E.faulted())
             throw swl::Error(SWL_ERR_FAULT, "2D step rejected: nonfinite fields or excessive late energy growth. Rebuild the session.");
+    });
+}
+swl_status swl2d_queue_create(int32_t dev, int32_t precision, swl2d_queue **out) {
+    return guarded([&] {
+        need(out, "out");
+        *out = nullptr;
+        if (precision != SWL_FP64 && precision != SWL_FP32) throw swl::Error(SWL_ERR_INVALID, "precision must be SWL_FP64 or SWL_FP32");
+        const int d = device(dev);
+        auto q = std::make_unique<swl2d_queue>();
+        q->impl = precision == SWL_FP64 ? swl::makeQueue2D64(d) : swl::makeQueue2D32(d);
+        *out = q.release();
+    });
+}
+void swl2d_queue_destroy(swl2d_queue *q) {
+    if (!q) return;
+    try {
+        delete q;
+    } catch (...) {
+    }
+}
+swl_status swl2d_queue_launch(swl2d_queue *q, swl2d_engine *const *engines, int32_t n, const int32_t *first, const int32_t *count,
+                              const double *dt, const double *frequency, const double *scale, const double *growthAfter) {
+    return guarded([&] {
+        need(q, "queue");
+        if (n < 0) throw swl::Error(SWL_ERR_INVALID, "engine count must be >= 0");
+        if (n == 0) return;
+        need(engines, "engines"), need(first, "first"), need(count, "count"), need(dt, "dt"), need(frequency, "frequency");
+        need(scale, "scale"), need(growthAfter, "check_growth_after");
+        std::vector<swl::Engine2D *> e(n);
+        for (int i = 0; i < n; ++i) {
+            need(engines[i], "engine");
+            e[i] = engines[i]->impl.get();
+        }
+        const std::vector<int> f(first, first + n), c(count, count + n);
+        q->impl->launch(e.data(), n, f.data(), c.data(), dt, frequency, scale, growthAfter);
+    });
+}
+swl_status swl2d_queue_query(swl2d_queue *q, int32_t *done) {
+    return guarded([&] {
+        need(q, "queue"), need(done, "done");
+        *done = 0;
+        *done = q->impl->query() ? 1 : 0;
+    });
+}
+swl_status swl2d_queue_wait(swl2d_queue *q) {
+    return guarded([&] {
+        need(q, "queue");
+        q->impl->finish();
     });
 }
 swl_status swl2d_rollback(swl2d_engine *e) { return guarded([&] { ENGINE(e); E.rollback(); }); }

@@ -14,6 +14,7 @@
 #include "../../include/swl_b200.h"
 #include "runtime.cuh"
 #include "launch2d.cuh"
+#include "launchq2d.cuh"
 #include "stage2d.cuh"
 #include <algorithm>
 #include <cmath>
@@ -21,6 +22,8 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
+#include <cstddef>
 #include <tuple>
 #include <vector>
 
@@ -58,6 +61,21 @@ class Engine2D {
 
 std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &, const int64_t *, int, int);
 std::unique_ptr<Engine2D> makeEngine2D32(const swl_mesh2d &, const int64_t *, int, int);
+
+// Persistent multi-shot launches (queue2d.cuh): the batches of several engines of one precision
+// and one GSLS mechanism count advance together in one launch on the queue's stream.  After the
+// launch each engine's batch completes like one of its own (query / finish).
+class Queue2D {
+  public:
+    virtual ~Queue2D() = default;
+    virtual void launch(Engine2D *const *engines, int n, const int *first, const int *count, const double *dt,
+                        const double *frequency, const double *scale, const double *growthAfter) = 0;
+    virtual bool query() = 0; // true once the launch completed; throws if a wait in it ran out
+    virtual void finish() = 0;
+    virtual int blocks() const = 0; // CTAs of the last launch
+};
+std::unique_ptr<Queue2D> makeQueue2D64(int device);
+std::unique_ptr<Queue2D> makeQueue2D32(int device);
 
 namespace detail2 {
 
@@ -142,6 +160,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     int registers_{};
     int64_t localBytes_{};
     cudaEvent_t done_{};    // completion of the in-flight batch
+    cudaEvent_t queued_{};  // the uploads of a queued batch (Queue2D)
     bool inflight_{false};
     int batchU0_{0};
     void settle() {
@@ -494,6 +513,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     }
     ~TypedEngine2D() override {
         if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
+        if (queued_) cudaEventDestroy(queued_);
         if (stream_) cudaStreamSynchronize(stream_);
         dropGraphs();
         if (ownStream_) cudaStreamDestroy(ownStream_);
@@ -673,6 +693,73 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
     }
     int segment() const { return m_.seg; }
+
+    // ---- queued batches (Queue2D): the two halves of launch() around the persistent kernel
+    int mechanisms() const { return mech_; }
+    int deviceId() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    long long tiles() const { return (long long)stageGrid_.x * stageGrid_.y; }
+    // The clock and forcing tables of `count` steps from `first`, enqueued on the engine's stream,
+    // and the kernel's description of the batch.
+    void queueBegin(int first, int count, double dt, double frequency, double scale, double growthAfter, k2::QueueShot<Real> &shot) {
+        DeviceScope scope(device_);
+        if (inflight_) throw Error(SWL_ERR_STATE, "a batch is already in flight on this engine");
+        if (faulted_) throw Error(SWL_ERR_STATE, "2D engine holds a rejected step; reset or rebuild it");
+        if (dt != dt_) dropGraphs(), dt_ = dt;
+        ensureCapacity(count);
+        hostClock_.step = first;
+        hostClock_.first = first;
+        hostClock_.faulted = 0;
+        hostClock_.fault_step = -1;
+        hostClock_.accepted = 0;
+        hostClock_.trace_steps = traceCap_;
+        hostClock_.dt = dt;
+        hostClock_.growth_after = growthAfter;
+        pushClock();
+        fillForcing(first, count, dt, frequency, scale);
+        const int su = u_, sa = a_;
+        for (int r = 0; r < 2; ++r) {
+            u_ = r, a_ = 1 - r;
+            for (int k = 0; k < 4; ++k) shot.stage[r][k] = args(k);
+            shot.stage[r][3].partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
+        }
+        u_ = su, a_ = sa;
+        shot.partials = partials_.as<k2::Partial>();
+        shot.receivers = recIdx_.as<long long>();
+        shot.traces = traces_.as<double>();
+        shot.clock = clock_.as<k2::Clock>();
+        shot.sets[0] = set_[0], shot.sets[1] = set_[1];
+        shot.count = count_;
+        shot.nrec = nrec_;
+        shot.tiles = int(tiles());
+        shot.tilesX = int(stageGrid_.x);
+        shot.u0 = u_;
+        shot.steps = count;
+        shot.first = first;
+    }
+    // The uploads of queueBegin, for the queue's stream to wait on.
+    cudaEvent_t queueReady() {
+        DeviceScope scope(device_);
+        if (!queued_) check(cudaEventCreateWithFlags(&queued_, cudaEventDisableTiming), "create queue event");
+        check(cudaEventRecord(queued_, stream_), "record queue uploads");
+        return queued_;
+    }
+    // After the kernel (`kernel`: its completion on the queue's stream): the trace rows and the clock
+    // come back with the batch on the engine's stream; its completion event.
+    void queueEnd(int count, cudaEvent_t kernel) {
+        DeviceScope scope(device_);
+        check(cudaStreamWaitEvent(stream_, kernel, 0), "order after the queued launch");
+        if (nrec_)
+            check(cudaMemcpyAsync(pinnedTraces_.ptr, traces_.ptr, std::size_t(count) * nrec_ * 2 * sizeof(double),
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "read traces");
+        pinnedRows_ = count;
+        clockStats_ = true;
+        check(cudaMemcpyAsync(pinnedClock_.ptr, clock_.ptr, sizeof(k2::Clock), cudaMemcpyDeviceToHost, stream_), "read clock");
+        check(cudaEventRecord(done_, stream_), "record batch completion");
+        batchU0_ = u_;
+        inflight_ = true;
+    }
     void diagnostics(swl_diag2d &d) override {
         settle();
         DeviceScope scope(device_);
@@ -805,4 +892,140 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     }
 };
 
+
+// The persistent multi-shot launch of engines of precision Real (Queue2D).  One device block
+// holds the queue header, the shot descriptions and the order tables; it is written from pinned
+// memory with one copy before the kernel, on the queue's own stream.  Each engine's uploads
+// (clock, forcing) and read-backs (traces, clock) stay on the engine's stream, ordered with the
+// kernel by events, so an engine outlives the queue and keeps working on its own afterwards.
+template <class Real> class TypedQueue2D final : public Queue2D {
+    int device_{}, sms_{}, blocks_{};
+    cudaStream_t stream_{};
+    cudaEvent_t done_{}, kernel_{};
+    DeviceBuffer dev_;
+    PinnedBuffer host_;
+    bool inflight_{false};
+    static std::size_t up(std::size_t n) { return (n + 63) / 64 * 64; }
+    int occupancy(int mech) const {
+        switch (mech) {
+        case 0: return detail2::queueOccupancy2D<Real, 0>();
+        case 1: return detail2::queueOccupancy2D<Real, 1>();
+        case 2: return detail2::queueOccupancy2D<Real, 2>();
+        default: return detail2::queueOccupancy2D<Real, 3>();
+        }
+    }
+    void run(int mech, int blocks, k2::QueueHeader *h, const k2::QueueShot<Real> *shots) {
+        switch (mech) {
+        case 0: detail2::launchQueue2D<Real, 0>(blocks, stream_, h, shots); break;
+        case 1: detail2::launchQueue2D<Real, 1>(blocks, stream_, h, shots); break;
+        case 2: detail2::launchQueue2D<Real, 2>(blocks, stream_, h, shots); break;
+        default: detail2::launchQueue2D<Real, 3>(blocks, stream_, h, shots); break;
+        }
+    }
+
+  public:
+    explicit TypedQueue2D(int device) : device_(device) {
+        DeviceScope scope(device_);
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create queue stream");
+        check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create queue event");
+        check(cudaEventCreateWithFlags(&kernel_, cudaEventDisableTiming), "create queue event");
+        check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "query SM count");
+    }
+    ~TypedQueue2D() override {
+        if (done_) cudaEventSynchronize(done_), cudaEventDestroy(done_);
+        if (kernel_) cudaEventDestroy(kernel_);
+        if (stream_) cudaStreamSynchronize(stream_), cudaStreamDestroy(stream_);
+    }
+    int blocks() const override { return blocks_; }
+    void launch(Engine2D *const *engines, int n, const int *first, const int *count, const double *dt, const double *frequency,
+                const double *scale, const double *growthAfter) override {
+        DeviceScope scope(device_);
+        if (inflight_) throw Error(SWL_ERR_STATE, "a queued launch is already in flight");
+        if (n <= 0) return;
+        std::vector<TypedEngine2D<Real> *> e(n);
+        for (int i = 0; i < n; ++i) {
+            e[i] = dynamic_cast<TypedEngine2D<Real> *>(engines[i]);
+            if (!e[i]) throw Error(SWL_ERR_INVALID, "queued engines must share the queue's precision");
+            if (e[i]->deviceId() != device_) throw Error(SWL_ERR_INVALID, "queued engines must live on the queue's device");
+            if (e[i]->mechanisms() != e[0]->mechanisms()) throw Error(SWL_ERR_INVALID, "queued engines must share one GSLS mechanism count");
+            if (count[i] <= 0 || !(dt[i] > 0) || first[i] < 0) throw Error(SWL_ERR_INVALID, "queued batches need count > 0, dt > 0, first >= 0");
+            for (int k = 0; k < i; ++k)
+                if (e[k] == e[i]) throw Error(SWL_ERR_INVALID, "an engine appears twice in one queued launch");
+        }
+        // shots in the order of their batch length, longest first: the shots stepping at step j
+        // are then a prefix of the order
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return count[a] > count[b]; });
+        const int maxSteps = count[order[0]];
+        const std::size_t oShots = up(sizeof(k2::QueueHeader)), oDone = oShots + up(sizeof(k2::QueueShot<Real>) * n);
+        const std::size_t oStart = oDone + up(sizeof(int) * n), oActive = oStart + up(sizeof(long long) * (maxSteps + 1));
+        const std::size_t oPrefix = oActive + up(sizeof(int) * maxSteps), oAbort = oPrefix + up(sizeof(long long) * (n + 1));
+        const std::size_t bytes = oAbort + 64;
+        if (dev_.bytes < bytes) dev_.allocate(bytes);
+        host_.reserve(bytes);
+        std::memset(host_.ptr, 0, bytes);
+        auto *hb = host_.as<unsigned char>();
+        auto *db = static_cast<unsigned char *>(dev_.ptr);
+        auto *shots = reinterpret_cast<k2::QueueShot<Real> *>(hb + oShots);
+        for (int s = 0; s < n; ++s) {
+            const int i = order[s];
+            new (shots + s) k2::QueueShot<Real>{};
+            e[i]->queueBegin(first[i], count[i], dt[i], frequency[i], scale[i], growthAfter[i], shots[s]);
+            check(cudaStreamWaitEvent(stream_, e[i]->queueReady(), 0), "order the queued launch after the uploads");
+        }
+        auto *prefix = reinterpret_cast<long long *>(hb + oPrefix);
+        for (int s = 0; s < n; ++s) prefix[s + 1] = prefix[s] + shots[s].tiles;
+        auto *start = reinterpret_cast<long long *>(hb + oStart);
+        auto *active = reinterpret_cast<int *>(hb + oActive);
+        for (int j = 0, a = n; j < maxSteps; ++j) {
+            while (a > 0 && count[order[a - 1]] <= j) --a;
+            active[j] = a;
+            start[j + 1] = start[j] + 4 * prefix[a] + a;
+        }
+        auto *h = reinterpret_cast<k2::QueueHeader *>(hb);
+        h->head = 0;
+        h->total = (unsigned long long)start[maxSteps];
+        h->abort = 0;
+        h->nshots = n;
+        h->maxSteps = maxSteps;
+        h->done = reinterpret_cast<int *>(db + oDone);
+        h->stepStart = reinterpret_cast<const long long *>(db + oStart);
+        h->active = reinterpret_cast<const int *>(db + oActive);
+        h->tilePrefix = reinterpret_cast<const long long *>(db + oPrefix);
+        check(cudaMemcpyAsync(dev_.ptr, host_.ptr, oAbort, cudaMemcpyHostToDevice, stream_), "upload queue");
+        const int mech = e[0]->mechanisms();
+        blocks_ = int(std::min<long long>((long long)occupancy(mech) * sms_, (long long)h->total));
+        run(mech, blocks_, reinterpret_cast<k2::QueueHeader *>(db), reinterpret_cast<const k2::QueueShot<Real> *>(db + oShots));
+        check(cudaEventRecord(kernel_, stream_), "record queued launch");
+        for (int i = 0; i < n; ++i) e[i]->queueEnd(count[i], kernel_);
+        check(cudaMemcpyAsync(hb + oAbort, db + offsetof(k2::QueueHeader, abort), sizeof(int), cudaMemcpyDeviceToHost, stream_),
+              "read queue status");
+        check(cudaEventRecord(done_, stream_), "record queue completion");
+        abortAt_ = oAbort;
+        inflight_ = true;
+    }
+    std::size_t abortAt_{};
+    void settled() {
+        inflight_ = false;
+        const int abort = *reinterpret_cast<const int *>(host_.as<unsigned char>() + abortAt_);
+        if (abort == 1) throw Error(SWL_ERR_CUDA, "CUDA 2D queue: a tensor-copy wait ran out");
+        if (abort) throw Error(SWL_ERR_CUDA, "CUDA 2D queue: a stage dependency wait ran out");
+    }
+    bool query() override {
+        if (!inflight_) return true;
+        DeviceScope scope(device_);
+        const cudaError_t st = cudaEventQuery(done_);
+        if (st == cudaErrorNotReady) return false;
+        check(st, "2D queue query");
+        settled();
+        return true;
+    }
+    void finish() override {
+        if (!inflight_) return;
+        DeviceScope scope(device_);
+        check(cudaEventSynchronize(done_), "2D queue completion");
+        settled();
+    }
+};
 } // namespace swl

@@ -7,4 +7,5 @@ namespace swl {
 std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &m, const int64_t *rec, int n, int device) {
     return std::make_unique<TypedEngine2D<double>>(m, rec, n, device);
 }
+std::unique_ptr<Queue2D> makeQueue2D64(int device) { return std::make_unique<TypedQueue2D<double>>(device); }
 } // namespace swl

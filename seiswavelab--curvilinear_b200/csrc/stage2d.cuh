@@ -101,6 +101,16 @@ template <class Real> struct StageArgs {
 template <class Real> constexpr bool kahan() { return sizeof(Real) == 4; }
 
 template <class Real> __device__ __forceinline__ Real ld(const Real *p) { return __ldg(p); }
+// Loads of state that the step itself writes (stage inputs, U, the ADE memories, the Kahan
+// terms).  A stage kernel only reads arrays that the previous launches wrote, so they may take
+// the read-only path; the persistent multi-shot kernel (queue2d.cuh) reads state that other CTAs
+// wrote in the same launch, which the read-only path may serve stale, so it is compiled with
+// SWL_STAGE_COHERENT and loads these words through L2.
+#ifdef SWL_STAGE_COHERENT
+template <class Real> __device__ __forceinline__ Real lds(const Real *p) { return __ldcg(p); }
+#else
+template <class Real> __device__ __forceinline__ Real lds(const Real *p) { return __ldg(p); }
+#endif
 
 // Correctly rounded y / 6 without a division instruction sequence.  y/6 = (y/2)/3 with y/2 exact,
 // and x/3 by Markstein's correction (P. W. Markstein, "Computation of elementary functions on the
@@ -328,7 +338,7 @@ __device__ __forceinline__ void store(const StageArgs<Real> &p, long long at, Re
 // ADE memory update of one slot value (same scheme as the fields).
 template <class Real, int STAGE>
 __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long long at, Real rate, Partial &diag, bool withDiag) {
-    const Real u = ld(p.pbase + at);
+    const Real u = lds(p.pbase + at);
     if (STAGE == 0) {
         p.pacc[at] = rate;
         p.pout[at] = u + p.weight * rate;
@@ -338,7 +348,7 @@ __device__ __forceinline__ void combineMemory(const StageArgs<Real> &p, long lon
     } else {
         Real v;
         if constexpr (kahan<Real>()) {
-            const Real y = div6(p.delta * (p.pacc[at] + rate)) - p.pcin[at];
+            const Real y = div6(p.delta * (p.pacc[at] + rate)) - lds(p.pcin + at);
             v = u + y;
             p.pcout[at] = (v - u) - y;
         } else {
@@ -386,7 +396,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
     vxs[0] = xv[0], vxs[1] = xv[1];
     Real prate[4] = {0, 0, 0, 0}; // ADE rates of the velocity-derivative memories: slot0 f0,f1, slot1 f0,f1
     if (CPML && slot0 >= 0)
-        for (int v = 0; v < 2; ++v) vxs[v] = stretch(prof0, ld(p.pin + slot0 + v), xv[v], prate[v]);
+        for (int v = 0; v < 2; ++v) vxs[v] = stretch(prof0, lds(p.pin + slot0 + v), xv[v], prate[v]);
     const Real lam = t.lam(m), mu = t.mu(m);
     if (depth == 0) { // surface eta-derivative from the traction-free condition (PointKernels2D.hpp:79-89)
         const Real c0 = a, c1 = b, c2 = c0 * c0 + c1 * c1, len = sqrt(c2);
@@ -396,8 +406,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
 #pragma unroll
         for (int l = 0; l < MECH; ++l) {
             const int mm = 6 + 4 * l;
-            tt[0] -= ld(w + mm * n + q) * c0 + ld(w + (mm + 2) * n + q) * c1;
-            tt[1] -= ld(w + (mm + 2) * n + q) * c0 + ld(w + (mm + 1) * n + q) * c1;
+            tt[0] -= lds(w + mm * n + q) * c0 + lds(w + (mm + 2) * n + q) * c1;
+            tt[1] -= lds(w + (mm + 2) * n + q) * c0 + lds(w + (mm + 1) * n + q) * c1;
         }
         const Real normal = tt[0] * nn[0] + tt[1] * nn[1];
         for (int v = 0; v < 2; ++v)
@@ -416,7 +426,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
         Real vz = ev[f];
-        if (CPML && slot1 >= 0) vz = stretch(prof1, ld(p.pin + slot1 + f), ev[f], prate[2 + f]);
+        if (CPML && slot1 >= 0) vz = stretch(prof1, lds(p.pin + slot1 + f), ev[f], prate[2 + f]);
         dxv[f] = vxs[f] + a * vz;
         dzv[f] = b * vz;
     }
@@ -433,7 +443,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         Real am[NM];
 #pragma unroll
         for (int j = 0; j < NM; ++j) am[j] = STAGE ? p.acc[(j < 4 * MECH ? 6 + j : 5) * n + q] : Real(0);
-        const Real w5 = damped ? ld(w + 5 * n + q) : Real(0);
+        const Real w5 = damped ? lds(w + 5 * n + q) : Real(0);
         Real r5 = lam * div;
 #pragma unroll
         for (int l = 0; l < MECH; ++l) {
@@ -442,7 +452,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
             const Real drive[4] = {dl * div + 2 * ds * dxv[0], dl * div + 2 * ds * dzv[1], ds * (dzv[0] + dxv[1]), dl * div};
             Real wm[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) wm[f] = ld(w + (mm + f) * n + q);
+            for (int f = 0; f < 4; ++f) wm[f] = lds(w + (mm + f) * n + q);
             r2 -= wm[0];
             r3 -= wm[1];
             r4 -= wm[2];
@@ -453,7 +463,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 if (damped) rm -= damp * wm[f];
                 const long long at = (mm + f) * n + q;
                 Real an;
-                const Real o = combine<Real, STAGE>(p, am[4 * l + f], ld(p.base + at), rm, KAHAN3 ? ld(p.cin + at) : Real(0), an);
+                const Real o = combine<Real, STAGE>(p, am[4 * l + f], lds(p.base + at), rm, KAHAN3 ? lds(p.cin + at) : Real(0), an);
                 store<Real, STAGE>(p, at, o, an);
                 if (withDiag && !isfinite(o)) diag.bad = 1;
             }
@@ -461,7 +471,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         if (damped) r5 -= damp * w5;
         const long long at = 5 * n + q;
         Real an;
-        const Real o = combine<Real, STAGE>(p, am[NM - 1], ld(p.base + at), r5, KAHAN3 ? ld(p.cin + at) : Real(0), an);
+        const Real o = combine<Real, STAGE>(p, am[NM - 1], lds(p.base + at), r5, KAHAN3 ? lds(p.cin + at) : Real(0), an);
         store<Real, STAGE>(p, at, o, an);
         if (withDiag && !isfinite(o)) diag.bad = 1;
     }
@@ -522,8 +532,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 X = tdrp<Real, DX>(t, m, f, 0) / rho;
                 Z = (a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1)) / rho;
             }
-            if (slot0 >= 0) X = stretch(prof0, ld(p.pin + slot0 + 2 + v), X, mrate[v]);
-            if (slot1 >= 0) Z = stretch(prof1, ld(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
+            if (slot0 >= 0) X = stretch(prof0, lds(p.pin + slot0 + 2 + v), X, mrate[v]);
+            if (slot1 >= 0) Z = stretch(prof1, lds(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
             rv[v] = X + Z;
         }
         r0 = rv[0], r1 = rv[1];
@@ -649,15 +659,22 @@ template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<R
     return !(pml || surface || source || sponge);
 }
 
+// Tile (bx, by) of the stage grid; its diagnostics go to partial `slot`.  `reinit`: the
+// mbarriers were used by an earlier tile of this CTA (every copy of which has landed) and are
+// invalidated before they are initialised again.  Returns false when a copy wait ran out.
+__device__ __forceinline__ void mbarInval(uint64_t *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smemAddr(bar)) : "memory");
+}
 template <class Real, int DX, int DZ, int MECH, int STAGE, bool EXACT, bool FULL>
-__device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw) {
+__device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw, int bx, int by, int slot,
+                                           bool reinit) {
     constexpr int T = STREAM_THREADS, PW = pwWords<Real>();
     constexpr unsigned S = sizeof(Real);
     constexpr unsigned chunkBytes = S * CH, fiveBytes = S * 5 * T, modelBytes = S * (STAGE == 3 ? 6 : 5) * T;
     constexpr unsigned wordBytes = (STAGE > 0 ? 2 * fiveBytes : 0) + modelBytes + (STAGE == 3 && kahan<Real>() ? fiveBytes : 0);
     const Mesh<Real> &m = p.m;
     const int lane = threadIdx.x, wy = threadIdx.y, tid = lane + SW * wy;
-    const int i0 = 3 + blockIdx.x * SW, z0 = 3 + blockIdx.y * (SB * m.seg), zb = z0 - 3;
+    const int i0 = 3 + bx * SW, z0 = 3 + by * (SB * m.seg), zb = z0 - 3;
     const int iEnd = m.nx - 3, kEnd = m.nz - 3;
     const int blocks = min(m.seg, (kEnd - z0 + SB - 1) / SB);
     __shared__ int stop;
@@ -678,6 +695,7 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
     };
     if (tid == 0) {
         stop = 0;
+        if (reinit) mbarInval(bar), mbarInval(bar + 1);
         mbarInit(bar, 1);
         mbarInit(bar + 1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -715,9 +733,28 @@ __device__ __forceinline__ void streamBody(const StageArgs<Real> &p, uint64_t *b
             const int issued = min(blocks, waited + 2);
             for (int g = waited; g < issued; ++g) mbarWait(bar + (g & 1), (g >> 1) & 1);
         }
-        return;
+        return false;
     }
-    if (withDiag) reducePartial(diag, p.partials, blockIdx.x + gridDim.x * blockIdx.y);
+    if (withDiag) reducePartial(diag, p.partials, slot);
+    return true;
+}
+
+// One tile of one stage in the form its position calls for: the interior form away from the
+// boundaries, the general form elsewhere; x/h by a product or the correctly rounded quotient.
+template <class Real, int DX, int DZ, int MECH, int STAGE>
+__device__ __forceinline__ bool streamTile(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw, int bx, int by, int slot,
+                                           bool reinit) {
+    const bool interior = interiorBlock(p.m, 3 + bx * SW, 3 + by * (SB * p.m.seg));
+    if constexpr (sizeof(Real) == 4) {
+        if (interior) return streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw, bx, by, slot, reinit);
+        return streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw, bx, by, slot, reinit);
+    } else if (p.m.hinvExact) {
+        if (interior) return streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw, bx, by, slot, reinit);
+        return streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw, bx, by, slot, reinit);
+    } else {
+        if (interior) return streamBody<Real, DX, DZ, MECH, STAGE, false, false>(p, bar, ring, pw, bx, by, slot, reinit);
+        return streamBody<Real, DX, DZ, MECH, STAGE, false, true>(p, bar, ring, pw, bx, by, slot, reinit);
+    }
 }
 
 // The streaming stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.  DX/DZ:
@@ -730,17 +767,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream
     uint64_t *bar = reinterpret_cast<uint64_t *>(base);
     Real *ring = reinterpret_cast<Real *>(base + 128);
     Real *pw = ring + CHUNKS * CH;
-    const bool interior = interiorBlock(p.m, 3 + blockIdx.x * SW, 3 + blockIdx.y * (SB * p.m.seg));
-    if constexpr (sizeof(Real) == 4) {
-        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw);
-    } else if (p.m.hinvExact) {
-        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, true, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, MECH, STAGE, true, true>(p, bar, ring, pw);
-    } else {
-        if (interior) streamBody<Real, DX, DZ, MECH, STAGE, false, false>(p, bar, ring, pw);
-        else streamBody<Real, DX, DZ, MECH, STAGE, false, true>(p, bar, ring, pw);
-    }
+    streamTile<Real, DX, DZ, MECH, STAGE>(p, bar, ring, pw, blockIdx.x, blockIdx.y, blockIdx.x + gridDim.x * blockIdx.y, false);
 }
 
 // ---------------------------------------------------------------- diagnostics ------------
