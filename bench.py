@@ -321,7 +321,8 @@ def serving_leg(args, device: int) -> dict:
             w.close()
     # batched FP32
     srv = V.Server(device=device, batch_steps=args.serving_batch, max_active=args.serving_active,
-                   build_threads=max(2, min(8, (os.cpu_count() or 4) // 2)), scheduler_threads=args.serving_schedulers)
+                   build_threads=max(2, min(8, (os.cpu_count() or 4) // 2)), scheduler_threads=args.serving_schedulers,
+                   persistent=bool(args.serving_persistent), persistent_ctas=args.serving_persistent_ctas)
     util = UtilSampler(device).start()
     t0 = time.perf_counter()
     ids = []
@@ -368,7 +369,8 @@ def serving_leg(args, device: int) -> dict:
     batched = {"shots_per_hour": len(reqs) / span32 * 3600, "p50_s": float(np.percentile(lat32, 50)),
                "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32, "peak_running": stats["peak_running"],
                "failed": failed, "mean_build_s": float(build32.mean()), "mean_run_s": float(gpu32.mean()),
-               "gpu_util_pct": util32, "scheduler_threads": args.serving_schedulers, "max_active": args.serving_active}
+               "gpu_util_pct": util32, "scheduler_threads": args.serving_schedulers, "max_active": args.serving_active,
+               "persistent_2d": bool(args.serving_persistent), "persistent_ctas_per_sm": args.serving_persistent_ctas}
     if args.serving_batched_only:
         return {"requests": len(reqs), "batched_fp32": batched}
     service, rec64, init64, util64, kinds64 = sequential(0)
@@ -398,6 +400,59 @@ def serving_leg(args, device: int) -> dict:
         "shots_per_hour_ratio": (shots / span32) / (shots / span64),
         "max_trace_rel_l2_fp32_vs_fp64": max(errs), "median_trace_rel_l2_fp32_vs_fp64": float(np.median(errs)),
     }
+
+
+def persistent_leg(args, device: int) -> dict:
+    """Throughput of the persistent multi-shot launch (swl2d_queue_launch) against the same shots'
+    own batches running concurrently on their own streams: FP32 2D shots of the serving mix, 64
+    steps per round, unforced (scale 0; the arithmetic and traffic do not depend on the values)."""
+    import ctypes as C
+    import importlib
+    swl = load_package()
+    W = importlib.import_module("swl_b200.workloads")
+    S = importlib.import_module("swl_b200.session")
+    reqs = [r for r in W.serving_mix(n=4 * args.persistent_shots, rate=100.0, seed=5, scale=args.serving_scale,
+                                     steps_scale=args.serving_steps) if r["dim"] == 2]
+    out = {"steps_per_round": 64, "rounds": 3, "unit": "Mpt-updates/s"}
+    for label, gsls in (("elastic", False), ("gsls3", True)):
+        group = [r for r in reqs if bool(r["params"].get("attenuation")) == gsls][:args.persistent_shots]
+        sims = [S.Simulation2D(dict(r["params"], precision=1, segmentRule=1), device=device) for r in group]
+        engs = []
+        for sm in sims:
+            e = swl.Engine2D.__new__(swl.Engine2D)
+            e._h = C.c_void_p(sm.engine_handle())
+            engs.append(e)
+        info = [sm.info() for sm in sims]
+        nodes = sum((i["nx"] - 6) * (i["nz"] - 6) for i in info)
+        dts, freqs = [i["dt"] for i in info], [r["params"]["frequency"] for r in group]
+        q = swl.Queue2D(1, device)
+
+        def streams(first):
+            for e, d, f in zip(engs, dts, freqs):
+                e.launch(first, 64, d, f, 0.0)
+            for e in engs:
+                e.wait()
+
+        def queued(first):
+            q.launch(engs, first, 64, dts, freqs, 0.0)
+            q.wait()
+            for e in engs:
+                e.wait()
+
+        res = {"shots": len(engs), "nodes": nodes}
+        for name, fn in (("own_streams", streams), ("persistent", queued)):
+            fn(0)  # warm-up (module load, tables)
+            t = time.perf_counter()
+            for k in range(3):
+                fn(64 * (k + 1))
+            res[name] = nodes * 64 * 3 / (time.perf_counter() - t) / 1e6
+        res["ratio"] = res["persistent"] / res["own_streams"]
+        out[label] = res
+        q.close()
+        for e in engs:
+            e._h = C.c_void_p()  # the sessions own the engines
+        del sims
+    return out
 
 
 def gpu_arm(args):
@@ -476,6 +531,8 @@ def gpu_arm(args):
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = serving_leg(args, local)
+        if args.persistent_shots > 0:
+            serving["persistent_launch"] = persistent_leg(args, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -537,6 +594,12 @@ def main():
     ap.add_argument("--ref-gpu-steps", type=int, default=10, help="timed steps of the reference CUDA engine")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=48, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--persistent-shots", type=int, default=24,
+                    help="FP32 2D shots per group in the persistent-launch vs own-stream comparison (0: skip)")
+    ap.add_argument("--serving-persistent", type=int, default=0,
+                    help="1: the 2D shots of the batched form advance together in one persistent launch per round")
+    ap.add_argument("--serving-persistent-ctas", type=int, default=-1,
+                    help="resident CTAs per SM of a persistent launch (0 all, n>0 at most n, n<0 all but -n)")
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")
     ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
     ap.add_argument("--serving-batch", type=int, default=64, help="steps per batch of a served shot")

@@ -132,6 +132,13 @@ void swl2d_queue_destroy(swl2d_queue *queue);
 swl_status swl2d_queue_launch(swl2d_queue *queue, swl2d_engine *const *engines, int32_t n, const int32_t *first,
                               const int32_t *count, const double *dt, const double *frequency, const double *scale,
                               const double *check_growth_after);
+/* Resident CTAs per SM the queue's launches may use: 0 all that fit (default); n > 0 at most n;
+ * n < 0 all but -n (at least one), which leaves room for other kernels beside the launch. */
+swl_status swl2d_queue_limit(swl2d_queue *queue, int32_t ctas_per_sm);
+/* Row blocks of 8 rows per work item (1, 2, 4 or 8), or 0 (default): per grid, the longest that
+ * still cuts it into at least 64 items per stage.  Either way a shot's decomposition depends on
+ * its grid only, never on the other shots of a launch. */
+swl_status swl2d_queue_segment(swl2d_queue *queue, int32_t segment);
 swl_status swl2d_queue_query(swl2d_queue *queue, int32_t *done);
 swl_status swl2d_queue_wait(swl2d_queue *queue);
 

@@ -29,6 +29,14 @@ typedef struct swl_server_config {
     int32_t build_threads; /* host threads building models (default 4) */
     int32_t scheduler_threads; /* host threads driving the running shots' batches (default 4); each
                                 * owns the shots it started: polls, records and relaunches them */
+    int32_t persistent;        /* 1: the 2D shots of one precision and GSLS mechanism count advance
+                                * together, one batch each, in ONE persistent launch per round
+                                * (swl2d_queue_launch), driven by one host thread; 0: each shot runs
+                                * its own batches on its own stream.  3D shots always run on their
+                                * own streams. */
+    int32_t persistent_ctas;   /* resident CTAs per SM of a persistent launch (swl2d_queue_limit);
+                                * default -1: all but one, leaving room for the 3D shots' kernels and
+                                * the engine builds beside it */
 } swl_server_config;
 
 enum { SWL_SHOT_QUEUED = 0, SWL_SHOT_BUILDING = 1, SWL_SHOT_RUNNING = 2, SWL_SHOT_DONE = 3, SWL_SHOT_FAILED = 4 };

@@ -150,6 +150,8 @@ def library() -> C.CDLL:
                                      C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.swl2d_queue_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+    L.swl2d_queue_limit.argtypes = [C.c_void_p, C.c_int32]
+    L.swl2d_queue_segment.argtypes = [C.c_void_p, C.c_int32]
     L.swl2d_queue_wait.argtypes = [C.c_void_p]
     L.swl3d_launch.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double]
     L.swl3d_query.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
@@ -199,6 +201,14 @@ class Queue2D:
         _check(library().swl2d_queue_launch(self._h, hs, n, vec(first, C.c_int32), vec(count, C.c_int32),
                                             vec(dt, C.c_double), vec(frequency, C.c_double), vec(scale, C.c_double),
                                             vec(growth_after, C.c_double, np.inf)))
+
+    def limit(self, ctas_per_sm: int):
+        """Resident CTAs per SM of later launches (0 all, n > 0 at most n, n < 0 all but -n)."""
+        _check(library().swl2d_queue_limit(self._h, int(ctas_per_sm)))
+
+    def segment(self, seg: int):
+        """Row blocks per work item (1, 2, 4, 8), or 0: chosen per grid."""
+        _check(library().swl2d_queue_segment(self._h, int(seg)))
 
     def query(self) -> bool:
         done = C.c_int32()

@@ -186,6 +186,18 @@ swl_status swl2d_queue_launch(swl2d_queue *q, swl2d_engine *const *engines, int3
         q->impl->launch(e.data(), n, f.data(), c.data(), dt, frequency, scale, growthAfter);
     });
 }
+swl_status swl2d_queue_limit(swl2d_queue *q, int32_t ctasPerSm) {
+    return guarded([&] {
+        need(q, "queue");
+        q->impl->limit(ctasPerSm);
+    });
+}
+swl_status swl2d_queue_segment(swl2d_queue *q, int32_t segment) {
+    return guarded([&] {
+        need(q, "queue");
+        q->impl->segment(segment);
+    });
+}
 swl_status swl2d_queue_query(swl2d_queue *q, int32_t *done) {
     return guarded([&] {
         need(q, "queue"), need(done, "done");

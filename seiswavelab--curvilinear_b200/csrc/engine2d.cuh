@@ -73,6 +73,11 @@ class Queue2D {
     virtual bool query() = 0; // true once the launch completed; throws if a wait in it ran out
     virtual void finish() = 0;
     virtual int blocks() const = 0; // CTAs of the last launch
+    // Resident CTAs per SM a launch may use: 0 all that fit; n > 0 at most n; n < 0 all but -n
+    // (at least one), leaving room for other shots' kernels beside the persistent launch.
+    virtual void limit(int ctasPerSm) = 0;
+    // Row blocks per work item (1, 2, 4 or 8), or 0: chosen per grid (queueSegment).
+    virtual void segment(int seg) = 0;
 };
 std::unique_ptr<Queue2D> makeQueue2D64(int device);
 std::unique_ptr<Queue2D> makeQueue2D32(int device);
@@ -698,10 +703,25 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     int mechanisms() const { return mech_; }
     int deviceId() const { return device_; }
     cudaStream_t stream() const { return stream_; }
-    long long tiles() const { return (long long)stageGrid_.x * stageGrid_.y; }
     // The clock and forcing tables of `count` steps from `first`, enqueued on the engine's stream,
     // and the kernel's description of the batch.
-    void queueBegin(int first, int count, double dt, double frequency, double scale, double growthAfter, k2::QueueShot<Real> &shot) {
+    // Row blocks per work item of a queued batch when the queue leaves it to the grid: the longest
+    // segment that still cuts the grid into at least 64 items per stage.  Long items amortise the
+    // ticket, wait and fences of an item (measured: full 64-row segments run a launch of 24 shots
+    // fastest); a tiny grid still gets enough items to spread over the SMs.  It depends on the grid
+    // only, never on the other shots of a launch.
+    int queueSegment() const {
+        const int qx = (nx_ - 6 + k2::SW - 1) / k2::SW;
+        int seg = k2::MAX_SEG;
+        while (seg > 1 && (long long)qx * ((nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg)) < 64) seg /= 2;
+        return seg;
+    }
+    long long queueTiles(int qseg) const {
+        if (qseg <= 0) qseg = queueSegment();
+        return (long long)((nx_ - 6 + k2::SW - 1) / k2::SW) * ((nz_ - 6 + k2::SB * qseg - 1) / (k2::SB * qseg));
+    }
+    void queueBegin(int first, int count, double dt, double frequency, double scale, double growthAfter, int qseg,
+                    k2::QueueShot<Real> &shot) {
         DeviceScope scope(device_);
         if (inflight_) throw Error(SWL_ERR_STATE, "a batch is already in flight on this engine");
         if (faulted_) throw Error(SWL_ERR_STATE, "2D engine holds a rejected step; reset or rebuild it");
@@ -717,13 +737,16 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         hostClock_.growth_after = growthAfter;
         pushClock();
         fillForcing(first, count, dt, frequency, scale);
+        // The queued form cuts the grid into work items of `qseg` row blocks (0: queueSegment()).
+        if (qseg <= 0) qseg = queueSegment();
         const int su = u_, sa = a_;
         for (int r = 0; r < 2; ++r) {
             u_ = r, a_ = 1 - r;
-            for (int k = 0; k < 4; ++k) shot.stage[r][k] = args(k);
+            for (int k = 0; k < 4; ++k) shot.stage[r][k] = args(k), shot.stage[r][k].m.seg = qseg;
             shot.stage[r][3].partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
         }
         u_ = su, a_ = sa;
+        const int qx = (nx_ - 6 + k2::SW - 1) / k2::SW, qy = (nz_ - 6 + k2::SB * qseg - 1) / (k2::SB * qseg);
         shot.partials = partials_.as<k2::Partial>();
         shot.receivers = recIdx_.as<long long>();
         shot.traces = traces_.as<double>();
@@ -731,8 +754,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         shot.sets[0] = set_[0], shot.sets[1] = set_[1];
         shot.count = count_;
         shot.nrec = nrec_;
-        shot.tiles = int(tiles());
-        shot.tilesX = int(stageGrid_.x);
+        shot.tiles = qx * qy; // the partials buffer holds at least one per one-block segment
+        shot.tilesX = qx;
         shot.u0 = u_;
         shot.steps = count;
         shot.first = first;
@@ -899,7 +922,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
 // (clock, forcing) and read-backs (traces, clock) stay on the engine's stream, ordered with the
 // kernel by events, so an engine outlives the queue and keeps working on its own afterwards.
 template <class Real> class TypedQueue2D final : public Queue2D {
-    int device_{}, sms_{}, blocks_{};
+    int device_{}, sms_{}, blocks_{}, limit_{0}, seg_{0};
     cudaStream_t stream_{};
     cudaEvent_t done_{}, kernel_{};
     DeviceBuffer dev_;
@@ -937,11 +960,17 @@ template <class Real> class TypedQueue2D final : public Queue2D {
         if (stream_) cudaStreamSynchronize(stream_), cudaStreamDestroy(stream_);
     }
     int blocks() const override { return blocks_; }
+    void limit(int ctasPerSm) override { limit_ = ctasPerSm; }
+    void segment(int seg) override {
+        if (seg != 0 && seg != 1 && seg != 2 && seg != 4 && seg != 8) throw Error(SWL_ERR_INVALID, "queue segment must be 0, 1, 2, 4 or 8");
+        seg_ = seg;
+    }
     void launch(Engine2D *const *engines, int n, const int *first, const int *count, const double *dt, const double *frequency,
                 const double *scale, const double *growthAfter) override {
         DeviceScope scope(device_);
         if (inflight_) throw Error(SWL_ERR_STATE, "a queued launch is already in flight");
         if (n <= 0) return;
+        if (n > k2::kQueueMaxShots) throw Error(SWL_ERR_INVALID, "a queued launch takes at most 256 engines");
         std::vector<TypedEngine2D<Real> *> e(n);
         for (int i = 0; i < n; ++i) {
             e[i] = dynamic_cast<TypedEngine2D<Real> *>(engines[i]);
@@ -960,7 +989,10 @@ template <class Real> class TypedQueue2D final : public Queue2D {
         const int maxSteps = count[order[0]];
         const std::size_t oShots = up(sizeof(k2::QueueHeader)), oDone = oShots + up(sizeof(k2::QueueShot<Real>) * n);
         const std::size_t oStart = oDone + up(sizeof(int) * n), oActive = oStart + up(sizeof(long long) * (maxSteps + 1));
-        const std::size_t oPrefix = oActive + up(sizeof(int) * maxSteps), oAbort = oPrefix + up(sizeof(long long) * (n + 1));
+        long long allTiles = 0;
+        for (int i = 0; i < n; ++i) allTiles += e[i]->queueTiles(seg_);
+        const std::size_t oPrefix = oActive + up(sizeof(int) * maxSteps), oProgress = oPrefix + up(sizeof(long long) * (n + 1));
+        const std::size_t oAbort = oProgress + up(sizeof(int) * std::size_t(allTiles));
         const std::size_t bytes = oAbort + 64;
         if (dev_.bytes < bytes) dev_.allocate(bytes);
         host_.reserve(bytes);
@@ -971,7 +1003,7 @@ template <class Real> class TypedQueue2D final : public Queue2D {
         for (int s = 0; s < n; ++s) {
             const int i = order[s];
             new (shots + s) k2::QueueShot<Real>{};
-            e[i]->queueBegin(first[i], count[i], dt[i], frequency[i], scale[i], growthAfter[i], shots[s]);
+            e[i]->queueBegin(first[i], count[i], dt[i], frequency[i], scale[i], growthAfter[i], seg_, shots[s]);
             check(cudaStreamWaitEvent(stream_, e[i]->queueReady(), 0), "order the queued launch after the uploads");
         }
         auto *prefix = reinterpret_cast<long long *>(hb + oPrefix);
@@ -990,12 +1022,16 @@ template <class Real> class TypedQueue2D final : public Queue2D {
         h->nshots = n;
         h->maxSteps = maxSteps;
         h->done = reinterpret_cast<int *>(db + oDone);
+        h->progress = reinterpret_cast<int *>(db + oProgress);
+        if (prefix[n] != allTiles) throw Error(SWL_ERR_STATE, "queued tile count mismatch");
         h->stepStart = reinterpret_cast<const long long *>(db + oStart);
         h->active = reinterpret_cast<const int *>(db + oActive);
         h->tilePrefix = reinterpret_cast<const long long *>(db + oPrefix);
         check(cudaMemcpyAsync(dev_.ptr, host_.ptr, oAbort, cudaMemcpyHostToDevice, stream_), "upload queue");
         const int mech = e[0]->mechanisms();
-        blocks_ = int(std::min<long long>((long long)occupancy(mech) * sms_, (long long)h->total));
+        const int occ = occupancy(mech);
+        const int perSm = limit_ > 0 ? std::min(limit_, occ) : limit_ < 0 ? std::max(1, occ + limit_) : occ;
+        blocks_ = int(std::min<long long>((long long)perSm * sms_, (long long)h->total));
         run(mech, blocks_, reinterpret_cast<k2::QueueHeader *>(db), reinterpret_cast<const k2::QueueShot<Real> *>(db + oShots));
         check(cudaEventRecord(kernel_, stream_), "record queued launch");
         for (int i = 0; i < n; ++i) e[i]->queueEnd(count[i], kernel_);

@@ -1,7 +1,11 @@
 // Serving request loop (include/swl_server.h): admission by device-memory budget, model builds
-// on a host thread pool, and one scheduler thread that keeps a batch in flight on every running
+// on a host thread pool, and scheduler threads that keep a batch in flight on every running
 // shot.  Each shot owns its engine and CUDA stream, so batches of different shots overlap on
-// the GPU.  Finished shots release their device memory at once, which admits the next request.
+// the GPU.  In the persistent form the 2D shots instead advance together: one host thread
+// gathers the running 2D shots of each (precision, GSLS mechanism count) into one persistent
+// multi-shot launch per round, admits new shots at the next round, and records each shot's batch
+// when the launch completes.  Finished shots release their device memory at once, which admits
+// the next request.
 #include "../../../include/swl_server.h"
 #include "sessions.hpp"
 #include <atomic>
@@ -71,6 +75,7 @@ class Server {
         }
         for (int t = 0; t < cfg_.build_threads; ++t) builders_.emplace_back([this] { buildLoop(); });
         for (int t = 0; t < cfg_.scheduler_threads; ++t) loops_.emplace_back([this] { schedule(); });
+        if (cfg_.persistent) loops_.emplace_back([this] { queueLoop(); });
         reaper_ = std::thread([this] { reapLoop(); });
     }
     ~Server() {
@@ -162,7 +167,7 @@ class Server {
     std::deque<std::shared_ptr<Shot>> reap_; // finished shots whose engines are still to be destroyed
     std::thread reaper_;
     std::deque<int64_t> queue_, unreported_;
-    std::deque<std::shared_ptr<Shot>> toBuild_, built_;
+    std::deque<std::shared_ptr<Shot>> toBuild_, built_, built2d_; // built2d_: 2D shots for the persistent form
     std::map<int64_t, std::shared_ptr<Shot>> shots_;
     int64_t nextId_{}, finished_{}, building_{};
     int running_{}, peakRunning_{};
@@ -225,7 +230,7 @@ class Server {
                 used_ += actual - s->bytes;
                 s->bytes = actual;
                 peakUsed_ = std::max(peakUsed_, used_);
-                built_.push_back(s);
+                (cfg_.persistent && s->dim == 2 ? built2d_ : built_).push_back(s);
                 cvWork_.notify_all();
             }
         }
@@ -345,6 +350,121 @@ class Server {
             if (s->s3 && s->s3->engine) swl3d_destroy(s->s3->engine), s->s3->engine = nullptr;
         }
     }
+    // The persistent form's thread: rounds of one multi-shot launch per (precision, mechanisms).
+    struct Group {
+        swl2d_queue *queue{};
+        std::vector<std::shared_ptr<Shot>> shots; // the shots of the launch in flight
+        bool inflight{false};
+    };
+    void finishRunning(const std::shared_ptr<Shot> &s, const std::string &error) {
+        std::lock_guard<std::mutex> g(mu_);
+        --running_;
+        finishShot(s, error.empty() ? SWL_SHOT_DONE : SWL_SHOT_FAILED, error, false);
+        reap_.push_back(s);
+        cvReap_.notify_one();
+    }
+    void queueLoop() {
+        std::map<std::pair<int, int>, Group> groups;
+        std::vector<std::shared_ptr<Shot>> running;
+        std::map<int64_t, std::string> failed; // shots whose launch went wrong
+        const auto kindOf = [](const Shot &s) { return std::make_pair(s.s2->params.precision, s.s2->model.mechanisms); };
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                if (stop_) break;
+                while (!built2d_.empty()) {
+                    built2d_.front()->state = SWL_SHOT_RUNNING;
+                    built2d_.front()->run = now();
+                    running.push_back(built2d_.front());
+                    built2d_.pop_front();
+                    ++running_;
+                }
+                peakRunning_ = std::max(peakRunning_, running_);
+                admit(running_);
+            }
+            bool progressed = false;
+            for (auto &[kind, grp] : groups) { // completed launches: record each shot's batch
+                if (!grp.inflight) continue;
+                int32_t done = 0;
+                const swl_status st = swl2d_queue_query(grp.queue, &done);
+                const std::string why = st == SWL_OK ? std::string() : std::string(swl_last_error());
+                if (st == SWL_OK && !done) continue;
+                if (st != SWL_OK) swl2d_queue_wait(grp.queue); // settle the launch
+                for (auto &s : grp.shots) {
+                    try {
+                        s->s2->pollBatch(true);
+                    } catch (const std::exception &e) {
+                        failed[s->id] = e.what();
+                    }
+                    if (!why.empty()) failed.emplace(s->id, why);
+                }
+                grp.shots.clear();
+                grp.inflight = false;
+                progressed = true;
+            }
+            for (std::size_t i = 0; i < running.size();) { // finished shots
+                auto &s = running[i];
+                const auto f = failed.find(s->id);
+                if (!s->s2->inflight && (f != failed.end() || s->s2->completed())) {
+                    finishRunning(s, f == failed.end() ? std::string() : f->second);
+                    if (f != failed.end()) failed.erase(f);
+                    running.erase(running.begin() + i);
+                    progressed = true;
+                    continue;
+                }
+                ++i;
+            }
+            std::map<std::pair<int, int>, std::vector<std::shared_ptr<Shot>>> ready;
+            for (auto &s : running)
+                if (!s->s2->inflight) ready[kindOf(*s)].push_back(s);
+            for (auto &[kind, shots] : ready) { // one launch per idle kind
+                Group &grp = groups[kind];
+                if (grp.inflight) continue;
+                if (!grp.queue && (swl2d_queue_create(device_, kind.first, &grp.queue) != SWL_OK ||
+                                   swl2d_queue_limit(grp.queue, cfg_.persistent_ctas) != SWL_OK)) {
+                    const std::string why = swl_last_error();
+                    for (auto &s : shots) failed[s->id] = why;
+                    progressed = true;
+                    continue;
+                }
+                std::vector<swl2d_engine *> engines;
+                std::vector<int32_t> first, count;
+                std::vector<double> dt, freq, scale, growth;
+                for (auto &s : shots) {
+                    int32_t f = 0;
+                    double d = 0, fr = 0, sc = 0, gr = 0;
+                    int n = 0;
+                    try {
+                        n = s->s2->queueBatch(cfg_.batch_steps, f, d, fr, sc, gr);
+                    } catch (const std::exception &e) {
+                        failed[s->id] = e.what();
+                    }
+                    if (n <= 0) continue;
+                    grp.shots.push_back(s);
+                    engines.push_back(s->s2->engine), first.push_back(f), count.push_back(n);
+                    dt.push_back(d), freq.push_back(fr), scale.push_back(sc), growth.push_back(gr);
+                }
+                if (engines.empty()) continue;
+                if (swl2d_queue_launch(grp.queue, engines.data(), int32_t(engines.size()), first.data(), count.data(), dt.data(),
+                                       freq.data(), scale.data(), growth.data()) != SWL_OK) {
+                    const std::string why = swl_last_error();
+                    for (auto &s : grp.shots) s->s2->inflight = 0, failed[s->id] = why;
+                    grp.shots.clear();
+                } else {
+                    grp.inflight = true;
+                }
+                progressed = true;
+            }
+            if (!progressed) {
+                std::unique_lock<std::mutex> g(mu_);
+                cvWork_.wait_for(g, std::chrono::microseconds(running.empty() ? 2000 : 100));
+            }
+        }
+        for (auto &[kind, grp] : groups) // abandoned on destruction: let the launches end first
+            if (grp.queue) swl2d_queue_wait(grp.queue), swl2d_queue_destroy(grp.queue);
+        for (auto &s : running)
+            if (s->s2 && s->s2->engine) swl2d_destroy(s->s2->engine), s->s2->engine = nullptr;
+    }
 };
 
 } // namespace swl::host
@@ -359,6 +479,8 @@ void swl_server_config_default(swl_server_config *c) {
     *c = swl_server_config{};
     c->device = -1, c->memory_budget = 0, c->max_active = 0, c->batch_steps = 64, c->build_threads = 4;
     c->scheduler_threads = 4;
+    c->persistent = 0;
+    c->persistent_ctas = -1;
 }
 swl_status swl_server_create(const swl_server_config *c, swl_server **out) {
     return swl::host::guard([&] {

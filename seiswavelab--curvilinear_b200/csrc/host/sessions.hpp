@@ -124,6 +124,18 @@ struct Session2D {
         inflight = n;
         return true;
     }
+    // The arguments of one batch that a persistent multi-shot launch will run (swl2d_queue_launch),
+    // at most n steps; the batch counts as in flight from here.  0: nothing to do.
+    int queueBatch(int n, int32_t &first, double &dt, double &frequency, double &scale, double &growthAfter) {
+        if (!engine) throw Failure(SWL_ERR_STATE, "Initialize the 2D model on a device first.");
+        if (!fault.empty()) throw Failure(SWL_ERR_STATE, fault);
+        n = std::max(0, std::min({n, model.total - step, maxBatch}));
+        if (n == 0) return 0;
+        batchStart = std::chrono::steady_clock::now();
+        first = step, dt = model.dt, frequency = params.frequency, scale = model.scale, growthAfter = 3 / params.frequency;
+        inflight = n;
+        return n;
+    }
     // Completion of the in-flight batch: records of the accepted steps (Simulation::Impl::sample),
     // and the sticky fault of a rejected step.  Returns false while the batch is still running.
     bool pollBatch(bool block) {

@@ -4,14 +4,16 @@
 // The work of a launch is a list of items in a fixed global order: for each step j of the
 // batch, for each phase (RK stages 0-3, then the verdict), for each shot still stepping at j
 // (shots sorted by batch length, longest first), the shot's stage tiles (or its one verdict
-// item).  A resident CTA takes the next item with an atomic ticket, waits until its shot has
-// finished every item of the previous phases (a per-shot counter), runs it -- a stage tile is
+// item).  A resident CTA takes the next item with an atomic ticket, waits until the items it
+// depends on have finished (per-tile counters for the 3x3 tiles of the previous stage; per-shot
+// counters for a verdict and for stage 0 after it), runs it -- a stage tile is
 // exactly the tile the per-shot stage kernel runs, a verdict is the per-shot verdict kernel's
 // reduction, acceptance rule, receiver record and clock advance -- and counts it done.  Items are
 // taken in order and an item only waits on items earlier in the order, all of which were taken
 // by CTAs that are running, so the queue always drains; every wait is bounded all the same, and
-// one that runs out stops the launch with an error word the host reports.  While one shot waits
-// at its stage barrier, the tiles of the other shots keep the SMs busy.
+// one that runs out stops the launch with an error word the host reports.  A tile starts its next
+// stage as soon as its neighbours finished theirs, so stages overlap within a shot, and the tiles
+// of the other shots keep the SMs busy while one shot waits at its verdict.
 #pragma once
 #include "stage2d.cuh"
 
@@ -36,6 +38,7 @@ struct QueueHeader {
     int abort;                    // 0 running; 1 a copy wait ran out; 2 a dependency wait ran out
     int nshots, maxSteps, pad;
     int *done;                    // [nshots] items finished per shot
+    int *progress;                // [tilePrefix[nshots]] stage items finished per tile (tilePrefix[s] + tile)
     const long long *stepStart;   // [maxSteps + 1] first item of step j
     const int *active;            // [maxSteps] shots stepping at step j (a prefix of the shot order)
     const long long *tilePrefix;  // [nshots + 1] stage tiles of the shots before shot s
@@ -150,9 +153,15 @@ __device__ __forceinline__ bool queueStage(const StageArgs<Real> &p, int stage, 
 
 // Bound of one dependency wait: far longer than any phase of any shot takes.
 constexpr unsigned long long kQueueWaitNs = 4000000000ull;
+// Shots per launch.
+constexpr int kQueueMaxShots = 256;
+
+// Resident CTAs per SM: the stage kernels' count.  (Two CTAs of the GSLS forms, which would keep
+// their values in registers, measured slower than three with a few hundred bytes of spills.)
+template <class Real, int MECH> constexpr int queueBlocks() { return streamBlocks<Real>(); }
 
 template <class Real, int MECH>
-__global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) queue2d(QueueHeader *hdr, const QueueShot<Real> *shots) {
+__global__ void __launch_bounds__(STREAM_THREADS, (queueBlocks<Real, MECH>())) queue2d(QueueHeader *hdr, const QueueShot<Real> *shots) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     unsigned char *base = smemRaw + ((128 - (smemAddr(smemRaw) & 127)) & 127);
     uint64_t *bar = reinterpret_cast<uint64_t *>(base);
@@ -160,7 +169,9 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) queue2
     Real *pw = ring + CHUNKS * CH;
     __shared__ unsigned long long item;
     __shared__ int go, ready;
+    __shared__ unsigned fenced[kQueueMaxShots * 8 / 32]; // tensor maps this CTA acquired: (shot, set, stage)
     const int tid = threadIdx.x + SW * threadIdx.y;
+    for (int w = tid; w < kQueueMaxShots * 8 / 32; w += STREAM_THREADS) fenced[w] = 0;
     bool used = false; // the mbarriers hold an earlier tile's (completed) phases
     for (;;) {
         if (tid == 0) {
@@ -198,33 +209,73 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) queue2
             s = int(o - 4 * perStage);
         }
         const QueueShot<Real> &q = shots[s];
-        // wait until the shot has finished every item of the earlier phases
-        if (tid == 0) {
-            const int need = j * (4 * q.tiles + 1) + phase * q.tiles;
-            ready = 1;
-            if (ldAcquire(hdr->done + s) < need) {
-                const unsigned long long t0 = globalTimer();
-                unsigned ns = 32;
-                for (;;) {
-                    __nanosleep(ns);
-                    ns = ns < 1024 ? 2 * ns : ns;
-                    if (ldAcquire(hdr->done + s) >= need) break;
-                    if (*(volatile int *)&hdr->abort) {
-                        ready = 0;
-                        break;
+        const int bx = int(tile % q.tilesX), by = int(tile / q.tilesX);
+        int *const prog = hdr->progress + __ldg(hdr->tilePrefix + s);
+        // Dependencies.  Stages 1-3 of a tile read the previous stage's output of the 3x3 tiles
+        // around it (the stencil halo is 4 columns and 3 rows, less than a tile) and overwrite
+        // what that stage read there, so they wait for those nine tiles only.  A verdict waits for
+        // every stage-3 tile of its step; stage 0 of a step waits for the previous verdict (the
+        // new state, the clock and a possible rejection), which covers everything before it.
+        if (tid < 32) {
+            int state = 1; // 1 ready, 0 stop
+            if (phase >= 1 && phase <= 3) {
+                const int need = 4 * j + phase;
+                const int tilesY = q.tiles / q.tilesX;
+                const int nx = bx + tid % 3 - 1, ny = by + tid / 3 - 1;
+                const bool mine = tid < 9 && nx >= 0 && nx < q.tilesX && ny >= 0 && ny < tilesY;
+                const int *flag = prog + (mine ? ny * q.tilesX + nx : 0);
+                if (!__all_sync(0xffffffffu, !mine || ldAcquire(flag) >= need)) {
+                    const unsigned long long t0 = globalTimer();
+                    unsigned ns = 32;
+                    for (;;) {
+                        __nanosleep(ns);
+                        ns = ns < 1024 ? 2 * ns : ns;
+                        if (__all_sync(0xffffffffu, !mine || ldAcquire(flag) >= need)) break;
+                        int stop = 0;
+                        if (tid == 0) {
+                            if (*(volatile int *)&hdr->abort) stop = 1;
+                            else if (globalTimer() - t0 > kQueueWaitNs) atomicCAS(&hdr->abort, 0, 2), stop = 1;
+                        }
+                        if (__shfl_sync(0xffffffffu, stop, 0)) {
+                            state = 0;
+                            break;
+                        }
                     }
-                    if (globalTimer() - t0 > kQueueWaitNs) {
-                        atomicCAS(&hdr->abort, 0, 2);
-                        ready = 0;
-                        break;
+                }
+            } else if (tid == 0) {
+                const int need = j * (4 * q.tiles + 1) + phase * q.tiles;
+                if (ldAcquire(hdr->done + s) < need) {
+                    const unsigned long long t0 = globalTimer();
+                    unsigned ns = 32;
+                    for (;;) {
+                        __nanosleep(ns);
+                        ns = ns < 1024 ? 2 * ns : ns;
+                        if (ldAcquire(hdr->done + s) >= need) break;
+                        if (*(volatile int *)&hdr->abort) {
+                            state = 0;
+                            break;
+                        }
+                        if (globalTimer() - t0 > kQueueWaitNs) {
+                            atomicCAS(&hdr->abort, 0, 2);
+                            state = 0;
+                            break;
+                        }
                     }
                 }
             }
+            if (tid == 0) ready = state;
+        }
+        if (tid == 0) {
+            asm volatile("fence.acq_rel.gpu;\n" ::: "memory"); // what the waiting lanes acquired, for the whole CTA
             fenceProxyAsync(); // the tensor copies below read what other CTAs wrote
-            if (phase < 4) {
-                const StageArgs<Real> &p = q.stage[(j & 1) ? 1 - q.u0 : q.u0][phase];
-                fenceTensorMap(&p.ringMap), fenceTensorMap(&p.uMap), fenceTensorMap(&p.aMap);
-                fenceTensorMap(&p.modelMap), fenceTensorMap(&p.compMap);
+            if (phase < 4) { // the maps of this (shot, set, stage), once per CTA and launch
+                const int set = (j & 1) ? 1 - q.u0 : q.u0, bit = (s * 2 + set) * 4 + phase;
+                if (!(fenced[bit >> 5] & (1u << (bit & 31)))) {
+                    const StageArgs<Real> &p = q.stage[set][phase];
+                    fenceTensorMap(&p.ringMap), fenceTensorMap(&p.uMap), fenceTensorMap(&p.aMap);
+                    fenceTensorMap(&p.modelMap), fenceTensorMap(&p.compMap);
+                    fenced[bit >> 5] |= 1u << (bit & 31);
+                }
             }
         }
         __syncthreads();
@@ -236,7 +287,6 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) queue2
             queueVerdict<Real>(q, q.sets[1 - r], reinterpret_cast<Partial *>(ring));
         } else if (!q.clock->faulted) {
             const StageArgs<Real> &p = q.stage[r][phase];
-            const int bx = int(tile % q.tilesX), by = int(tile / q.tilesX);
             const int dx = queueDirection(step, phase, 0), dz = queueDirection(step, phase, 1);
             if (dx == 0 && dz == 0) ok = queueStage<Real, MECH, 0, 0>(p, phase, bar, ring, pw, bx, by, int(tile), used);
             else if (dx == 0) ok = queueStage<Real, MECH, 0, 1>(p, phase, bar, ring, pw, bx, by, int(tile), used);
@@ -246,9 +296,9 @@ __global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) queue2
         }
         fenceProxyAsync(); // this item's writes, before they are published to later copies
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0) { // publish: the barrier orders the CTA's writes before these releases
             if (!ok) atomicCAS(&hdr->abort, 0, 1);
-            __threadfence();
+            if (phase < 4) redRelease(prog + tile, 1);
             redRelease(hdr->done + s, 1);
         }
     }

@@ -22,7 +22,8 @@ _dp = C.POINTER(C.c_double)
 
 class Config(C.Structure):
     _fields_ = [("device", C.c_int32), ("memory_budget", C.c_int64), ("max_active", C.c_int32),
-                ("batch_steps", C.c_int32), ("build_threads", C.c_int32), ("scheduler_threads", C.c_int32)]
+                ("batch_steps", C.c_int32), ("build_threads", C.c_int32), ("scheduler_threads", C.c_int32),
+                ("persistent", C.c_int32), ("persistent_ctas", C.c_int32)]
 
 
 class ShotStatus(C.Structure):
@@ -64,13 +65,16 @@ def _bind():
 
 class Server:
     def __init__(self, device: int = -1, memory_budget: int = 0, max_active: int = 0, batch_steps: int = 64,
-                 build_threads: int = 4, scheduler_threads: int = 4):
+                 build_threads: int = 4, scheduler_threads: int = 4, persistent: bool = False,
+                 persistent_ctas: int = -1):
         L = _bind()
         c = Config()
         L.swl_server_config_default(C.byref(c))
         c.device, c.memory_budget, c.max_active = device, int(memory_budget), int(max_active)
         c.batch_steps, c.build_threads = int(batch_steps), int(build_threads)
         c.scheduler_threads = int(scheduler_threads)
+        c.persistent = int(bool(persistent))
+        c.persistent_ctas = int(persistent_ctas)
         h = C.c_void_p()
         _check(L.swl_server_create(C.byref(c), C.byref(h)))
         self._h = h

@@ -44,10 +44,21 @@ def alone(S, dim, params):
     return sim.records()
 
 
-def test_each_result_is_the_same_alone_and_in_the_mix(mods):
+def alone_persistent(V, dim, params):
+    # the persistent form alone: the shot is the only one in its multi-shot launches
+    srv = V.Server(device=0, batch_steps=7, persistent=True)
+    sid = srv.submit(params, dim)
+    srv.drain()
+    out = srv.records(sid)
+    srv.close()
+    return out
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_each_result_is_the_same_alone_and_in_the_mix(persistent, mods):
     S, V = mods
     shots = mix()
-    srv = V.Server(device=0, batch_steps=7)
+    srv = V.Server(device=0, batch_steps=7, persistent=persistent)
     ids = [srv.submit(p, dim) for dim, p in shots]
     srv.drain()
     st = srv.stats()
@@ -55,7 +66,7 @@ def test_each_result_is_the_same_alone_and_in_the_mix(mods):
     assert st["peak_running"] >= 2  # shots really overlapped
     for (dim, p), sid in zip(shots, ids):
         got = srv.records(sid)
-        want = alone(S, dim, p)
+        want = alone_persistent(V, dim, p) if persistent and dim == 2 else alone(S, dim, p)
         assert len(got) == len(want)
         for g, w in zip(got, want):
             np.testing.assert_array_equal(g, w)
