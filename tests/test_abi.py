@@ -58,3 +58,14 @@ def test_null_arguments_are_rejected(swl):
     assert lib.swl2d_step(None, 0.0, 1e-3, 10.0, 1.0, 0) == swl.ERR_INVALID
     assert lib.swl3d_create(None, None, 0, -1, None) == swl.ERR_INVALID
     assert lib.swl2d_resident_bytes(None) == 0
+
+
+def test_queue_needs_a_device_and_valid_arguments(swl):
+    lib = swl.library()
+    h = C.c_void_p()
+    assert lib.swl2d_queue_create(-1, 7, C.byref(h)) == swl.ERR_INVALID  # precision
+    assert b"precision" in lib.swl_last_error()
+    assert lib.swl2d_queue_launch(None, None, 0, None, None, None, None, None, None) == swl.ERR_INVALID
+    assert lib.swl2d_queue_segment(None, 8) == swl.ERR_INVALID
+    if swl.device_count() == 0:  # no CPU fallback: a queue needs a device
+        assert lib.swl2d_queue_create(-1, swl.SWL_FP32, C.byref(h)) == swl.ERR_UNAVAILABLE
