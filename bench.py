@@ -322,7 +322,7 @@ def serving_leg(args, device: int) -> dict:
     # batched FP32
     srv = V.Server(device=device, batch_steps=args.serving_batch, max_active=args.serving_active,
                    build_threads=max(2, min(8, (os.cpu_count() or 4) // 2)), scheduler_threads=args.serving_schedulers,
-                   persistent=bool(args.serving_persistent), persistent_ctas=args.serving_persistent_ctas)
+                   persistent=args.serving_persistent, persistent_ctas=args.serving_persistent_ctas)
     util = UtilSampler(device).start()
     t0 = time.perf_counter()
     ids = []
@@ -370,7 +370,7 @@ def serving_leg(args, device: int) -> dict:
                "p99_s": float(np.percentile(lat32, 99)), "makespan_s": span32, "peak_running": stats["peak_running"],
                "failed": failed, "mean_build_s": float(build32.mean()), "mean_run_s": float(gpu32.mean()),
                "gpu_util_pct": util32, "scheduler_threads": args.serving_schedulers, "max_active": args.serving_active,
-               "persistent_2d": bool(args.serving_persistent), "persistent_ctas_per_sm": args.serving_persistent_ctas}
+               "persistent_2d": args.serving_persistent, "persistent_ctas_per_sm": args.serving_persistent_ctas}
     if args.serving_batched_only:
         return {"requests": len(reqs), "batched_fp32": batched}
     service, rec64, init64, util64, kinds64 = sequential(0)
@@ -531,8 +531,10 @@ def gpu_arm(args):
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = serving_leg(args, local)
-        if args.persistent_shots > 0:
-            serving["persistent_launch"] = persistent_leg(args, local)
+    persistent = None
+    if rank == 0 and world == 1 and args.persistent_shots > 0:
+        persistent = persistent_leg(args, local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -552,6 +554,8 @@ def gpu_arm(args):
             line["reference_gpu"] = ref_gpu
         if serving:
             line["serving"] = serving
+        if persistent:
+            line["persistent_launch"] = persistent
         line["profile_fp64"] = r64["profile"]
         print(json.dumps(line), flush=True)
     if dist:
@@ -597,7 +601,8 @@ def main():
     ap.add_argument("--persistent-shots", type=int, default=24,
                     help="FP32 2D shots per group in the persistent-launch vs own-stream comparison (0: skip)")
     ap.add_argument("--serving-persistent", type=int, default=0,
-                    help="1: the 2D shots of the batched form advance together in one persistent launch per round")
+                    help="1: the 2D shots of the batched form advance together in one persistent launch per round; "
+                         "2: the elastic 2D shots only; 0: every shot on its own stream")
     ap.add_argument("--serving-persistent-ctas", type=int, default=-1,
                     help="resident CTAs per SM of a persistent launch (0 all, n>0 at most n, n<0 all but -n)")
     ap.add_argument("--serving-scale", type=float, default=0.5, help="grid-edge scale of the serving mix")

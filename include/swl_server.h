@@ -31,9 +31,9 @@ typedef struct swl_server_config {
                                 * owns the shots it started: polls, records and relaunches them */
     int32_t persistent;        /* 1: the 2D shots of one precision and GSLS mechanism count advance
                                 * together, one batch each, in ONE persistent launch per round
-                                * (swl2d_queue_launch), driven by one host thread; 0: each shot runs
-                                * its own batches on its own stream.  3D shots always run on their
-                                * own streams. */
+                                * (swl2d_queue_launch), driven by one host thread; 2: the same for the
+                                * elastic 2D shots only; 0: each shot runs its own batches on its own
+                                * stream.  3D shots always run on their own streams. */
     int32_t persistent_ctas;   /* resident CTAs per SM of a persistent launch (swl2d_queue_limit);
                                 * default -1: all but one, leaving room for the 3D shots' kernels and
                                 * the engine builds beside it */

@@ -230,7 +230,8 @@ class Server {
                 used_ += actual - s->bytes;
                 s->bytes = actual;
                 peakUsed_ = std::max(peakUsed_, used_);
-                (cfg_.persistent && s->dim == 2 ? built2d_ : built_).push_back(s);
+                const bool queued = s->dim == 2 && (cfg_.persistent == 1 || (cfg_.persistent == 2 && s->s2->model.mechanisms == 0));
+                (queued ? built2d_ : built_).push_back(s);
                 cvWork_.notify_all();
             }
         }

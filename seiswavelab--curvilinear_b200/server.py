@@ -65,7 +65,7 @@ def _bind():
 
 class Server:
     def __init__(self, device: int = -1, memory_budget: int = 0, max_active: int = 0, batch_steps: int = 64,
-                 build_threads: int = 4, scheduler_threads: int = 4, persistent: bool = False,
+                 build_threads: int = 4, scheduler_threads: int = 4, persistent: int = 0,
                  persistent_ctas: int = -1):
         L = _bind()
         c = Config()
@@ -73,7 +73,7 @@ class Server:
         c.device, c.memory_budget, c.max_active = device, int(memory_budget), int(max_active)
         c.batch_steps, c.build_threads = int(batch_steps), int(build_threads)
         c.scheduler_threads = int(scheduler_threads)
-        c.persistent = int(bool(persistent))
+        c.persistent = int(persistent)
         c.persistent_ctas = int(persistent_ctas)
         h = C.c_void_p()
         _check(L.swl_server_create(C.byref(c), C.byref(h)))
