@@ -706,14 +706,15 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // The clock and forcing tables of `count` steps from `first`, enqueued on the engine's stream,
     // and the kernel's description of the batch.
     // Row blocks per work item of a queued batch when the queue leaves it to the grid: the longest
-    // segment that still cuts the grid into at least 64 items per stage.  Long items amortise the
+    // segment that still cuts the grid into at least kQueueItems items per stage.  Long items amortise the
     // ticket, wait and fences of an item (measured: full 64-row segments run a launch of 24 shots
     // fastest); a tiny grid still gets enough items to spread over the SMs.  It depends on the grid
     // only, never on the other shots of a launch.
+    static constexpr long long kQueueItems = 64; // 128 measured 0.85x / 1.00x of own streams for 8 / 24 shots, 64 gives 0.62x / 1.10x
     int queueSegment() const {
         const int qx = (nx_ - 6 + k2::SW - 1) / k2::SW;
         int seg = k2::MAX_SEG;
-        while (seg > 1 && (long long)qx * ((nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg)) < 64) seg /= 2;
+        while (seg > 1 && (long long)qx * ((nz_ - 6 + k2::SB * seg - 1) / (k2::SB * seg)) < kQueueItems) seg /= 2;
         return seg;
     }
     long long queueTiles(int qseg) const {
