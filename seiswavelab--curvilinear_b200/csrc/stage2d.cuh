@@ -179,9 +179,10 @@ template <class Real, bool EXACT, int STAGE> struct StreamNode {
     long long q;
     int centre;      // ring row (0..RING-1) of this node
     __device__ __forceinline__ Real at(int f, int dx, int dz) const {
-        int s = centre + dz;
+        int s = centre + dz; // dz in [-3, 3]: one wrap at most
         s = s < 0 ? s + RING : s >= RING ? s - RING : s;
-        return col[(s / SB) * CH + f * RF + (s % SB) * RC + dx];
+        const unsigned u = unsigned(s); // non-negative: the chunk and row are a shift and a mask
+        return col[(u / unsigned(SB)) * CH + f * RF + (u % unsigned(SB)) * RC + dx];
     }
     __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
     __device__ __forceinline__ Real u(const StageArgs<Real> &, int f) const { return STAGE == 0 ? at(f, 0, 0) : word(PW_U + f); }
