@@ -1,6 +1,6 @@
 // Instantiations of the persistent multi-shot 2D kernel for one precision (SWL_STAGE_REAL) and
 // one GSLS mechanism count (SWL_STAGE_MECH); build.py compiles this unit once per pair, with
-// SWL_STAGE_COHERENT (state written within the launch is read through L2, not the read-only path).
+// SWL_STAGE_COHERENT (state written within the launch is read by coherent loads, not the read-only path).
 #include "launchq2d.cuh"
 
 #ifndef SWL_STAGE_REAL

@@ -104,10 +104,11 @@ template <class Real> __device__ __forceinline__ Real ld(const Real *p) { return
 // Loads of state that the step itself writes (stage inputs, U, the ADE memories, the Kahan
 // terms).  A stage kernel only reads arrays that the previous launches wrote, so they may take
 // the read-only path; the persistent multi-shot kernel (queue2d.cuh) reads state that other CTAs
-// wrote in the same launch, which the read-only path may serve stale, so it is compiled with
-// SWL_STAGE_COHERENT and loads these words through L2.
+// wrote in the same launch, which the non-coherent read-only path may serve stale, so it is
+// compiled with SWL_STAGE_COHERENT and uses ordinary cached loads (ld.global.ca), which see those
+// writes after the acquire fence each work item starts with.
 #ifdef SWL_STAGE_COHERENT
-template <class Real> __device__ __forceinline__ Real lds(const Real *p) { return __ldcg(p); }
+template <class Real> __device__ __forceinline__ Real lds(const Real *p) { return __ldca(p); }
 #else
 template <class Real> __device__ __forceinline__ Real lds(const Real *p) { return __ldg(p); }
 #endif
