@@ -837,8 +837,18 @@ __global__ void __launch_bounds__(1024) verdict2d(const Partial *__restrict__ pa
                                                   double *__restrict__ traces, Clock *clk, int check) {
     __shared__ Partial sh[1024];
     __shared__ int accept;
+    // The clock's words are read once, in parallel, by the first warp: the rule and the record
+    // below then read shared memory instead of a chain of dependent global loads.
+    __shared__ union {
+        Clock c;
+        int w[sizeof(Clock) / sizeof(int)];
+    } snap;
+    static_assert(sizeof(Clock) % sizeof(int) == 0 && sizeof(Clock) / sizeof(int) <= 32, "Clock must fit one warp's loads");
     const int t = threadIdx.x;
-    if (clk->faulted) return;
+    if (t < int(sizeof(Clock) / sizeof(int))) snap.w[t] = reinterpret_cast<const int *>(clk)[t];
+    __syncthreads();
+    const Clock &c0 = snap.c;
+    if (c0.faulted) return;
     Partial s{0, 0, 0, 0, 0};
     if (check) {
         for (int b = t; b < nparts; b += blockDim.x) {
@@ -867,15 +877,15 @@ __global__ void __launch_bounds__(1024) verdict2d(const Partial *__restrict__ pa
         if (check) {
             const Partial tot = sh[0];
             const bool finite = !tot.bad && isfinite(tot.energy);
-            const bool growth = (clk->step + 1) * clk->dt > clk->growth_after && clk->peak_energy > 0 &&
-                                tot.energy > clk->peak_energy * 10000;
+            const bool growth = (c0.step + 1) * c0.dt > c0.growth_after && c0.peak_energy > 0 &&
+                                tot.energy > c0.peak_energy * 10000;
             ok = finite && !growth;
             clk->finite = finite;
             if (ok) {
                 clk->energy = tot.energy;
                 clk->max_velocity = tot.velocity;
                 clk->traction = tot.traction;
-                clk->peak_energy = fmax(clk->peak_energy, tot.energy);
+                clk->peak_energy = fmax(c0.peak_energy, tot.energy);
             }
         }
         accept = ok;
@@ -884,12 +894,12 @@ __global__ void __launch_bounds__(1024) verdict2d(const Partial *__restrict__ pa
     if (!accept) {
         if (t == 0) {
             clk->faulted = 1;
-            clk->fault_step = clk->step;
+            clk->fault_step = c0.step;
         }
         return;
     }
-    const int row = clk->step - clk->first;
-    if (row < clk->trace_steps)
+    const int row = c0.step - c0.first;
+    if (row < c0.trace_steps)
         for (int r = t; r < nrec; r += blockDim.x) {
             const long long qq = receivers[r];
             traces[((long long)row * nrec + r) * 2] = double(w[qq]);
@@ -897,8 +907,8 @@ __global__ void __launch_bounds__(1024) verdict2d(const Partial *__restrict__ pa
         }
     __syncthreads();
     if (t == 0) {
-        clk->step += 1;
-        clk->accepted += 1;
+        clk->step = c0.step + 1;
+        clk->accepted = c0.accepted + 1;
     }
 }
 
