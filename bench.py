@@ -174,24 +174,58 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def cpu_baseline(params: dict, dim: int, steps: int, warmup: int) -> dict | None:
-    """The reference's own CPU solver on a bounded sample of the same shot, all host threads."""
+def cpu_baseline(params: dict, dim: int, steps: int, warmup: int, keep: bool = False):
+    """The reference's own CPU solver on a bounded sample of the same shot, all host threads.
+    With `keep`, also returns the run's final fields and records (the reference's answer for
+    the same warmup + steps, against which the GPU path's error is reported)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     threads = min(64, os.cpu_count() or 1)
     run = O.run_reference_2d if dim == 2 else O.run_reference_3d
     ref = O.REF2D if dim == 2 else O.REF3D
     if not ref.exists():
-        return None
+        return (None, None) if keep else None
     p = dict(params)
     p["maxSteps"] = warmup + steps
     p["precision"] = 0
     r = run(p, steps=steps, threads=threads, dump_mesh=False, warmup=warmup)
     pts = float(np.prod([int(r[k]) - 6 for k in (("nx", "nz") if dim == 2 else ("nx", "ny", "nz"))]))
     sec = float(r["runMs"]) / 1e3
-    return {"value": pts * steps / sec / 1e6, "unit": UNIT, "cores": int(r["threads"]), "kind": "reference",
+    base = {"value": pts * steps / sec / 1e6, "unit": UNIT, "cores": int(r["threads"]), "kind": "reference",
             "sample": f"{steps} timed steps after {warmup} warm-up of the same shot (reference CPU solver, FP64, "
                       f"{int(r['threads'])} OpenMP threads); {float(r['msPerStep']):.1f} ms/step, init {float(r['initMs'])/1e3:.1f} s"}
+    return (base, r) if keep else base
+
+
+def error_vs_reference(S, params: dict, dim: int, ref: dict, device: int) -> dict:
+    """Trace and wavefield error of the GPU path against the reference CPU solver's own run of the
+    same shot and step count (the run the CPU baseline timed): FP64 plain and FP32 chosen form."""
+    steps = int(ref["steps"])
+    nfields = int(ref["fieldCount"]) if dim == 2 else 9
+    comps = ("Vx", "Vz") if dim == 2 else ("Vx", "Vy", "Vz")
+    R, Sm = int(ref["receivers"]), int(ref["samples"])
+    want_tr = [ref[f"traces{c}"].reshape(R, Sm) for c in comps]
+    want_f = [ref[f"field{f}"] for f in range(nfields)]
+
+    def rel(a, b):
+        den = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+    out = {"steps": steps, "reference": "reference CPU solver (oracle/_ref), FP64, same shot and steps"}
+    for prec, key in ((0, "fp64"), (1, "fp32")):
+        sim = (S.Simulation2D if dim == 2 else S.Simulation3D)(dict(params, precision=prec), device=device)
+        sim.advance(steps)
+        got_tr = list(sim.records())
+        got_f = [sim.field(f) for f in range(nfields)]
+        tr = max(rel(a, b) for a, b in zip(got_tr, want_tr))
+        fl = max(rel(a, b) for a, b in zip(got_f, want_f) if np.any(b))
+        res = {"trace_rel_l2": tr, "field_rel_l2": fl}
+        if prec == 0:
+            res["bitwise"] = bool(all(np.array_equal(a, b) for a, b in zip(got_tr, want_tr)) and
+                                  all(np.array_equal(a, b) for a, b in zip(got_f, want_f)))
+        out[key] = res
+        sim.close()
+    return out
 
 
 def traffic_from_profiles(workload_name: str, dtype: str):
@@ -522,9 +556,12 @@ def gpu_arm(args):
     if not args.no_fp32:
         sim32, r32 = measure(1)
         del sim32
-    base = None
+    base = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        base = cpu_baseline(r64["params"], dim, args.cpu_steps, 1)
+        base, ref_run = cpu_baseline(r64["params"], dim, args.cpu_steps, 1, keep=True)
+        if ref_run is not None:
+            parity = error_vs_reference(S, r64["params"], dim, ref_run, local)
+            del ref_run
     ref_gpu = None
     if rank == 0 and world == 1 and dim == 2 and not args.no_ref_gpu:
         ref_gpu = reference_gpu(r64["params"], args.ref_gpu_steps, 2)
@@ -545,7 +582,7 @@ def gpu_arm(args):
                        "parallelism": "one independent shot per GPU" if world > 1 else "single shot",
                        "init_s": round(r64["init_s"], 3)},
             "roofline": r64["roofline"], "e2e": e2e, "gpu_launches": int(args.steps * r64["profile"]["launches_per_step"]),
-            "clocks": r64["clocks"], "cpu_baseline": base,
+            "clocks": r64["clocks"], "cpu_baseline": base, "error_vs_reference": parity,
         }
         if r32:
             line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],

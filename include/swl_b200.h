@@ -175,6 +175,18 @@ typedef struct swl_profile {
 } swl_profile;
 swl_status swl2d_profile(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency, double scale,
                          swl_profile *out);
+/* How the stage kernels decompose the grid: CTAs walk strips of strip_width columns down
+ * segments of segment_blocks blocks of block_rows rows; interior_ctas of the strips x segments
+ * CTAs touch no absorber, source support or surface row and run the interior form; exact_h says
+ * that x/h is formed as x*(1/h) (h a power of two, or FP32) rather than as the correctly rounded
+ * quotient.  No counterpart in the reference (its kernels use one form for every node). */
+typedef struct swl_layout2d {
+    int32_t strip_width, block_rows, segment_blocks;
+    int32_t strips, segments;
+    int64_t interior_ctas;
+    int32_t exact_h, precision;
+} swl_layout2d;
+swl_status swl2d_layout(swl2d_engine *engine, swl_layout2d *out);
 /* Run the engine's work on a caller-provided cudaStream_t (NULL restores its own stream).
  * No counterpart in the reference (its engines launch on the legacy default stream). */
 swl_status swl2d_set_stream(swl2d_engine *engine, void *cuda_stream);
@@ -231,10 +243,15 @@ typedef struct swl_state2d_view {
  * latency-critical loops where an allocation could synchronise the device.  Its per-block partial
  * sums live in one fixed device array inside this library, sized for at most 65,536 blocks of
  * 32x8 nodes (about 16.7 million physical nodes); larger states are rejected with SWL_ERR_INVALID.
- * Every GPU that loads the library holds that array (2 MiB) until the process exits.  The first
- * call on a device looks up the array's device address, so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (on different streams, or on
- * the same device from several threads) race and must be serialised by the caller.
+ * Every GPU that loads the library holds that array (2 MiB) until the process exits.  Each call
+ * that is not being captured looks up the array's device address in the current CUDA context (so a
+ * device reset or another context is followed); a call made during stream capture reuses the
+ * address of the last uncaptured call in the same context, so make one call before any capture.
+ * All calls share the array: calls that overlap on the GPU (on different streams, or on the same
+ * device from several threads) race and must be serialised by the caller.  The finiteness flag
+ * covers the five wavefields and, when given, the CFS-PML memories; a GSLS state's Syy and
+ * relaxation memories are not passed and not checked.  CFS-PML widths beyond the grid
+ * (2*wx > nx-6 or wz > nz-6) are rejected with SWL_ERR_INVALID.
  * No counterpart in the reference. */
 swl_status swl2d_stats_noalloc(const swl_state2d_view *state, double *out, void *cuda_stream);
 

@@ -55,10 +55,18 @@ def _ptr(a):
     return a.ctypes.data_as(_dp)
 
 
+def reference_root() -> Path | None:
+    """The reference checkout the Makefile compiles from (SWL_REFERENCE_ROOT or the recipe's
+    default), or None when its sources are not on this machine."""
+    out = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], capture_output=True, text=True)
+    root = Path(out.stdout.strip()) if out.returncode == 0 and out.stdout.strip() else None
+    return root if root is not None and (root / "src").is_dir() else None
+
+
 def build():
     """Compile liboracle.so (and the reference binaries when its sources are present)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
-    if Path(os.environ.get("SWL_REFERENCE_ROOT", "/root/reference")).is_dir():
+    if reference_root() is not None:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
 
 

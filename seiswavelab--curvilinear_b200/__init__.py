@@ -85,6 +85,15 @@ class Profile(C.Structure):
                 "bytes_per_step": self.bytes_per_step}
 
 
+class Layout2D(C.Structure):
+    _fields_ = [("strip_width", C.c_int32), ("block_rows", C.c_int32), ("segment_blocks", C.c_int32),
+                ("strips", C.c_int32), ("segments", C.c_int32), ("interior_ctas", C.c_int64),
+                ("exact_h", C.c_int32), ("precision", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -119,6 +128,7 @@ def library() -> C.CDLL:
     L.swl2d_probes.argtypes = [C.c_void_p, _i64p, C.c_int32, _dp]
     L.swl2d_resident_bytes.argtypes = [C.c_void_p]
     L.swl2d_resident_bytes.restype = C.c_int64
+    L.swl2d_layout.argtypes = [C.c_void_p, C.POINTER(Layout2D)]
     L.swl3d_create.argtypes = [C.POINTER(Mesh3D), _i64p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
     L.swl3d_destroy.argtypes = [C.c_void_p]
     L.swl3d_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32]
@@ -167,6 +177,14 @@ def _check(status: int):
 
 def device_count() -> int:
     return int(library().swl_device_count())
+
+
+def layout2d(engine_handle) -> dict:
+    """swl2d_layout of an engine handle (Engine2D._h, or a session's engine_handle())."""
+    out = Layout2D()
+    h = engine_handle if isinstance(engine_handle, C.c_void_p) else C.c_void_p(engine_handle)
+    _check(library().swl2d_layout(h, C.byref(out)))
+    return out.as_dict()
 
 
 def _f64(a):
@@ -358,6 +376,10 @@ class Engine2D:
         p = Profile()
         _check(library().swl2d_profile(self._h, first, count, dt, frequency, scale, C.byref(p)))
         return p.as_dict()
+
+    def layout(self) -> dict:
+        """Stage decomposition: strips x segments CTAs, how many run the interior form, exact 1/h."""
+        return layout2d(self._h)
 
     def set_stream(self, stream_handle: int | None):
         _check(library().swl2d_set_stream(self._h, C.c_void_p(stream_handle or 0)))

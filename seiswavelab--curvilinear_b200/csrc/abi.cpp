@@ -266,6 +266,13 @@ swl_status swl2d_probes(swl2d_engine *e, const int64_t *nodes, int32_t n, double
     });
 }
 int64_t swl2d_resident_bytes(const swl2d_engine *e) { return e && e->impl ? e->impl->residentBytes() : 0; }
+swl_status swl2d_layout(swl2d_engine *e, swl_layout2d *out) {
+    return guarded([&] {
+        ENGINE(e);
+        need(out, "out");
+        E.layout(*out);
+    });
+}
 swl_status swl2d_profile(swl2d_engine *e, int32_t first, int32_t count, double dt, double frequency, double scale,
                          swl_profile *out) {
     return guarded([&] {

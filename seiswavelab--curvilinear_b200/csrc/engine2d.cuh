@@ -57,6 +57,8 @@ class Engine2D {
     virtual void launch(int first, int count, double dt, double frequency, double scale, double growthAfter) = 0;
     virtual bool query(int &accepted) = 0;
     virtual int finish() = 0;
+    // How the stage kernels decompose the grid, and how many CTAs take each compiled form.
+    virtual void layout(swl_layout2d &) const = 0;
 };
 
 std::unique_ptr<Engine2D> makeEngine2D64(const swl_mesh2d &, const int64_t *, int, int);
@@ -698,6 +700,19 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         u_ = 0, a_ = 1, previous_ = false, faulted_ = false;
     }
     int segment() const { return m_.seg; }
+    void layout(swl_layout2d &out) const override {
+        out = swl_layout2d{};
+        out.strip_width = k2::SW;
+        out.block_rows = k2::SB;
+        out.segment_blocks = m_.seg;
+        out.strips = int32_t(stageGrid_.x);
+        out.segments = int32_t(stageGrid_.y);
+        for (unsigned by = 0; by < stageGrid_.y; ++by)
+            for (unsigned bx = 0; bx < stageGrid_.x; ++bx)
+                out.interior_ctas += k2::interiorBlock(m_, 3 + int(bx) * k2::SW, 3 + int(by) * (k2::SB * m_.seg)) ? 1 : 0;
+        out.exact_h = m_.hinvExact;
+        out.precision = sizeof(Real) == 8 ? SWL_FP64 : SWL_FP32;
+    }
 
     // ---- queued batches (Queue2D): the two halves of launch() around the persistent kernel
     int mechanisms() const { return mech_; }

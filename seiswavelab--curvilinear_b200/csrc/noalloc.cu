@@ -19,23 +19,59 @@ constexpr int kMaxBlocks = 65536; // 16.7 M physical nodes at 256 nodes per bloc
 
 // Scratch for the per-block partials (2 MiB).  Every device that loads the library holds it.
 // Host code must not pass this symbol to a kernel: on the host it is only a stand-in for the
-// device array; its device address comes from cudaGetSymbolAddress (scratchOn below).
+// device array; its device address comes from cudaGetSymbolAddress (scratchAddress below).
 static __device__ __align__(256) Part stats2dScratch[kMaxBlocks];
 
-constexpr int kMaxDevices = 64;
-Part *scratchAddress[kMaxDevices] = {};
+// The array's device address belongs to the CUDA context the module was loaded into.  A device
+// reset (cudaDeviceReset) or another context on the same device gives the array a new address, so
+// the address is looked up again on every call that is not being captured into a graph, and the
+// last address seen per context is kept only for calls made during a capture (where the lookup,
+// which may load the module, is not made).
+using CtxGetCurrent = CUresult (*)(CUcontext *);
+constexpr int kMaxContexts = 64;
+struct CachedAddress {
+    CUcontext context;
+    Part *address;
+};
+CachedAddress scratchCache[kMaxContexts] = {};
 std::mutex scratchMutex;
 
-// Device address of the scratch array on `device` (current), looked up once per device.
-Part *scratchOn(int device) {
-    if (device < 0 || device >= kMaxDevices) throw swl::Error(SWL_ERR_INVALID, "device index out of range");
-    std::lock_guard<std::mutex> lock(scratchMutex);
-    if (!scratchAddress[device]) {
-        void *p = nullptr;
+CUcontext currentContext() {
+    static CtxGetCurrent fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        swl::check(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q), "find cuCtxGetCurrent");
+        if (!f || q != cudaDriverEntryPointSuccess) throw swl::Error(SWL_ERR_CUDA, "the driver has no cuCtxGetCurrent");
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS || !c) throw swl::Error(SWL_ERR_CUDA, "no current CUDA context");
+    return c;
+}
+
+// Device address of the scratch array in the current context.  Outside a capture the lookup
+// comes first: it also makes the device's primary context current if nothing has yet.
+Part *scratchAddress(cudaStream_t stream) {
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    swl::check(cudaStreamIsCapturing(stream, &capture), "query stream capture");
+    void *p = nullptr;
+    if (capture == cudaStreamCaptureStatusNone)
         swl::check(cudaGetSymbolAddress(&p, stats2dScratch), "look up the diagnostics scratch array");
-        scratchAddress[device] = static_cast<Part *>(p);
+    const CUcontext ctx = currentContext();
+    std::lock_guard<std::mutex> lock(scratchMutex);
+    int slot = -1, empty = -1;
+    for (int c = 0; c < kMaxContexts; ++c) {
+        if (scratchCache[c].context == ctx) slot = c;
+        if (!scratchCache[c].context && empty < 0) empty = c;
     }
-    return scratchAddress[device];
+    if (capture != cudaStreamCaptureStatusNone) {
+        if (slot < 0 || !scratchCache[slot].address)
+            throw swl::Error(SWL_ERR_INVALID, "swl2d_stats_noalloc: make the first call in this context before stream capture");
+        return scratchCache[slot].address;
+    }
+    if (slot < 0) slot = empty >= 0 ? empty : 0; // more contexts than slots: reuse the first
+    scratchCache[slot] = {ctx, static_cast<Part *>(p)};
+    return static_cast<Part *>(p);
 }
 
 __global__ void __launch_bounds__(kBlockX *kBlockY) partials(const swl_state2d_view v, Part *scratch) {
@@ -129,15 +165,18 @@ extern "C" swl_status swl2d_stats_noalloc(const swl_state2d_view *v, double *out
             throw swl::Error(SWL_ERR_INVALID, "every field and model pointer of the state is required");
         if (v->pml && (v->cpml_width_x < 0 || v->cpml_width_z < 1))
             throw swl::Error(SWL_ERR_INVALID, "CFS-PML widths are required with the memories");
+        // The memory slots of a node are computed from the widths; widths wider than the grid
+        // would index past the caller's memories (the reference caps them at a third of the grid,
+        // src/two_d/CurvilinearSolver2D.cpp:507).
+        if (v->pml && (2 * int64_t(v->cpml_width_x) > v->nx - 6 || v->cpml_width_z > v->nz - 6))
+            throw swl::Error(SWL_ERR_INVALID, "CFS-PML widths exceed the grid: need 2*wx <= nx-6 and wz <= nz-6");
         const dim3 block(kBlockX, kBlockY), grid((v->nx - 6 + kBlockX - 1) / kBlockX, (v->nz - 6 + kBlockY - 1) / kBlockY);
         const long long blocks = (long long)grid.x * grid.y;
         if (blocks > kMaxBlocks)
             throw swl::Error(SWL_ERR_INVALID, "state too large for swl2d_stats_noalloc: " + std::to_string(blocks) +
                                                   " blocks of 32x8 nodes, at most " + std::to_string(kMaxBlocks));
-        int device = 0;
-        swl::check(cudaGetDevice(&device), "query current device");
-        Part *scratch = scratchOn(device);
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        Part *scratch = scratchAddress(s);
         partials<<<grid, block, 0, s>>>(*v, scratch);
         swl::check(cudaGetLastError(), "no-allocation diagnostics launch");
         finish<<<1, 1024, 0, s>>>(scratch, int(blocks), out);

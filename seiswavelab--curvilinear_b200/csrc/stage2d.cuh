@@ -294,14 +294,6 @@ __device__ __forceinline__ Real stretch(const Real *prof, Real psi, Real d, Real
     return d / kappa + psi;
 }
 
-__device__ __forceinline__ void cpAsync(void *smem, const void *gmem, int bytes) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
-    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 // RK combine of one value (reference order, src/two_d/CurvilinearSolver2D.cpp:89):
 // stage 0: A = k, out = U + w k;  stages 1-2: A = A + 2k, out = U + w k;  stage 3: U + dt (A + k) / 6.
 // `acc` is the node's A (unused in stage 0); `accOut` receives the new A (stages 0-2).
@@ -651,8 +643,9 @@ __device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int 
 template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 3; }
 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
-// strips, the sponge, the source support and the surface rows 3..6).
-template <class Real> __device__ __forceinline__ bool interiorBlock(const Mesh<Real> &m, int i0, int z0) {
+// strips, the sponge, the source support and the surface rows 3..6).  The host evaluates the
+// same predicate to report how many CTAs take the interior form (swl2d_layout).
+template <class Real> __host__ __device__ __forceinline__ bool interiorBlock(const Mesh<Real> &m, int i0, int z0) {
     const int i1 = i0 + SW, z1 = z0 + SB * m.seg; // exclusive ends
     const bool pml = i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || z1 - 3 > m.nz - 6 - m.wz;
     const bool surface = z0 < 7;

@@ -118,21 +118,23 @@ def grf_dem(nx: int, ny: int, spacing: float, correlation: float, relief: float,
 
 
 def elastic_3d(precision: int = 0, steps: int = 1500, nx: int = 400, ny: int = 288, nz: int = 200,
-               receivers: int = 40) -> dict:
+               receivers: int = 40, relief: float = 150.0, flatten_depth: float = 800.0) -> dict:
     """400x288x200 3D elastic, h=10 m, DEM terrain (seed 4, correlation 500 m, relief 150 m on a
     25 m lattice), blend depth 800 m, layers 200 m / 600 m / basement below the surface, 15 Hz
-    explosive source 5 nodes deep, 20-cell sponge, 40x40 areal surface receivers."""
+    explosive source 5 nodes deep, 20-cell sponge, 40x40 areal surface receivers.  Reduced grids
+    need a smaller relief and blend depth (the blend must fit the model depth and exceed 2.6 times
+    the relief)."""
     h = 10.0
     dem_dx = 25.0
     dnx = int(np.ceil((nx - 1) * h / dem_dx)) + 1
     dny = int(np.ceil((ny - 1) * h / dem_dx)) + 1
-    elev = grf_dem(dnx, dny, dem_dx, 500.0, 150.0, seed=4)
+    elev = grf_dem(dnx, dny, dem_dx, 500.0, relief, seed=4)
     sx = max(1, (nx - 2) // receivers)
     sy = max(1, (ny - 2) // receivers)
     return dict(precision=precision, nx=nx, ny=ny, nz=nz, spacing=h, frequency=15.0, cfl=0.8, duration=2.0,
                 maxSteps=steps, sourceX=nx // 2, sourceY=ny // 2, sourceZ=5, sourceKind=1,
                 demShape=[dnx, dny, dem_dx, 0.0, 0.0, 0.0], demElevations=elev.ravel().tolist(),
-                flattenDepth=800.0, layered=1, layerDepthMode=1,
+                flattenDepth=float(flatten_depth), layered=1, layerDepthMode=1,
                 layers=[200, 1200, 600, 1800, 600, 2400, 1300, 2100, 0, 3800, 2200, 2400],
                 absorbing=1, absorbingCells=[20, 20, 20], absorbingStrength=3.0,
                 receiverArray=[3, (nx - (receivers - 1) * sx) // 2, (ny - (receivers - 1) * sy) // 2, 0,

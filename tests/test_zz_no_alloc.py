@@ -84,3 +84,16 @@ def test_noalloc_rejects_states_beyond_its_scratch(swl):
         setattr(v, k, 16)  # never dereferenced: the size check fails before any launch
     assert lib.swl2d_stats_noalloc(C.byref(v), C.c_void_p(16), None) == swl.ERR_INVALID
     assert b"too large" in lib.swl_last_error()
+
+
+def test_noalloc_rejects_cpml_widths_beyond_the_grid(swl):
+    lib = swl.library()
+    lib.swl2d_stats_noalloc.argtypes = [C.POINTER(StateView), C.c_void_p, C.c_void_p]
+    v = StateView()
+    v.nx, v.nz, v.h = 46, 36, 5.0
+    for k in ("vx", "vz", "sxx", "szz", "sxz", "lam", "mu", "rho", "jac", "normals", "pml"):
+        setattr(v, k, 16)  # never dereferenced: the width check fails before any launch
+    for wx, wz in ((21, 6), (6, 31)):  # 2*wx > nx-6, wz > nz-6
+        v.cpml_width_x, v.cpml_width_z = wx, wz
+        assert lib.swl2d_stats_noalloc(C.byref(v), C.c_void_p(16), None) == swl.ERR_INVALID
+        assert b"widths exceed" in lib.swl_last_error()
