@@ -364,7 +364,12 @@ template <class Real, int DX, int DZ, int MECH, int STAGE, bool FULL, class S>
 __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, int i, int k, Partial &diag, bool withDiag) {
     const Mesh<Real> &m = p.m;
     constexpr bool KAHAN3 = STAGE == 3 && kahan<Real>();
-    const bool CPML = FULL && m.wz > 0;
+    // A mesh with CFS-PML sums every node's momentum per axis, x/rho + z/rho, and stretches the
+    // terms of the nodes that own memory slots (PointKernels2D.hpp:148-153); without CFS-PML the
+    // momentum is one quotient, (x + z)/rho.  SPLIT follows the mesh; CPML (slot handling) is
+    // compiled out of the interior form, whose nodes own no slots.
+    const bool SPLIT = m.wz > 0;
+    const bool CPML = FULL && SPLIT;
     const long long n = m.count, q = t.q;
     const int depth = FULL ? k - 3 : 4; // any depth past the near-surface rows
     const Real *__restrict__ w = p.in;
@@ -500,7 +505,7 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
     const Real rho = t.rho(m);
     Real r0, r1;
     const bool near = depth <= (DZ ? 3 : 1);
-    if (!CPML) {
+    if (!SPLIT) {
         if (near) {
             const Real jac = t.jac(m);
             r0 = momentum<Real, DX, DZ>(m, t, jac, rho, 0, depth, -1);
@@ -526,14 +531,14 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 X = tdrp<Real, DX>(t, m, f, 0) / rho;
                 Z = (a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1)) / rho;
             }
-            if (slot0 >= 0) X = stretch(prof0, lds(p.pin + slot0 + 2 + v), X, mrate[v]);
-            if (slot1 >= 0) Z = stretch(prof1, lds(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
+            if (CPML && slot0 >= 0) X = stretch(prof0, lds(p.pin + slot0 + 2 + v), X, mrate[v]);
+            if (CPML && slot1 >= 0) Z = stretch(prof1, lds(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
             rv[v] = X + Z;
         }
         r0 = rv[0], r1 = rv[1];
-        if (slot0 >= 0)
+        if (CPML && slot0 >= 0)
             for (int v = 0; v < 2; ++v) combineMemory<Real, STAGE>(p, slot0 + 2 + v, mrate[v], diag, withDiag);
-        if (slot1 >= 0)
+        if (CPML && slot1 >= 0)
             for (int v = 0; v < 2; ++v) combineMemory<Real, STAGE>(p, slot1 + 2 + v, mrate[2 + v], diag, withDiag);
     }
     if (FULL && i >= m.src_i0 && i < m.src_i1 && k >= m.src_k0 && k < m.src_k1) {
