@@ -339,6 +339,21 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             m_.hinvExact = (pow2 || sizeof(Real) == 4) ? 1 : 0;
         }
         {
+            // divBy's correctly rounded quotient needs a divisor in [2^-20, 2^20] (the densities of
+            // the computational nodes; ghost nodes are never divisors)
+            const auto rho = detail2::convert<Real>(g.rho, nu, ap, "rho");
+            bool ok = true;
+            for (int k = 3; ok && k < g.nz - 3; ++k)
+                for (int i = 3; i < g.nx - 3; ++i) {
+                    const Real r = rho[i + std::size_t(g.nx) * k];
+                    if (!(r >= Real(0x1p-20) && r <= Real(0x1p+20))) {
+                        ok = false;
+                        break;
+                    }
+                }
+            m_.rhoRecip = ok ? 1 : 0;
+        }
+        {
             pack_.allocate(6 * n * sizeof(Real));
             const void *src[6] = {g.a, g.b, g.lambda, g.mu, g.rho, g.jac};
             const char *names[6] = {"a", "b", "lambda", "mu", "rho", "jac"};

@@ -34,6 +34,7 @@ template <class Real> struct Mesh {
     int seg;         // row blocks per streaming segment (chosen per grid by the engine's tuner)
     Real h, hinv;   // hinv = RN(1/h); x/h is x*hinv when h is a power of two (or in FP32),
     int hinvExact;  // else the correctly rounded divBy(x, h, hinv)
+    int rhoRecip;   // every density lies in divBy's divisor range: x/rho = divBy(x, rho, RN(1/rho))
     const Real *a, *b, *jac, *normals, *lambda, *mu, *rho, *damping, *source, *sgx, *sgz;
     Real sdx, sdz;             // unit force direction (x, z)
     int src_i0, src_i1, src_k0, src_k1; // source support box [i0,i1) x [k0,k1), padded indices
@@ -503,6 +504,10 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
 
     // ---- phase 2: stress derivatives -> velocity rates
     const Real rho = t.rho(m);
+    // The node's quotients by rho (two to four of them) from one reciprocal: divBy forms the
+    // correctly rounded quotient, the same value as the division.
+    const Real rinv = m.rhoRecip ? Real(1) / rho : Real(0);
+    auto byRho = [&](Real x) { return m.rhoRecip ? divBy(x, rho, rinv) : x / rho; };
     Real r0, r1;
     const bool near = depth <= (DZ ? 3 : 1);
     if (!SPLIT) {
@@ -513,8 +518,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         } else {
             const Real x2 = tdrp<Real, DX>(t, m, 2, 0), x4 = tdrp<Real, DX>(t, m, 4, 0);
             const Real e2 = tdrp<Real, DZ>(t, m, 2, 1), e3 = tdrp<Real, DZ>(t, m, 3, 1), e4 = tdrp<Real, DZ>(t, m, 4, 1);
-            r0 = ((x2 + a * e2) + b * e4) / rho;
-            r1 = ((x4 + a * e4) + b * e3) / rho;
+            r0 = byRho((x2 + a * e2) + b * e4);
+            r1 = byRho((x4 + a * e4) + b * e3);
         }
     } else {
         Real mrate[4] = {0, 0, 0, 0}; // ADE rates of the momentum memories: slot0 f2,f3, slot1 f2,f3
@@ -528,8 +533,8 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
                 X = momentum<Real, DX, DZ>(m, t, jac, rho, v, depth, 0);
                 Z = momentum<Real, DX, DZ>(m, t, jac, rho, v, depth, 1);
             } else {
-                X = tdrp<Real, DX>(t, m, f, 0) / rho;
-                Z = (a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1)) / rho;
+                X = byRho(tdrp<Real, DX>(t, m, f, 0));
+                Z = byRho(a * tdrp<Real, DZ>(t, m, f, 1) + b * tdrp<Real, DZ>(t, m, o, 1));
             }
             if (CPML && slot0 >= 0) X = stretch(prof0, lds(p.pin + slot0 + 2 + v), X, mrate[v]);
             if (CPML && slot1 >= 0) Z = stretch(prof1, lds(p.pin + slot1 + 2 + v), Z, mrate[2 + v]);
@@ -545,12 +550,12 @@ __device__ __forceinline__ void stageNode(const StageArgs<Real> &p, const S &t, 
         const Clock *clk = p.clock;
         const Real forcing = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
         if (m.sgx) {
-            r0 += forcing * ld(m.sgx + q) / rho;
-            r1 += forcing * ld(m.sgz + q) / rho;
+            r0 += byRho(forcing * ld(m.sgx + q));
+            r1 += byRho(forcing * ld(m.sgz + q));
         } else {
             const Real s = ld(m.source + q);
-            r0 += forcing * (s * m.sdx) / rho;
-            r1 += forcing * (s * m.sdz) / rho;
+            r0 += byRho(forcing * (s * m.sdx));
+            r1 += byRho(forcing * (s * m.sdz));
         }
     }
     if (damped) {

@@ -34,6 +34,7 @@ template <class Real> struct Mesh {
     Real h, lambda, mu, density;    // uniform material (used when the material arrays are null)
     Real hinv;                      // RN(1/h)
     int hinvExact;                  // h is a power of two (or FP32): x/h = x*hinv
+    int rhoRecip;                   // every density lies in divBy's divisor range [2^-20, 2^20]
     const Real *metric[9];          // d(xi,eta,zeta)/d(x,y,z), row-major 3x3 per node
     const Real *jac, *damping, *source, *sg[3];
     const Real *mlambda, *mmu, *mdensity;
@@ -64,6 +65,18 @@ using k2::ld;
 
 // x / h as the reference forms it: the product with 1/h when that is exact, else the correctly
 // rounded FMA quotient (both equal the IEEE division bit for bit).
+// The three momentum quotients of a node by its density from one reciprocal: divBy forms the
+// correctly rounded quotient, the same value as the division.
+template <class Real> __device__ __forceinline__ void byRho3(const Mesh<Real> &m, Real rho, Real (&r)[9], Real m0, Real m1, Real m2) {
+    if (m.rhoRecip) {
+        const Real rinv = Real(1) / rho;
+        r[0] = k2::divBy(m0, rho, rinv);
+        r[1] = k2::divBy(m1, rho, rinv);
+        r[2] = k2::divBy(m2, rho, rinv);
+    } else {
+        byRho3(m, rho, r, m0, m1, m2);
+    }
+}
 template <class Real, bool EXACT> __device__ __forceinline__ Real overH(const Mesh<Real> &m, Real r) {
     if constexpr (EXACT) return r * m.hinv;
     else return k2::divBy(r, m.h, m.hinv);
@@ -307,9 +320,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, a, depth, rho);
     } else {
-        r[0] = (gr[3][0] + gr[6][1] + gr[7][2]) / rho;
-        r[1] = (gr[6][0] + gr[4][1] + gr[8][2]) / rho;
-        r[2] = (gr[7][0] + gr[8][1] + gr[5][2]) / rho;
+        byRho3(m, rho, r, (gr[3][0] + gr[6][1]) + gr[7][2], (gr[6][0] + gr[4][1]) + gr[8][2], (gr[7][0] + gr[8][1]) + gr[5][2]);
     }
     if (i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
         const Real s = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
@@ -397,9 +408,7 @@ __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
         grad(7, g, true, false, true), m0 = m0 + g[2], t70 = g[0];
         grad(8, g, false, true, true), m1 = m1 + g[2], m2 = (t70 + g[1]) + t52;
         const Real rho = m.mdensity ? ld(m.mdensity + q) : m.density;
-        r[0] = m0 / rho;
-        r[1] = m1 / rho;
-        r[2] = m2 / rho;
+        byRho3(m, rho, r, m0, m1, m2);
     }
     if (DAMP && !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
         const Real d = ld(m.damping + q);
