@@ -408,7 +408,10 @@ def serving_leg(args, device: int) -> dict:
     if args.serving_batched_only:
         return {"requests": len(reqs), "batched_fp32": batched}
     service, rec64, init64, util64, kinds64 = sequential(0)
-    service32, _, init32, util32s, kinds32 = sequential(1)
+    if args.serving_fp32_sequential:
+        service32, _, init32, util32s, kinds32 = sequential(1)
+    else:
+        service32, init32, util32s, kinds32 = [], None, None, None
     finish, lat64, clock = [], [], 0.0
     for r, s in zip(reqs, service):
         start = max(clock, r["arrival"] - a0)
@@ -428,9 +431,11 @@ def serving_leg(args, device: int) -> dict:
         "batched_fp32": batched,
         "sequential_fp64": {"shots_per_hour": shots / span64 * 3600, "p50_s": float(np.percentile(lat64, 50)),
                             "p99_s": float(np.percentile(lat64, 99)), "makespan_s": span64,
-                            "sum_init_s": init64, "gpu_util_pct": util64, "by_kind": kinds64},
+                            "sum_init_s": init64, "gpu_util_pct": util64, "by_kind": kinds64,
+                            "latency_model": "the requests ran one after another; each one's measured service time is "
+                                             "queued at its arrival time (FIFO, one GPU) to give its latency"},
         "sequential_fp32": {"sum_service_s": float(np.sum(service32)), "sum_init_s": init32, "gpu_util_pct": util32s,
-                            "by_kind": kinds32},
+                            "by_kind": kinds32} if args.serving_fp32_sequential else None,
         "shots_per_hour_ratio": (shots / span32) / (shots / span64),
         "max_trace_rel_l2_fp32_vs_fp64": max(errs), "median_trace_rel_l2_fp32_vs_fp64": float(np.median(errs)),
     }
@@ -646,6 +651,8 @@ def main():
     ap.add_argument("--serving-steps", type=float, default=0.25, help="step-count scale of the serving mix")
     ap.add_argument("--serving-batch", type=int, default=64, help="steps per batch of a served shot")
     ap.add_argument("--serving-schedulers", type=int, default=2, help="server threads driving the running shots")
+    ap.add_argument("--serving-fp32-sequential", type=int, default=1,
+                    help="also run the requests one after another in FP32 (separates precision from batching; 0: skip)")
     ap.add_argument("--serving-batched-only", action="store_true",
                     help="run only the batched leg (to compare serving settings; no ratio)")
     ap.add_argument("--serving-active", type=int, default=32, help="shots built or running at once (0: memory-bound only)")

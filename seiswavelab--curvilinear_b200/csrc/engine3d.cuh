@@ -275,6 +275,23 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             m_.mdensity = upload(conv(g.material_density));
         }
         {
+            // divBy's correctly rounded quotient needs a divisor in [2^-20, 2^20]; only the
+            // computational nodes' densities are divisors
+            auto inRange = [](Real r) { return r >= Real(0x1p-20) && r <= Real(0x1p+20); };
+            bool ok = inRange(m_.density);
+            if (g.material_density) {
+                const auto rho = conv(g.material_density);
+                for (int k = 3; ok && k < g.nz - 3; ++k)
+                    for (int j = 3; ok && j < g.ny - 3; ++j)
+                        for (int i = 3; i < g.nx - 3; ++i)
+                            if (!inRange(rho[i + std::size_t(m_.px) * j + std::size_t(m_.plane) * k])) {
+                                ok = false;
+                                break;
+                            }
+            }
+            m_.rhoRecip = ok ? 1 : 0;
+        }
+        {
             std::vector<Real> nrm(3 * std::size_t(m_.plane), Real(0));
             const std::size_t nx = std::size_t(g.nx), top = std::size_t(3) * nx * g.ny;
             for (std::size_t j = 0; j < std::size_t(g.ny); ++j)

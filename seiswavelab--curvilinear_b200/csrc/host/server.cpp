@@ -6,6 +6,7 @@
 // multi-shot launch per round, admits new shots at the next round, and records each shot's batch
 // when the launch completes.  Finished shots release their device memory at once, which admits
 // the next request.
+#include "../../../include/swl_fleet.h"
 #include "../../../include/swl_server.h"
 #include "sessions.hpp"
 #include <atomic>
@@ -468,10 +469,128 @@ class Server {
     }
 };
 
+// Worst-fit placement (include/swl_fleet.h): the slot with the most budget left after its
+// charges, lower slot on ties; -1 when the charge exceeds every slot's whole budget.
+int chooseSlot(int n, const int64_t *budgets, const int64_t *charged, int64_t charge) {
+    int best = -1;
+    int64_t bestLeft = 0;
+    for (int d = 0; d < n; ++d) {
+        if (charge > budgets[d]) continue; // can never run there
+        const int64_t left = budgets[d] - charged[d];
+        if (best < 0 || left > bestLeft) best = d, bestLeft = left;
+    }
+    return best;
+}
+
+// One request loop per device and a front that places each request by budget.  The front keeps
+// each shot's charge against its slot until the shot's server reports it finished.
+class Fleet {
+  public:
+    explicit Fleet(const swl_fleet_config &c) {
+        std::vector<int> devices;
+        if (c.n_devices > 0) {
+            if (c.n_devices > SWL_FLEET_MAX_DEVICES) throw Failure(SWL_ERR_INVALID, "too many fleet devices");
+            devices.assign(c.devices, c.devices + c.n_devices);
+        } else {
+            int n = 0;
+            if (cudaGetDeviceCount(&n) != cudaSuccess) cudaGetLastError(), n = 0;
+            for (int d = 0; d < n && int(devices.size()) < SWL_FLEET_MAX_DEVICES; ++d) {
+                cudaDeviceProp pr{};
+                if (cudaGetDeviceProperties(&pr, d) == cudaSuccess && pr.major == 10) devices.push_back(d);
+            }
+        }
+        if (devices.empty()) throw Failure(SWL_ERR_UNAVAILABLE, "no usable sm_100 CUDA device for the fleet");
+        for (int d : devices) {
+            if (selectDevice(d) != d) throw Failure(SWL_ERR_UNAVAILABLE, "fleet device " + std::to_string(d) + " is not usable");
+            swl_server_config sc = c.server;
+            sc.device = d;
+            servers_.push_back(std::make_unique<Server>(sc));
+            devices_.push_back(d);
+            budgets_.push_back(servers_.back()->stats().memory_budget);
+        }
+    }
+    int size() const { return int(servers_.size()); }
+    int device(int slot) const { return slot >= 0 && slot < size() ? devices_[slot] : -1; }
+    int64_t submit(std::shared_ptr<Shot> s, int &slot) {
+        std::lock_guard<std::mutex> g(mu_);
+        const int64_t charge = estimate(*s);
+        refresh();
+        std::vector<int64_t> charged(size(), 0);
+        for (const auto &kv : shots_)
+            if (!kv.second.done) charged[kv.second.slot] += kv.second.charge;
+        slot = chooseSlot(size(), budgets_.data(), charged.data(), charge);
+        if (slot < 0)
+            throw Failure(SWL_ERR_MEMORY, "request needs " + std::to_string(charge) + " device bytes, more than any fleet device's budget");
+        const int64_t local = servers_[slot]->submit(std::move(s));
+        const int64_t id = next_++;
+        shots_[id] = Entry{slot, local, charge, false};
+        return id;
+    }
+    swl_shot_status status(int64_t id, int &slot) {
+        const Entry e = entry(id);
+        slot = e.slot;
+        swl_shot_status o = servers_[e.slot]->status(e.local);
+        o.id = id;
+        return o;
+    }
+    void records(int64_t id, double *vx, double *vy, double *vz) {
+        const Entry e = entry(id);
+        servers_[e.slot]->records(e.local, vx, vy, vz);
+    }
+    void release(int64_t id) {
+        const Entry e = entry(id);
+        servers_[e.slot]->release(e.local);
+        std::lock_guard<std::mutex> g(mu_);
+        shots_.erase(id);
+    }
+    void drain() {
+        for (auto &sv : servers_) sv->drain();
+    }
+    swl_server_stats stats(int slot, int64_t &charged) {
+        if (slot < 0 || slot >= size()) throw Failure(SWL_ERR_INVALID, "fleet slot out of range");
+        std::lock_guard<std::mutex> g(mu_);
+        refresh();
+        charged = 0;
+        for (const auto &kv : shots_)
+            if (!kv.second.done && kv.second.slot == slot) charged += kv.second.charge;
+        return servers_[slot]->stats();
+    }
+
+  private:
+    struct Entry {
+        int slot;
+        int64_t local, charge;
+        bool done;
+    };
+    Entry entry(int64_t id) {
+        std::lock_guard<std::mutex> g(mu_);
+        const auto it = shots_.find(id);
+        if (it == shots_.end()) throw Failure(SWL_ERR_INVALID, "unknown fleet shot id");
+        return it->second;
+    }
+    // Finished shots stop counting against their device (caller holds mu_).
+    void refresh() {
+        for (auto &kv : shots_) {
+            if (kv.second.done) continue;
+            const int st = servers_[kv.second.slot]->status(kv.second.local).state;
+            kv.second.done = st == SWL_SHOT_DONE || st == SWL_SHOT_FAILED;
+        }
+    }
+    std::vector<std::unique_ptr<Server>> servers_;
+    std::vector<int> devices_;
+    std::vector<int64_t> budgets_;
+    std::map<int64_t, Entry> shots_;
+    int64_t next_{0};
+    std::mutex mu_;
+};
+
 } // namespace swl::host
 
 struct swl_server : swl::host::Server {
     using Server::Server;
+};
+struct swl_fleet : swl::host::Fleet {
+    using Fleet::Fleet;
 };
 
 extern "C" {
@@ -536,6 +655,98 @@ swl_status swl_server_drain(swl_server *s) {
     return swl::host::guard([&] {
         if (!s) throw swl::host::Failure(SWL_ERR_INVALID, "server is null");
         s->drain();
+    });
+}
+swl_status swl_request_bytes2d(const swl_params2d *p, int64_t *bytes) {
+    return swl::host::guard([&] {
+        if (!p || !bytes) throw swl::host::Failure(SWL_ERR_INVALID, "params and bytes are required");
+        swl::host::Shot shot;
+        shot.dim = 2;
+        shot.p2 = swl::host::toParams(*p);
+        *bytes = swl::host::estimate(shot);
+    });
+}
+swl_status swl_request_bytes3d(const swl_params3d *p, int64_t *bytes) {
+    return swl::host::guard([&] {
+        if (!p || !bytes) throw swl::host::Failure(SWL_ERR_INVALID, "params and bytes are required");
+        swl::host::Shot shot;
+        shot.dim = 3;
+        shot.p3 = swl::host::toParams(*p);
+        *bytes = swl::host::estimate(shot);
+    });
+}
+int32_t swl_fleet_choose(int32_t n, const int64_t *budgets, const int64_t *charged, int64_t charge) {
+    if (n <= 0 || !budgets || !charged || charge < 0) return -1;
+    return swl::host::chooseSlot(n, budgets, charged, charge);
+}
+void swl_fleet_config_default(swl_fleet_config *c) {
+    if (!c) return;
+    *c = swl_fleet_config{};
+    swl_server_config_default(&c->server);
+}
+swl_status swl_fleet_create(const swl_fleet_config *c, swl_fleet **out) {
+    return swl::host::guard([&] {
+        if (!c || !out) throw swl::host::Failure(SWL_ERR_INVALID, "config and out are required");
+        *out = new swl_fleet(*c);
+    });
+}
+void swl_fleet_destroy(swl_fleet *f) { delete f; }
+int32_t swl_fleet_size(const swl_fleet *f) { return f ? f->size() : 0; }
+int32_t swl_fleet_device(const swl_fleet *f, int32_t slot) { return f ? f->device(slot) : -1; }
+swl_status swl_fleet_submit2d(swl_fleet *f, const swl_params2d *p, int64_t *id, int32_t *slot) {
+    return swl::host::guard([&] {
+        if (!f || !p || !id) throw swl::host::Failure(SWL_ERR_INVALID, "fleet, params and id are required");
+        auto shot = std::make_shared<swl::host::Shot>();
+        shot->dim = 2;
+        shot->p2 = swl::host::toParams(*p);
+        int sl = -1;
+        *id = f->submit(shot, sl);
+        if (slot) *slot = sl;
+    });
+}
+swl_status swl_fleet_submit3d(swl_fleet *f, const swl_params3d *p, int64_t *id, int32_t *slot) {
+    return swl::host::guard([&] {
+        if (!f || !p || !id) throw swl::host::Failure(SWL_ERR_INVALID, "fleet, params and id are required");
+        auto shot = std::make_shared<swl::host::Shot>();
+        shot->dim = 3;
+        shot->p3 = swl::host::toParams(*p);
+        int sl = -1;
+        *id = f->submit(shot, sl);
+        if (slot) *slot = sl;
+    });
+}
+swl_status swl_fleet_status(swl_fleet *f, int64_t id, swl_shot_status *out, int32_t *slot) {
+    return swl::host::guard([&] {
+        if (!f || !out) throw swl::host::Failure(SWL_ERR_INVALID, "fleet and out are required");
+        int sl = -1;
+        *out = f->status(id, sl);
+        if (slot) *slot = sl;
+    });
+}
+swl_status swl_fleet_records(swl_fleet *f, int64_t id, double *vx, double *vy, double *vz) {
+    return swl::host::guard([&] {
+        if (!f) throw swl::host::Failure(SWL_ERR_INVALID, "fleet is null");
+        f->records(id, vx, vy, vz);
+    });
+}
+swl_status swl_fleet_release(swl_fleet *f, int64_t id) {
+    return swl::host::guard([&] {
+        if (!f) throw swl::host::Failure(SWL_ERR_INVALID, "fleet is null");
+        f->release(id);
+    });
+}
+swl_status swl_fleet_drain(swl_fleet *f) {
+    return swl::host::guard([&] {
+        if (!f) throw swl::host::Failure(SWL_ERR_INVALID, "fleet is null");
+        f->drain();
+    });
+}
+swl_status swl_fleet_stats(swl_fleet *f, int32_t slot, swl_server_stats *out, int64_t *charged) {
+    return swl::host::guard([&] {
+        if (!f || !out) throw swl::host::Failure(SWL_ERR_INVALID, "fleet and out are required");
+        int64_t c = 0;
+        *out = f->stats(slot, c);
+        if (charged) *charged = c;
     });
 }
 swl_status swl_server_stats_get(swl_server *s, swl_server_stats *out) {

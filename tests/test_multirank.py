@@ -70,3 +70,71 @@ def test_two_ranks_each_run_their_own_shot(tmp_path):
         _, _, mesh = load_2d(SHOTS[rank])
         alone, _, _, _ = orc.run2d(mesh, 20)
         np.testing.assert_array_equal(r["state"], alone)
+
+
+def _fleet_rank(rank: int, world: int, port: int, out_dir: str):
+    """One rank of a request stream sharded over `world` devices: every rank computes the same
+    placement plan from the request list and the budgets alone, and serves its own slot's shots
+    (here: builds their models, SWL_MODEL_ONLY, without a GPU).  The ranks exchange nothing on the
+    data path; the plan is compared across ranks only to check that it is the same everywhere."""
+    import importlib
+    import pickle
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    from conftest import load_package
+
+    load_package()
+    F = importlib.import_module("swl_b200.fleet")
+    S = importlib.import_module("swl_b200.session")
+    W = importlib.import_module("swl_b200.workloads")
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    reqs = FLEET_REQUESTS(W)
+    budget = 3 * max(F.request_bytes(r["params"], r["dim"]) for r in reqs)
+    slots = F.plan(reqs, [budget] * world)
+    plans = [None] * world
+    dist.all_gather_object(plans, slots)
+    mine = {}
+    for i, (r, s) in enumerate(zip(reqs, slots)):
+        if s != rank:
+            continue
+        sim = (S.Simulation2D if r["dim"] == 2 else S.Simulation3D)(r["params"], device=S.MODEL_ONLY)
+        info = sim.info()
+        mine[i] = (info["dt"], info["total_steps"], info["nx"], info["nz"])
+    with open(Path(out_dir) / f"fleet{rank}.pkl", "wb") as f:
+        pickle.dump({"plans": plans, "mine": mine}, f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def FLEET_REQUESTS(W):
+    return [r for r in W.serving_mix(n=16, scale=0.25, steps_scale=0.01) if r["dim"] == 2][:10]
+
+
+def test_two_ranks_shard_a_request_stream(tmp_path):
+    import importlib
+    import pickle
+
+    mp = pytest.importorskip("torch.multiprocessing")
+    world, port = 2, _free_port()
+    mp.start_processes(_fleet_rank, args=(world, port, str(tmp_path)), nprocs=world, join=True, start_method="spawn")
+    sys.path.insert(0, str(ROOT / "tests"))
+    from conftest import load_package
+
+    load_package()
+    S = importlib.import_module("swl_b200.session")
+    W = importlib.import_module("swl_b200.workloads")
+    got = [pickle.load(open(tmp_path / f"fleet{r}.pkl", "rb")) for r in range(world)]
+    assert got[0]["plans"][0] == got[0]["plans"][1] == got[1]["plans"][0]  # one plan everywhere
+    served = {}
+    for r in range(world):
+        assert not set(served) & set(got[r]["mine"])                        # no request served twice
+        served.update(got[r]["mine"])
+    reqs = FLEET_REQUESTS(W)
+    assert sorted(served) == list(range(len(reqs)))                          # every request served once
+    assert all(len(g["mine"]) > 0 for g in got)                              # both ranks have work
+    for i, r in enumerate(reqs):                                             # as if run alone
+        info = S.Simulation2D(r["params"], device=S.MODEL_ONLY).info()
+        assert served[i] == (info["dt"], info["total_steps"], info["nx"], info["nz"])

@@ -131,3 +131,26 @@ def test_engine_async_batches_match_blocking_advance(swl):
     while not b.query()[0]:
         time.sleep(0.001)
     np.testing.assert_array_equal(a.fields(), b.fields())
+
+
+def test_fleet_places_by_budget_and_each_result_is_the_same_alone(mods):
+    # Two device slots on the one GPU of the test box: each slot is its own request loop, the front
+    # places every shot by budget, and every shot's records equal those of the shot run alone.  The
+    # slots' shots never wait on one another (shots are independent), so sharing one GPU is safe.
+    S, V = mods
+    F = importlib.import_module("swl_b200.fleet")
+    shots = mix()
+    fleet = F.Fleet(devices=[0, 0], batch_steps=7)
+    assert fleet.size() == 2 and fleet.device(0) == fleet.device(1) == 0
+    placed = [fleet.submit(p, dim) for dim, p in shots]
+    assert {slot for _, slot in placed} == {0, 1}  # the front spread the mix over both slots
+    fleet.drain()
+    for (dim, p), (sid, slot) in zip(shots, placed):
+        st = fleet.status(sid)
+        assert st["state"] == "done" and st["slot"] == slot
+        for g, w in zip(fleet.records(sid), alone(S, dim, p)):
+            np.testing.assert_array_equal(g, w)
+    for slot in (0, 1):
+        s = fleet.stats(slot)
+        assert s["failed"] == 0 and s["charged"] == 0  # finished shots no longer count
+    fleet.close()
