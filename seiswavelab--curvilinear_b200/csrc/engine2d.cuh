@@ -148,6 +148,8 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // tensor maps of the streaming kernel: stage-input ring boxes of sets 0-3, word boxes of the
     // state / accumulator sets 0-1 and of their compensation sets 4-5, model words without / with J
     CUtensorMap ringMap_[4]{}, pwMap_[2]{}, compMap_[2]{}, modelMap_[2]{};
+    CUtensorMap gslsIn_[4]{}, gslsComp_[2]{}, strengthMap_{}; // GSLS L2 prefetch boxes (per set)
+    DeviceBuffer strengths_;
     // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
     // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
     static constexpr int kSets = k2::kahan<Real>() ? 6 : 4;
@@ -221,6 +223,14 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             p.aMap = pwMap_[a_];
             p.modelMap = modelMap_[stage == 3 ? 1 : 0];
             p.compMap = compMap_[u_];
+            if (mech_) {
+                p.gslsInMap = gslsIn_[in];
+                p.gslsUMap = gslsIn_[u_];
+                p.gslsAMap = gslsIn_[a_];
+                p.gslsCompMap = gslsComp_[u_];
+                p.strengthMap = strengthMap_;
+                p.gslsPrefetch = 1;
+            }
         }
         return p;
     }
@@ -419,10 +429,18 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             m_.wx = g.cpml_width_x;
             m_.wz = g.cpml_width_z;
         }
+        // GSLS relaxation strengths: one allocation of 2L pitched arrays (dP0, dS0, dP1, ...), so one
+        // tensor box covers a row block's strengths
+        if (mech_) strengths_.allocate(2 * std::size_t(mech_) * n * sizeof(Real));
         for (int l = 0; l < mech_; ++l) {
             m_.rates[l] = static_cast<Real>(g.rates[l]);
-            m_.dP[l] = node(g.delta_p[l], 1, "delta_p");
-            m_.dS[l] = node(g.delta_s[l], 1, "delta_s");
+            Real *dp = strengths_.as<Real>() + std::size_t(2 * l) * n, *ds = dp + n;
+            const auto vp = pitched(detail2::convert<Real>(g.delta_p[l], nu, ap, "delta_p"), 1);
+            const auto vs = pitched(detail2::convert<Real>(g.delta_s[l], nu, ap, "delta_s"), 1);
+            check(cudaMemcpy(dp, vp.data(), n * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
+            check(cudaMemcpy(ds, vs.data(), n * sizeof(Real), cudaMemcpyHostToDevice), "upload model");
+            m_.dP[l] = dp;
+            m_.dS[l] = ds;
         }
         m_.fc = fc_;
         sets_.allocate(kSets * std::size_t(fc_) * n * sizeof(Real));
@@ -453,6 +471,15 @@ template <class Real> class TypedEngine2D final : public Engine2D {
                 for (int r = 0; r < 2; ++r) encodeTensorMap3D(&compMap_[r], f64, set_[4 + r], d5, st, w5);
             encodeTensorMap3D(&modelMap_[0], f64, pack_.ptr, d6, st, w5);
             encodeTensorMap3D(&modelMap_[1], f64, pack_.ptr, d6, st, w6);
+            if (mech_) { // L2 prefetch boxes of the GSLS words (fields 5 .. 5+4L) and the strengths
+                const uint32_t gm = uint32_t(4 * mech_ + 1), gs = uint32_t(2 * mech_);
+                const uint64_t dg[3] = {uint64_t(pitch_), uint64_t(nz_), gm}, dst2[3] = {uint64_t(pitch_), uint64_t(nz_), gs};
+                const uint32_t bg[3] = {k2::SW, k2::SB, gm}, bs[3] = {k2::SW, k2::SB, gs};
+                for (int t = 0; t < 4; ++t) encodeTensorMap3D(&gslsIn_[t], f64, set_[t] + 5 * n, dg, st, bg);
+                if (k2::kahan<Real>())
+                    for (int r = 0; r < 2; ++r) encodeTensorMap3D(&gslsComp_[r], f64, set_[4 + r] + 5 * n, dg, st, bg);
+                encodeTensorMap3D(&strengthMap_, f64, strengths_.ptr, dst2, st, bs);
+            }
         }
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
@@ -773,7 +800,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         const int su = u_, sa = a_;
         for (int r = 0; r < 2; ++r) {
             u_ = r, a_ = 1 - r;
-            for (int k = 0; k < 4; ++k) shot.stage[r][k] = args(k), shot.stage[r][k].m.seg = qseg;
+            for (int k = 0; k < 4; ++k) shot.stage[r][k] = args(k), shot.stage[r][k].m.seg = qseg, shot.stage[r][k].gslsPrefetch = 0;
             shot.stage[r][3].partials = partials_.as<k2::Partial>(); // diagnostics fused into stage 3
         }
         u_ = su, a_ = sa;
@@ -941,7 +968,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     int64_t residentBytes() const override {
         int64_t b = 0;
         for (const auto &x : model_) b += x.bytes;
-        for (const auto *x : {&pack_, &sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_}) b += x->bytes;
+        for (const auto *x : {&pack_, &strengths_, &sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_}) b += x->bytes;
         return b;
     }
 };

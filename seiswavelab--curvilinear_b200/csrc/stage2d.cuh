@@ -95,6 +95,13 @@ template <class Real> struct StageArgs {
     // U, A and the compensation terms as 32x8x5 boxes, the model words as 32x8x5 (stages 0-2) or
     // 32x8x6 (stage 3, with J) boxes.
     CUtensorMap ringMap, uMap, aMap, modelMap, compMap;
+    // GSLS only: the per-node words the node arithmetic reads from global memory -- Syy and the
+    // 4L memories of the stage input, of U and of A (and their FP32 compensation), and the 2L
+    // relaxation strengths -- as 32x8x(4L+1) and 32x8x2L boxes.  The CTA's copy thread prefetches a
+    // row block's boxes into L2 with the tensor copies of its stencil rows, two blocks ahead of the
+    // arithmetic, so the per-node loads hit L2 instead of waiting on DRAM.  gslsPrefetch = 0: off.
+    CUtensorMap gslsInMap, gslsUMap, gslsAMap, gslsCompMap, strengthMap;
+    int gslsPrefetch;
 };
 
 // The FP32 form adds each step's increment to the state with compensated (Kahan) summation;
@@ -641,6 +648,12 @@ __device__ __forceinline__ bool mbarWait(uint64_t *bar, unsigned parity) {
         if (mbarTryWait(bar, parity)) return true;
     return false;
 }
+// L2 prefetch of a 3D tensor box (no shared memory, no completion to wait for).
+__device__ __forceinline__ void tmaPrefetch3(const CUtensorMap *map, int x, int y, int z) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];\n" ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x),
+                 "r"(y), "r"(z)
+                 : "memory");
+}
 // 3D tiled tensor copy global -> shared (no multicast), completing on `bar`.
 __device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
     asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
@@ -697,6 +710,12 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
         }
         tmaLoad3(dst + PW_a * T, &p.modelMap, x, y, 0, b);
         if (STAGE == 3 && kahan<Real>()) tmaLoad3(dst + PW_C * T, &p.compMap, x, y, 0, b);
+        if (MECH > 0 && p.gslsPrefetch) {
+            tmaPrefetch3(&p.gslsInMap, x, y, 0);
+            if (STAGE > 0) tmaPrefetch3(&p.gslsUMap, x, y, 0), tmaPrefetch3(&p.gslsAMap, x, y, 0);
+            if (STAGE == 3 && kahan<Real>()) tmaPrefetch3(&p.gslsCompMap, x, y, 0);
+            tmaPrefetch3(&p.strengthMap, x, y, 0);
+        }
     };
     if (tid == 0) {
         stop = 0;
