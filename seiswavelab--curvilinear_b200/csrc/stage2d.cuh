@@ -186,11 +186,28 @@ template <class Real, bool EXACT, int STAGE> struct StreamNode {
     const Real *col; // ring chunk 0, field 0, row 0, this node's column
     const Real *pw;  // this node's per-node words (stride STREAM_THREADS)
     long long q;
-    int centre;      // ring row (0..RING-1) of this node
-    __device__ __forceinline__ Real at(int f, int dx, int dz) const {
+    // Offset in the ring of the row dz = -3..3 away from this node's (chunk and row within the
+    // chunk, wrapped): set once per row block (it is the same for a whole warp), so that every tap
+    // is one shared-memory load at a constant offset from one of seven bases.
+    int row[7];
+    int centre; // ring row (0..RING-1) of this node
+    __device__ __forceinline__ void setCentre(int c) {
+        centre = c;
+#pragma unroll
+        for (int d = -3; d <= 3; ++d) {
+            int s = c + d; // one wrap at most
+            s = s < 0 ? s + RING : s >= RING ? s - RING : s;
+            const unsigned u = unsigned(s);
+            row[d + 3] = int((u / unsigned(SB)) * CH + (u % unsigned(SB)) * RC);
+        }
+    }
+    // dz a compile-time constant (the stencil taps): a load from one of the seven row bases
+    __device__ __forceinline__ Real at(int f, int dx, int dz) const { return col[row[dz + 3] + f * RF + dx]; }
+    // dz known only at run time (the traction-image taps near the surface): the row is computed
+    __device__ __forceinline__ Real atRow(int f, int dx, int dz) const {
         int s = centre + dz; // dz in [-3, 3]: one wrap at most
         s = s < 0 ? s + RING : s >= RING ? s - RING : s;
-        const unsigned u = unsigned(s); // non-negative: the chunk and row are a shift and a mask
+        const unsigned u = unsigned(s);
         return col[(u / unsigned(SB)) * CH + f * RF + (u % unsigned(SB)) * RC + dx];
     }
     __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
@@ -261,7 +278,7 @@ template <class Real, class S>
 __device__ __forceinline__ Real flux(const Mesh<Real> &m, const S &t, int dx, int dz, int axis, int comp) {
     const long long qq = t.q + dx + (long long)dz * m.pitch;
     const Real x = axis ? ld(m.a + qq) : Real(1), z = axis ? ld(m.b + qq) : Real(0);
-    return ld(m.jac + qq) * (x * t.at(comp ? 4 : 2, dx, dz) + z * t.at(comp ? 3 : 4, dx, dz));
+    return ld(m.jac + qq) * (x * t.atRow(comp ? 4 : 2, dx, dz) + z * t.atRow(comp ? 3 : 4, dx, dz));
 }
 
 // Conservative traction-image momentum near the surface (PointKernels2D.hpp:94-120):
@@ -745,7 +762,7 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
             s.pw = pw + (blk & 1) * (PW * T) + tid;
             s.q = i + m.xoff + (long long)m.pitch * k;
             const int c = SB * (blk % 3) + wy + 3; // ring row of row k (rows counted from zb)
-            s.centre = c >= RING ? c - RING : c;
+            s.setCentre(c >= RING ? c - RING : c);
             stageNode<Real, DX, DZ, MECH, STAGE, FULL>(p, s, i, k, diag, withDiag);
         }
         __syncthreads(); // block blk's ring chunk and word buffer are free
