@@ -535,7 +535,10 @@ def gpu_arm(args):
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                             "traffic": traffic_from_profiles(args.workload, "f64" if precision == 0 else "f32"),
                             "kernel": "fused RK stage kernels (4 per step)", "peak_source": peak_src,
-                            "bytes_per_step": prof["bytes_per_step"], "stage_ms_per_step": stage_ms}}
+                            "bytes_per_step": prof["bytes_per_step"], "stage_ms_per_step": stage_ms,
+                            "bytes_rule": "17F + 4M per node-step plus 17 words per CFS-PML memory (algorithmic)",
+                            "kahan_bytes_per_step": prof["extra_bytes_per_step"],
+                            "frac_with_kahan": (prof["bytes_per_step"] + prof["extra_bytes_per_step"]) / (stage_ms * 1e-3) / 1e9 / peak}}
         return sim, res
 
     sim64, r64 = measure(0)

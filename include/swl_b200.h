@@ -171,7 +171,10 @@ typedef struct swl_profile {
     double stage_ms[4]; /* mean duration of each RK-stage kernel */
     double stats_ms, verdict_ms, step_ms;
     int64_t steps, launches_per_step;
-    double bytes_per_step; /* algorithmic HBM bytes of the four stage kernels per step */
+    double bytes_per_step;  /* algorithmic HBM bytes of one step: 17 F + 4 M per node (F, M: state and
+                             * model bytes of a node) plus 17 words per CFS-PML memory */
+    double extra_bytes_per_step; /* bytes the FP32 form moves beyond those: its Kahan compensation
+                                  * terms (and, in 3D, U) in the last stage; 0 in FP64 */
 } swl_profile;
 swl_status swl2d_profile(swl2d_engine *engine, int32_t first, int32_t count, double dt, double frequency, double scale,
                          swl_profile *out);

@@ -77,12 +77,12 @@ class Diag3D(C.Structure):
 class Profile(C.Structure):
     _fields_ = [("stage_ms", C.c_double * 4), ("stats_ms", C.c_double), ("verdict_ms", C.c_double),
                 ("step_ms", C.c_double), ("steps", C.c_int64), ("launches_per_step", C.c_int64),
-                ("bytes_per_step", C.c_double)]
+                ("bytes_per_step", C.c_double), ("extra_bytes_per_step", C.c_double)]
 
     def as_dict(self) -> dict:
         return {"stage_ms": list(self.stage_ms), "stats_ms": self.stats_ms, "verdict_ms": self.verdict_ms,
                 "step_ms": self.step_ms, "steps": self.steps, "launches_per_step": self.launches_per_step,
-                "bytes_per_step": self.bytes_per_step}
+                "bytes_per_step": self.bytes_per_step, "extra_bytes_per_step": self.extra_bytes_per_step}
 
 
 class Layout2D(C.Structure):

@@ -259,11 +259,19 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // Algorithmic HBM bytes of the four stage kernels of one step: 17 F + 4 M per physical
     // node (stage reads/writes of U, A, S and the per-node model arrays a, b, rho, lambda, mu
     // and the GSLS strengths) plus 17 values per CFS-PML memory.
+    // Algorithmic HBM bytes of one step: 17 F + 4 M per physical node (stage 0 reads U and writes
+    // S and A: 3F; stages 1-2 read S, U, A and write S, A: 5F each; stage 3 reads S, U, A and writes
+    // the new state: 4F; every stage reads the model words M), plus 17 words per ADE memory.
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.nz - 6);
-        // FP32 adds the read and write of the compensation terms in stage 3: 19 F + 4 M
-        const double F = fc_ * s, M = (5 + 2 * mech_) * s, words = k2::kahan<Real>() ? 19 : 17;
-        return points * (words * F + 4 * M) + double(pcount_) * words * s;
+        const double F = fc_ * s, M = (5 + 2 * mech_) * s;
+        return points * (17 * F + 4 * M) + double(pcount_) * 17 * s;
+    }
+    // FP32 only: the compensation terms read and written by stage 3 (2 F, and 2 words per memory).
+    double extraBytesPerStep() const {
+        if (!k2::kahan<Real>()) return 0;
+        const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.nz - 6);
+        return points * 2 * fc_ * s + double(pcount_) * 2 * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -610,6 +618,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         out.steps = hostClock_.accepted;
         out.launches_per_step = 5;
         out.bytes_per_step = bytesPerStep();
+        out.extra_bytes_per_step = extraBytesPerStep();
         const int accepted = hostClock_.accepted;
         u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
         a_ = 1 - u_;

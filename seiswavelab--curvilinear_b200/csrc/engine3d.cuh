@@ -171,14 +171,20 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         }
         std::swap(u_, a_);
     }
-    // Algorithmic HBM bytes of the four stage kernels of one step: 16 F + 4 M per physical node
-    // (the accumulator carries the partial state sum, so the last stage does not read U); M =
-    // nine metrics plus lambda, mu, rho when the material varies.  FP32 reads U and reads and
-    // writes the compensation terms in the last stage: 19 F + 4 M.
+    // Algorithmic HBM bytes of one step, the fused classic-RK4 count 17 F + 4 M per physical node;
+    // M = nine metrics plus lambda, mu, rho when the material varies.  The FP64 kernels move one F
+    // less (the accumulator carries the partial state sum, so the last stage does not read U).
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
         const double F = 9 * s, M = (m_.mlambda ? 12 : 9) * s;
-        return points * ((k2::kahan<Real>() ? 19 : 16) * F + 4 * M);
+        return points * (17 * F + 4 * M);
+    }
+    // FP32 only: the last stage's compensation terms read and written (2 F); it also reads U, which
+    // the count above already holds.
+    double extraBytesPerStep() const {
+        if (!k2::kahan<Real>()) return 0;
+        const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
+        return points * 2 * 9 * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -402,6 +408,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         out.steps = hostClock_.accepted;
         out.launches_per_step = 6;
         out.bytes_per_step = bytesPerStep();
+        out.extra_bytes_per_step = extraBytesPerStep();
         const int accepted = hostClock_.accepted;
         u_ = (accepted % 2 == 0) ? u0 : 1 - u0;
         a_ = 1 - u_;
