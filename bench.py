@@ -68,6 +68,9 @@ def workload(name: str, precision: int) -> tuple[dict, str]:
         return W.gsls_medium(precision=precision), "2D GSLS (3 mechanisms) 2001x801, 40 m sinusoidal terrain, 30-cell CFS-PML"
     if name == "elastic_3d":
         return W.elastic_3d(precision=precision), "3D nine-field elastic 400x288x200 h=10 m, DEM terrain, 3 layers, 20-cell sponge"
+    if name == "elastic_3d_cpml":
+        return (W.elastic_3d(precision=precision, absorber=1),
+                "3D nine-field elastic 400x288x200 h=10 m, DEM terrain, 3 layers, 20-cell CFS-PML slabs")
     if name == "small_3d":
         return (W.elastic_3d(precision=precision, nx=200, ny=144, nz=100),
                 "3D nine-field elastic 200x144x100 (profiling size of elastic_3d)")
@@ -510,7 +513,7 @@ def gpu_arm(args):
     swl = load_package()
     import importlib
     S = importlib.import_module("swl_b200.session")
-    dim = 3 if args.workload in ("elastic_3d", "small_3d") else 2
+    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "small_3d") else 2
     Sim = S.Simulation2D if dim == 2 else S.Simulation3D
     peak, peak_src = measured_hbm_peak()
 
@@ -613,7 +616,7 @@ def reference_arm(args):
     if rank != 0:
         return
     load_package()
-    dim = 3 if args.workload in ("elastic_3d", "small_3d") else 2
+    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "small_3d") else 2
     params, desc = workload(args.workload, 0)
     steps = min(args.steps, args.cpu_steps)
     base = cpu_baseline(params, dim, steps, min(args.warmup, 2))
@@ -636,7 +639,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", choices=["swl", "reference"], default="swl")
     ap.add_argument("--workload", default="curvilinear_large",
-                    choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d", "small_3d"])
+                    choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d", "elastic_3d_cpml",
+                             "small_3d"])
     ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA engine")

@@ -273,6 +273,13 @@ typedef struct swl_mesh3d {
     double source_direction[3], source_amplitude;
     const double *source_gradient[3];
     int32_t precision;
+    /* CFS-PML ADE (no counterpart in the reference's 3D path, which has only the sponge):
+     * (d, kappa, alpha) per computational index along x, y and z, the slab widths (x and y on both
+     * sides, z at the bottom) and the memory count 6*(2wx*ny*nz + 2wy*nx*nz + wz*nx*ny) over the
+     * computational grid; cpml_count = 0: none.  Memories are read and written as field -1. */
+    const double *cpml_x, *cpml_y, *cpml_z;
+    int32_t cpml_width_x, cpml_width_y, cpml_width_z;
+    int64_t cpml_count;
 } swl_mesh3d;
 
 typedef struct swl_diag3d {

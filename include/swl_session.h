@@ -108,6 +108,10 @@ typedef struct swl_params3d {
     double absorbing_strength;
     int32_t device_geometry; /* 1: build the FP64 node geometry on the session's GPU (swl3d_build_geometry) */
     const char *const *layer_names; /* n_layers UTF-8 names (MaterialLayer3D::name), or null: unnamed */
+    /* 0: the reference's sponge; 1: CFS-PML ADE slabs of absorbing_cells widths (x, y both sides, z at the
+     * bottom) with the 2D profiles per axis.  No counterpart in the reference's 3D path. */
+    int32_t absorber;
+    double cpml_reflection, cpml_kappa_max, cpml_frequency; /* frequency 0: the source frequency */
 } swl_params3d;
 
 typedef struct swl_info3d {
@@ -130,7 +134,8 @@ swl_status swl3d_session_info(const swl3d_session *s, swl_info3d *out);
 swl_status swl3d_session_records(const swl3d_session *s, double *vx, double *vy, double *vz);
 swl_status swl3d_session_snapshot(swl3d_session *s, int32_t field, double *out);
 /* "coordinates", "metrics", "jacobian", "normals", "source", "damping", "sourceGradient0..2",
- * "materialLambda", "materialMu", "materialDensity". */
+ * "materialLambda", "materialMu", "materialDensity"; with CFS-PML "cpmlX", "cpmlY", "cpmlZ" (d, kappa,
+ * alpha per computational index) and "cpmlShape" (wx, wy, wz, memory count). */
 swl_status swl3d_session_model(const swl3d_session *s, const char *name, double *out, int64_t *n);
 swl3d_engine *swl3d_session_engine(swl3d_session *s);
 /* writeVts (src/three_d/VtsWriter.cpp) of the current state: the physical nodes as a VTK

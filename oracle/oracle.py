@@ -45,6 +45,8 @@ class Mesh3D(C.Structure):
         ("metrics", _dp), ("normals", _dp), ("jacobian", _dp), ("source", _dp), ("damping", _dp),
         ("material_lambda", _dp), ("material_mu", _dp), ("material_density", _dp),
         ("source_direction", C.c_double * 3), ("source_amplitude", C.c_double), ("source_gradient", _dp * 3),
+        ("cpml_x", _dp), ("cpml_y", _dp), ("cpml_z", _dp), ("cpml_width_x", C.c_int32), ("cpml_width_y", C.c_int32),
+        ("cpml_width_z", C.c_int32), ("cpml_count", C.c_int64),
     ]
 
 
@@ -82,9 +84,9 @@ class Oracle:
         L.swlo2d_rhs.argtypes = [C.POINTER(Mesh2D), C.POINTER(_dp), _dp, C.POINTER(_dp), _dp, C.c_double, C.c_int,
                                  C.c_int]
         L.swlo2d_project.argtypes = [C.POINTER(Mesh2D), C.POINTER(_dp)]
-        L.swlo3d_run.argtypes = [C.POINTER(Mesh3D), _dp, C.c_int, C.c_int, C.c_double, C.c_double,
+        L.swlo3d_run.argtypes = [C.POINTER(Mesh3D), _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.POINTER(C.c_int64), C.c_int, _dp, _dp, _dp]
-        L.swlo3d_rhs.argtypes = [C.POINTER(Mesh3D), C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int, C.c_int]
+        L.swlo3d_rhs.argtypes = [C.POINTER(Mesh3D), C.POINTER(_dp), _dp, C.POINTER(_dp), _dp, C.c_double, C.c_int, C.c_int]
 
     # -- 2D ---------------------------------------------------------------------------------
     @staticmethod
@@ -172,28 +174,37 @@ class Oracle:
             g.source_direction[a] = float(m.get("sourceDirection", (0, 0, 1))[a])
             g.source_gradient[a] = arr(f"sourceGradient{a}")
         g.source_amplitude = float(m["sourceAmplitude"])
+        # CFS-PML (keys as the 3D session's model names them; absent: no CFS-PML)
+        g.cpml_x, g.cpml_y, g.cpml_z = arr("cpmlX"), arr("cpmlY"), arr("cpmlZ")
+        g.cpml_width_x, g.cpml_width_y = int(m.get("cpmlWidthX", 0)), int(m.get("cpmlWidthY", 0))
+        g.cpml_width_z, g.cpml_count = int(m.get("cpmlWidthZ", 0)), int(m.get("cpmlCount", 0))
         return g, keep
 
-    def run3d(self, m: dict, steps: int, first: int = 0, state=None, receivers=()):
+    def run3d(self, m: dict, steps: int, first: int = 0, state=None, receivers=(), pml=None, with_pml=False):
         g, keep = self.mesh3d(m)
         n = g.count
         state = np.zeros(9 * n) if state is None else np.array(state, dtype=np.float64, copy=True)
+        pml = np.zeros(max(g.cpml_count, 1)) if pml is None else np.array(pml, dtype=np.float64, copy=True)
         rec = np.ascontiguousarray(receivers, dtype=np.int64)
         tr = [np.zeros((len(rec), steps)) for _ in range(3)]
-        rc = self.lib.swlo3d_run(C.byref(g), _ptr(state), first, steps, float(m["dt"]), float(m["frequency"]),
+        rc = self.lib.swlo3d_run(C.byref(g), _ptr(state), _ptr(pml), first, steps, float(m["dt"]), float(m["frequency"]),
                                  rec.ctypes.data_as(C.POINTER(C.c_int64)), len(rec), *(_ptr(t) for t in tr))
         if rc:
             raise MemoryError("oracle 3D run failed")
+        if with_pml:
+            return state.reshape(9, n), tr, pml[: g.cpml_count]
         return state.reshape(9, n), tr
 
-    def rhs3d(self, m: dict, state, source, step, stage):
+    def rhs3d(self, m: dict, state, source, step, stage, pml=None):
         g, keep = self.mesh3d(m)
         n = g.count
         state = np.ascontiguousarray(state, dtype=np.float64).reshape(9, n)
         out = np.zeros((9, n))
+        pml = np.ascontiguousarray(pml if pml is not None and len(pml) else np.zeros(max(g.cpml_count, 1)), dtype=np.float64)
+        out_pml = np.zeros(max(g.cpml_count, 1))
         ins = (_dp * 9)(*[_ptr(state[f]) for f in range(9)])
         outs = (_dp * 9)(*[_ptr(out[f]) for f in range(9)])
-        self.lib.swlo3d_rhs(C.byref(g), ins, outs, float(source), step, stage)
+        self.lib.swlo3d_rhs(C.byref(g), ins, _ptr(pml), outs, _ptr(out_pml), float(source), step, stage)
         return out
 
 

@@ -318,10 +318,52 @@ void swlo3d_project(const swlo_mesh3d *g, double *const *f) {
         }
 }
 
+/* ---- 3D CFS-PML (no counterpart in the reference, whose 3D path has only the quadratic sponge,
+ * include/Seis3D/AbsorbingBoundary3D.hpp:17-21).  The 2D ADE of src/two_d/PointKernels2D.hpp:50-64
+ * carried over axis by axis: slabs of width wx on both x sides, wy on both y sides, wz at the
+ * bottom; six memories per active axis of a node -- the axis derivative of Vx, Vy, Vz (0..2) and
+ * the axis part of the three momentum components (3..5).  A node in any slab sums its momentum
+ * per axis (x/rho + y/rho + z/rho, each stretched where the axis is active), as the 2D ADE does;
+ * a node outside every slab keeps the sponge-free form. */
+static ptrdiff_t pml_slot3(const swlo_mesh3d *g, ptrdiff_t q, int axis) {
+    if (!g->cpml_count) return -1;
+    const ptrdiff_t plane = (ptrdiff_t)g->nx * g->ny;
+    const int i = (int)(q % g->nx) - 3, j = (int)((q / g->nx) % g->ny) - 3, k = (int)(q / plane) - 3;
+    const int nx = g->nx - 6, ny = g->ny - 6, nz = g->nz - 6;
+    const int wx = g->cpml_width_x, wy = g->cpml_width_y, wz = g->cpml_width_z;
+    const ptrdiff_t c0 = 6 * (ptrdiff_t)2 * wx * ny * nz, c1 = 6 * (ptrdiff_t)2 * wy * nx * nz;
+    if (axis == 0) {
+        const int s = i < wx ? i : i >= nx - wx ? wx + i - (nx - wx) : -1;
+        return s < 0 ? -1 : 6 * (((ptrdiff_t)k * ny + j) * 2 * wx + s);
+    }
+    if (axis == 1) {
+        const int s = j < wy ? j : j >= ny - wy ? wy + j - (ny - wy) : -1;
+        return s < 0 ? -1 : c0 + 6 * (((ptrdiff_t)k * 2 * wy + s) * nx + i);
+    }
+    return k < nz - wz ? -1 : c0 + c1 + 6 * (((ptrdiff_t)(k - (nz - wz)) * ny + j) * nx + i);
+}
+/* psi' = -(d/kappa + alpha) psi - d/kappa^2 * derivative; returns derivative/kappa + psi
+ * (PointKernels2D.hpp:57-64 per axis). */
+static double stretched3(const swlo_mesh3d *g, const double *in_pml, double *out_pml, ptrdiff_t q, int axis, int field,
+                         double derivative) {
+    const ptrdiff_t slot = pml_slot3(g, q, axis);
+    if (slot < 0) return derivative;
+    const ptrdiff_t plane = (ptrdiff_t)g->nx * g->ny;
+    const int at = axis == 0 ? (int)(q % g->nx) - 3 : axis == 1 ? (int)((q / g->nx) % g->ny) - 3 : (int)(q / plane) - 3;
+    const double *pr = (axis == 0 ? g->cpml_x : axis == 1 ? g->cpml_y : g->cpml_z) + 3 * at;
+    const double d = pr[0], kappa = pr[1], alpha = pr[2], psi = in_pml[slot + field];
+    out_pml[slot + field] = -(d / kappa + alpha) * psi - d / (kappa * kappa) * derivative;
+    return derivative / kappa + psi;
+}
+static int in_slab3(const swlo_mesh3d *g, ptrdiff_t q) {
+    return g->cpml_count && (pml_slot3(g, q, 0) >= 0 || pml_slot3(g, q, 1) >= 0 || pml_slot3(g, q, 2) >= 0);
+}
+
 /* src/three_d/PointKernels3D.hpp:52-66 -- surface zeta-derivative of the velocity from
- * the local traction-free solve. */
+ * the local traction-free solve; `xy` (3 velocities x (xi, eta)) are the CFS-PML-stretched
+ * derivatives when the node lies in a slab, else null. */
 static void surface_derivative3(const swlo_mesh3d *g, double *const *w, ptrdiff_t q, double *res, int dx_dir,
-                                int dy_dir) {
+                                int dy_dir, const double *xy) {
     const double *m = g->metrics + 9 * q;
     const double lambda = lam3(g, q), mu = mu3(g, q);
     const double c[3] = {m[6], m[7], m[8]};
@@ -329,7 +371,7 @@ static void surface_derivative3(const swlo_mesh3d *g, double *const *w, ptrdiff_
     const double n[3] = {c[0] / len, c[1] / len, c[2] / len};
     double gr[9] = {0}, t[3] = {0, 0, 0};
     for (int v = 0; v < 3; ++v) {
-        const double dx = d3(w[v], g, q, 0, dx_dir, -1), dy = d3(w[v], g, q, 1, dy_dir, -1);
+        const double dx = xy ? xy[2 * v] : d3(w[v], g, q, 0, dx_dir, -1), dy = xy ? xy[2 * v + 1] : d3(w[v], g, q, 1, dy_dir, -1);
         for (int a = 0; a < 3; ++a) gr[3 * v + a] = m[a] * dx + m[3 + a] * dy;
     }
     const double trace = gr[0] + gr[4] + gr[8];
@@ -348,10 +390,12 @@ static double traction_flux(const swlo_mesh3d *g, double *const *w, ptrdiff_t q,
     return g->jacobian[q] * v;
 }
 
-/* src/three_d/PointKernels3D.hpp:73-91 */
-static double surface_momentum(const swlo_mesh3d *g, double *const *w, ptrdiff_t q, int comp, const int *dirs, int depth) {
+/* src/three_d/PointKernels3D.hpp:73-91; `only` >= 0: that axis's part alone (the CFS-PML split). */
+static double surface_momentum(const swlo_mesh3d *g, double *const *w, ptrdiff_t q, int comp, const int *dirs, int depth,
+                               int only) {
     double sum = 0;
     for (int axis = 0; axis < 3; ++axis) {
+        if (only >= 0 && axis != only) continue;
         int off[5];
         double c[5];
         const int n = stencil(dirs[axis], -1, off, c);
@@ -373,27 +417,51 @@ static double surface_momentum(const swlo_mesh3d *g, double *const *w, ptrdiff_t
     return sum / (g->h * g->jacobian[q] * rho3(g, q));
 }
 
-/* src/three_d/PointKernels3D.hpp:92-112 -- nine-field right-hand side at one node. */
-static void rhs3_point(const swlo_mesh3d *g, double *const *w, double *const *out, ptrdiff_t q, double source,
-                       int step, int stage) {
+/* src/three_d/PointKernels3D.hpp:92-112 -- nine-field right-hand side at one node, with the
+ * CFS-PML terms above for the nodes in a slab. */
+static void rhs3_point(const swlo_mesh3d *g, double *const *w, const double *in_pml, double *const *out, double *out_pml,
+                       ptrdiff_t q, double source, int step, int stage) {
+    static const int F[3][3] = {{3, 6, 7}, {6, 4, 8}, {7, 8, 5}};
     const double lambda = lam3(g, q), mu = mu3(g, q), density = rho3(g, q);
-    double gr[9][3];
+    double gr[9][3], D[9][3];
     const double *m = g->metrics + 9 * q;
     const int depth = (int)(q / ((ptrdiff_t)g->nx * g->ny)) - 3;
     const int dirs[3] = {swlo_direction(step, stage, 0), swlo_direction(step, stage, 1), swlo_direction(step, stage, 2)};
+    const int split = in_slab3(g, q);
+    for (int f = 0; f < 9; ++f)
+        for (int a = 0; a < 2; ++a) D[f][a] = d3(w[f], g, q, a, dirs[a], -1);
+    if (split) /* the velocities' xi and eta derivatives, stretched before the surface solve */
+        for (int v = 0; v < 3; ++v)
+            for (int a = 0; a < 2; ++a) D[v][a] = stretched3(g, in_pml, out_pml, q, a, v, D[v][a]);
     double dzs[3] = {0, 0, 0};
-    if (depth == 0) surface_derivative3(g, w, q, dzs, dirs[0], dirs[1]);
-    for (int f = 0; f < 9; ++f) {
-        double d[3];
-        for (int a = 0; a < 3; ++a)
-            d[a] = f < 3 && a == 2 && depth == 0 ? dzs[f] : d3(w[f], g, q, a, dirs[a], f < 3 && a == 2 ? depth : -1);
-        for (int a = 0; a < 3; ++a) gr[f][a] = m[a] * d[0] + m[3 + a] * d[1] + m[6 + a] * d[2];
+    if (depth == 0) {
+        const double xy[6] = {D[0][0], D[0][1], D[1][0], D[1][1], D[2][0], D[2][1]};
+        surface_derivative3(g, w, q, dzs, dirs[0], dirs[1], split ? xy : 0);
     }
-    out[0][q] = (gr[3][0] + gr[6][1] + gr[7][2]) / density;
-    out[1][q] = (gr[6][0] + gr[4][1] + gr[8][2]) / density;
-    out[2][q] = (gr[7][0] + gr[8][1] + gr[5][2]) / density;
-    if (depth <= (dirs[2] ? 3 : 1))
-        for (int a = 0; a < 3; ++a) out[a][q] = surface_momentum(g, w, q, a, dirs, depth);
+    for (int f = 0; f < 9; ++f) {
+        D[f][2] = f < 3 && depth == 0 ? dzs[f] : d3(w[f], g, q, 2, dirs[2], f < 3 ? depth : -1);
+        if (split && f < 3) D[f][2] = stretched3(g, in_pml, out_pml, q, 2, f, D[f][2]);
+        for (int a = 0; a < 3; ++a) gr[f][a] = m[a] * D[f][0] + m[3 + a] * D[f][1] + m[6 + a] * D[f][2];
+    }
+    const int near = depth <= (dirs[2] ? 3 : 1);
+    if (!split) {
+        out[0][q] = (gr[3][0] + gr[6][1] + gr[7][2]) / density;
+        out[1][q] = (gr[6][0] + gr[4][1] + gr[8][2]) / density;
+        out[2][q] = (gr[7][0] + gr[8][1] + gr[5][2]) / density;
+        if (near)
+            for (int a = 0; a < 3; ++a) out[a][q] = surface_momentum(g, w, q, a, dirs, depth, -1);
+    } else {
+        for (int c = 0; c < 3; ++c) {
+            double part[3];
+            for (int a = 0; a < 3; ++a) {
+                const double *ma = m + 3 * a; /* d(xi_a)/d(x, y, z) */
+                part[a] = near ? surface_momentum(g, w, q, c, dirs, depth, a)
+                               : (ma[0] * D[F[c][0]][a] + ma[1] * D[F[c][1]][a] + ma[2] * D[F[c][2]][a]) / density;
+            }
+            out[c][q] = stretched3(g, in_pml, out_pml, q, 0, 3 + c, part[0]) + stretched3(g, in_pml, out_pml, q, 1, 3 + c, part[1]) +
+                        stretched3(g, in_pml, out_pml, q, 2, 3 + c, part[2]);
+        }
+    }
     for (int a = 0; a < 3; ++a)
         out[a][q] += source * (g->source_gradient[a] ? g->source_gradient[a][q] : g->source[q] * g->source_direction[a]) *
                      (g->density / density);
@@ -408,12 +476,14 @@ static void rhs3_point(const swlo_mesh3d *g, double *const *w, double *const *ou
 }
 
 /* src/three_d/CurvilinearSolver.cpp:70-89 */
-void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, double *const *out, double source, int step, int stage) {
+void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, const double *in_pml, double *const *out, double *out_pml,
+                double source, int step, int stage) {
     for (int f = 0; f < 9; ++f) memset(out[f], 0, sizeof(double) * (size_t)g->count);
+    if (g->cpml_count) memset(out_pml, 0, sizeof(double) * (size_t)g->cpml_count);
     for (int k = 3; k < g->nz - 3; ++k)
         for (int j = 3; j < g->ny - 3; ++j)
             for (int i = 3; i < g->nx - 3; ++i)
-                rhs3_point(g, in, out, i + (ptrdiff_t)g->nx * (j + (ptrdiff_t)g->ny * k), source, step, stage);
+                rhs3_point(g, in, in_pml, out, out_pml, i + (ptrdiff_t)g->nx * (j + (ptrdiff_t)g->ny * k), source, step, stage);
 }
 
 /* src/three_d/CurvilinearSolver.cpp:75-77 -- Ricker force/moment per unit volume. */
@@ -430,11 +500,13 @@ static void combine3(double *out, const double *base, const double *a, double wa
         out[q] = base[q] + wa * a[q] + (b ? wb * b[q] : 0.0) + (c ? wc * c[q] : 0.0) + (d ? wd * d[q] : 0.0);
 }
 
-/* src/three_d/CurvilinearSolver.cpp:445-513 (CPU branch :460-473). */
-int swlo3d_run(const swlo_mesh3d *g, double *state, int first, int steps, double dt, double frequency,
+/* src/three_d/CurvilinearSolver.cpp:445-513 (CPU branch :460-473); the CFS-PML memories follow
+ * the fields' RK sums. */
+int swlo3d_run(const swlo_mesh3d *g, double *state, double *pml, int first, int steps, double dt, double frequency,
                const int64_t *receivers, int nreceivers, double *trace_vx, double *trace_vy, double *trace_vz) {
-    const size_t n = (size_t)g->count;
-    double *mem = (double *)calloc(6 * 9 * n, sizeof(double));
+    const size_t n = (size_t)g->count, np = (size_t)(pml ? g->cpml_count : 0);
+    if (g->cpml_count && !pml) return -1;
+    double *mem = (double *)calloc(6 * 9 * n + 6 * (np + 1), sizeof(double));
     if (!mem) return -1;
     double *st[9], *base[9], *k[4][9], *sg[9];
     for (int f = 0; f < 9; ++f) {
@@ -443,22 +515,29 @@ int swlo3d_run(const swlo_mesh3d *g, double *state, int first, int steps, double
         for (int s = 0; s < 4; ++s) k[s][f] = mem + (size_t)(1 + s) * 9 * n + f * n;
         sg[f] = mem + 5 * 9 * n + f * n;
     }
+    double *pb = mem + 6 * 9 * n, *pk[4], *ps = pb + 5 * (np + 1);
+    for (int s = 0; s < 4; ++s) pk[s] = pb + (size_t)(1 + s) * (np + 1);
     for (int it = 0; it < steps; ++it) {
         const int step = first + it;
         memcpy(mem, state, sizeof(double) * 9 * n);
+        if (np) memcpy(pb, pml, sizeof(double) * np);
         const double t = step * dt;
-        swlo3d_rhs(g, st, k[0], source3(g, t, frequency), step, 0);
+        swlo3d_rhs(g, st, pml, k[0], pk[0], source3(g, t, frequency), step, 0);
         for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[0][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
+        if (np) combine3(ps, pb, pk[0], 0.5 * dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
-        swlo3d_rhs(g, sg, k[1], source3(g, t + 0.5 * dt, frequency), step, 1);
+        swlo3d_rhs(g, sg, ps, k[1], pk[1], source3(g, t + 0.5 * dt, frequency), step, 1);
         for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[1][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
+        if (np) combine3(ps, pb, pk[1], 0.5 * dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
-        swlo3d_rhs(g, sg, k[2], source3(g, t + 0.5 * dt, frequency), step, 2);
+        swlo3d_rhs(g, sg, ps, k[2], pk[2], source3(g, t + 0.5 * dt, frequency), step, 2);
         for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[2][f], dt, 0, 0, 0, 0, 0, 0, n);
+        if (np) combine3(ps, pb, pk[2], dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
-        swlo3d_rhs(g, sg, k[3], source3(g, t + dt, frequency), step, 3);
+        swlo3d_rhs(g, sg, ps, k[3], pk[3], source3(g, t + dt, frequency), step, 3);
         for (int f = 0; f < 9; ++f)
             combine3(st[f], base[f], k[0][f], dt / 6.0, k[1][f], dt / 3.0, k[2][f], dt / 3.0, k[3][f], dt / 6.0, n);
+        if (np) combine3(pml, pb, pk[0], dt / 6.0, pk[1], dt / 3.0, pk[2], dt / 3.0, pk[3], dt / 6.0, np);
         swlo3d_project(g, st);
         for (int r = 0; r < nreceivers; ++r) {
             const int64_t q = receivers[r];

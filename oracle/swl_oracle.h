@@ -39,6 +39,12 @@ typedef struct swlo_mesh3d {
     const double *material_lambda, *material_mu, *material_density; /* null for a uniform model */
     double source_direction[3], source_amplitude;
     const double *source_gradient[3];
+    /* CFS-PML ADE in 3D (the reference has the sponge only; this build extends its 2D ADE, see
+     * swl_oracle.c): (d, kappa, alpha) per computational index along x, y and z, the slab widths
+     * (x and y on both sides, z at the bottom) and the compact memory count (0: no CFS-PML). */
+    const double *cpml_x, *cpml_y, *cpml_z;
+    int32_t cpml_width_x, cpml_width_y, cpml_width_z;
+    int64_t cpml_count;
 } swlo_mesh3d;
 
 int swlo_direction(int step, int stage, int axis);
@@ -55,11 +61,12 @@ int swlo2d_run(const swlo_mesh2d *g, double *state, double *pml, int first, int 
                double frequency, double scale, const int64_t *receivers, int nreceivers, double *trace_vx,
                double *trace_vz);
 
-void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, double *const *out, double source, int step,
-                int stage);
+void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, const double *in_pml, double *const *out, double *out_pml,
+                double source, int step, int stage);
 void swlo3d_project(const swlo_mesh3d *g, double *const *fields);
-/* state: 9*count doubles.  traces: receivers x steps for Vx, Vy, Vz. */
-int swlo3d_run(const swlo_mesh3d *g, double *state, int first, int steps, double dt, double frequency,
+/* state: 9*count doubles; pml: cpml_count doubles (null without CFS-PML).  traces: receivers x
+ * steps for Vx, Vy, Vz. */
+int swlo3d_run(const swlo_mesh3d *g, double *state, double *pml, int first, int steps, double dt, double frequency,
                const int64_t *receivers, int nreceivers, double *trace_vx, double *trace_vy, double *trace_vz);
 
 #ifdef __cplusplus

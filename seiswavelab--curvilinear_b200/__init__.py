@@ -65,6 +65,8 @@ class Mesh3D(C.Structure):
         ("material_lambda", _dp), ("material_mu", _dp), ("material_density", _dp),
         ("source_direction", C.c_double * 3), ("source_amplitude", C.c_double), ("source_gradient", _dp * 3),
         ("precision", C.c_int32),
+        ("cpml_x", _dp), ("cpml_y", _dp), ("cpml_z", _dp), ("cpml_width_x", C.c_int32), ("cpml_width_y", C.c_int32),
+        ("cpml_width_z", C.c_int32), ("cpml_count", C.c_int64),
     ]
 
 
@@ -419,7 +421,11 @@ class Engine3D:
             g.source_gradient[a] = arr(f"sourceGradient{a}")
         g.source_amplitude = float(mesh["sourceAmplitude"])
         g.precision = int(precision)
+        g.cpml_x, g.cpml_y, g.cpml_z = arr("cpmlX"), arr("cpmlY"), arr("cpmlZ")
+        g.cpml_width_x, g.cpml_width_y = int(mesh.get("cpmlWidthX", 0)), int(mesh.get("cpmlWidthY", 0))
+        g.cpml_width_z, g.cpml_count = int(mesh.get("cpmlWidthZ", 0)), int(mesh.get("cpmlCount", 0))
         self.count, self.nrec = g.count, len(receivers)
+        self.cpml_count = g.cpml_count
         rec = np.ascontiguousarray(receivers, dtype=np.int64)
         h = C.c_void_p()
         _check(L.swl3d_create(C.byref(g), rec.ctypes.data_as(_i64p), len(rec), int(device), C.byref(h)))
@@ -469,9 +475,10 @@ class Engine3D:
         return t
 
     def field(self, f: int) -> np.ndarray:
-        out = np.zeros(self.count)
+        """Field f (0..8) of the current state, or f = -1: the CFS-PML memories."""
+        out = np.zeros(max(self.cpml_count, 1) if f == -1 else self.count)
         _check(library().swl3d_snapshot(self._h, f, out.ctypes.data_as(_dp)))
-        return out
+        return out[: self.cpml_count] if f == -1 else out
 
     def fields(self) -> np.ndarray:
         return np.stack([self.field(f) for f in range(9)])

@@ -45,14 +45,19 @@ std::unique_ptr<Engine3D> makeEngine3D32(const swl_mesh3d &, const int64_t *, in
 
 namespace detail3 {
 template <class Real> struct Launch {
+    template <int DX, int DY, int DZ, bool CPML>
+    static void stc(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
+        switch (stage) {
+        case 0: k3::stage3d<Real, DX, DY, DZ, 0, CPML><<<g, b, 0, s>>>(a); break;
+        case 1: k3::stage3d<Real, DX, DY, DZ, 1, CPML><<<g, b, 0, s>>>(a); break;
+        case 2: k3::stage3d<Real, DX, DY, DZ, 2, CPML><<<g, b, 0, s>>>(a); break;
+        default: k3::stage3d<Real, DX, DY, DZ, 3, CPML><<<g, b, 0, s>>>(a); break;
+        }
+    }
     template <int DX, int DY, int DZ>
     static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
-        switch (stage) {
-        case 0: k3::stage3d<Real, DX, DY, DZ, 0><<<g, b, 0, s>>>(a); break;
-        case 1: k3::stage3d<Real, DX, DY, DZ, 1><<<g, b, 0, s>>>(a); break;
-        case 2: k3::stage3d<Real, DX, DY, DZ, 2><<<g, b, 0, s>>>(a); break;
-        default: k3::stage3d<Real, DX, DY, DZ, 3><<<g, b, 0, s>>>(a); break;
-        }
+        if (a.m.cpml) stc<DX, DY, DZ, true>(stage, g, b, s, a);
+        else stc<DX, DY, DZ, false>(stage, g, b, s, a);
     }
     static void stage(int dx, int dy, int dz, int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
         switch (dx * 4 + dy * 2 + dz) {
@@ -81,6 +86,10 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
     static constexpr int kSets = k2::kahan<Real>() ? 6 : 4;
     Real *set_[6]{};
+    // CFS-PML memories: the same sets and roles as the fields (pcount_ values each)
+    DeviceBuffer psets_;
+    Real *pset_[6]{};
+    long long pcount_{0};
     int u_{0}, a_{1};
     bool previous_{false};
     int nrec_{}, traceCap_{}, forcingCap_{};
@@ -149,6 +158,17 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         p.w3 = static_cast<Real>(dt_ / 3.0);
         p.surfRate = surfRate_.as<double>();
         if (k2::kahan<Real>()) p.cin = set_[4 + u_], p.cout = set_[4 + a_];
+        if (pcount_) {
+            Real *PU = pset_[u_], *PA = pset_[a_], *PS1 = pset_[2], *PS2 = pset_[3];
+            p.pbase = PU, p.pacc = PA;
+            switch (stage) {
+            case 0: p.pin = PU, p.pout = PS1; break;
+            case 1: p.pin = PS1, p.pout = PS2; break;
+            case 2: p.pin = PS2, p.pout = PS1; break;
+            default: p.pin = PS1, p.pout = nullptr; break;
+            }
+            if (k2::kahan<Real>()) p.pcin = pset_[4 + u_], p.pcout = pset_[4 + a_];
+        }
         return p;
     }
     void enqueueStep(int step, bool verdict, cudaEvent_t *ev = nullptr) {
@@ -177,14 +197,14 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
         const double F = 9 * s, M = (m_.mlambda ? 12 : 9) * s;
-        return points * (17 * F + 4 * M);
+        return points * (17 * F + 4 * M) + double(pcount_) * 17 * s;
     }
     // FP32 only: the last stage's compensation terms read and written (2 F); it also reads U, which
     // the count above already holds.
     double extraBytesPerStep() const {
         if (!k2::kahan<Real>()) return 0;
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
-        return points * 2 * 9 * s;
+        return points * 2 * 9 * s + double(pcount_) * 2 * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -340,6 +360,25 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         }
         sets_.allocate(kSets * 9 * n * sizeof(Real));
         for (int s = 0; s < kSets; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * 9 * n;
+        if (g.cpml_count) { // CFS-PML slabs (swl_mesh3d)
+            const int NX = g.nx - 6, NY = g.ny - 6, NZ = g.nz - 6;
+            if (g.cpml_width_x < 0 || g.cpml_width_y < 0 || g.cpml_width_z < 0 || 2 * g.cpml_width_x > NX ||
+                2 * g.cpml_width_y > NY || g.cpml_width_z > NZ || !g.cpml_x || !g.cpml_y || !g.cpml_z ||
+                g.cpml_count != 6 * (2 * int64_t(g.cpml_width_x) * NY * NZ + 2 * int64_t(g.cpml_width_y) * NX * NZ +
+                                     int64_t(g.cpml_width_z) * NX * NY))
+                throw Error(SWL_ERR_INVALID, "3D CFS-PML needs widths within the grid, three profiles and "
+                                             "cpml_count = 6*(2wx*ny*nz + 2wy*nx*nz + wz*nx*ny) over the computational grid");
+            auto prof = [&](const double *src, int len) {
+                std::vector<Real> v(3 * std::size_t(len));
+                for (std::size_t q = 0; q < v.size(); ++q) v[q] = static_cast<Real>(src[q]);
+                return upload(v);
+            };
+            m_.cpml = 1, m_.wx = g.cpml_width_x, m_.wy = g.cpml_width_y, m_.wz = g.cpml_width_z;
+            m_.cpx = prof(g.cpml_x, NX), m_.cpy = prof(g.cpml_y, NY), m_.cpz = prof(g.cpml_z, NZ);
+            pcount_ = g.cpml_count;
+            psets_.allocate(kSets * std::size_t(pcount_) * sizeof(Real));
+            for (int s = 0; s < kSets; ++s) pset_[s] = psets_.as<Real>() + std::size_t(s) * pcount_;
+        }
         surfRate_.allocate(2 * std::size_t(m_.plane) * sizeof(double));
         std::vector<long long> idx(nrec);
         for (int r = 0; r < nrec; ++r) {
@@ -356,7 +395,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "create batch event");
         ensureCapacity(8);
         cudaFuncAttributes attr{};
-        check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1>), "3D kernel compatibility");
+        check(cudaFuncGetAttributes(&attr, k3::stage3d<Real, 0, 0, 0, 1, false>), "3D kernel compatibility");
         registers_ = attr.numRegs;
     }
     ~TypedEngine3D() override {
@@ -524,6 +563,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         settle();
         DeviceScope scope(device_);
         check(cudaMemsetAsync(sets_.ptr, 0, sets_.bytes, stream_), "3D reset");
+        if (psets_.ptr) check(cudaMemsetAsync(psets_.ptr, 0, psets_.bytes, stream_), "3D memory reset");
         if (traces_.ptr) check(cudaMemsetAsync(traces_.ptr, 0, traces_.bytes, stream_), "3D trace reset");
         check(cudaMemsetAsync(surfRate_.ptr, 0, surfRate_.bytes, stream_), "3D surface reset");
         hostClock_ = k2::Clock{};
@@ -608,6 +648,13 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void snapshot(int field, double *out) override {
         settle();
         DeviceScope scope(device_);
+        if (field == -1 && pcount_) { // the CFS-PML memories
+            check(cudaStreamSynchronize(stream_), "snapshot ordering");
+            std::vector<Real> tmp(pcount_);
+            check(cudaMemcpy(tmp.data(), pset_[u_], pcount_ * sizeof(Real), cudaMemcpyDeviceToHost), "memory download");
+            for (long long q = 0; q < pcount_; ++q) out[q] = double(tmp[q]);
+            return;
+        }
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "snapshot field out of range");
         check(cudaStreamSynchronize(stream_), "snapshot ordering");
         std::vector<Real> tmp(count_);
@@ -620,6 +667,16 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void load(int field, const double *in) override {
         settle();
         DeviceScope scope(device_);
+        if (field == -1 && pcount_) {
+            clockStats_ = false;
+            check(cudaStreamSynchronize(stream_), "load ordering");
+            std::vector<Real> tmp(pcount_);
+            for (long long q = 0; q < pcount_; ++q) tmp[q] = static_cast<Real>(in[q]);
+            check(cudaMemcpy(pset_[u_], tmp.data(), pcount_ * sizeof(Real), cudaMemcpyHostToDevice), "memory upload");
+            if (k2::kahan<Real>()) check(cudaMemset(pset_[4 + u_], 0, pcount_ * sizeof(Real)), "clear compensation");
+            previous_ = false;
+            return;
+        }
         if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
         clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "load ordering");
@@ -636,7 +693,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     int64_t residentBytes() const override {
         int64_t b = 0;
         for (const auto &x : model_) b += x.bytes;
-        for (const auto *x : {&sets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_, &surfRate_}) b += x->bytes;
+        for (const auto *x : {&sets_, &psets_, &recIdx_, &traces_, &forcing_, &clock_, &partials_, &surfRate_}) b += x->bytes;
         return b;
     }
 };

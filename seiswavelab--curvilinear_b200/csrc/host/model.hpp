@@ -140,6 +140,10 @@ struct Params3D {
     bool absorbing{true};
     std::array<int, 3> absorbingCells{8, 6, 8};
     double absorbingStrength{3};
+    // 0: the reference's quadratic sponge; 1: CFS-PML ADE slabs of the same widths (no counterpart
+    // in the reference's 3D path; the 2D profiles of src/two_d/CfsPml2D.hpp:31-41 per axis)
+    int absorber{0};
+    double cpmlReflection{1e-4}, cpmlKappaMax{3}, cpmlFrequency{};
     int receiverLimit{1024}; // the reference caps traces at 1024; the engine has no such limit
     // FP64 node geometry built on this CUDA device (-1: the largest) instead of on the host
     bool deviceGeometry{false};
@@ -158,10 +162,21 @@ struct Model3D {
     double dt{};
     int total{};
     double minJacobian{}, maxMetricNorm{}, minCellLength{}, maxCellEdge{}, waveDt{}, dampingDt{}, sourceDt{}, ppw{};
+    // CFS-PML: (d, kappa, alpha) per computational index along x, y, z; slab widths; memories
+    std::vector<double> cpmlX, cpmlY, cpmlZ;
+    std::array<int, 3> cpmlWidth{};
+    std::int64_t cpmlCount{};
+    std::vector<double> cpmlShape; // wx, wy, wz, memory count (as model array "cpmlShape")
+    double cpmlDt{};
     std::vector<std::int64_t> receiverNodes;
     std::vector<std::array<double, 3>> receiverPositions;
 };
 // CpuSimulation3D::initialize (src/three_d/CurvilinearSolver.cpp:301-442), model part.
 Model3D buildModel3D(const Params3D &);
+// src/two_d/CfsPml2D.hpp:31-41: (d, kappa, alpha) for `nodes` computational indices, a layer of
+// `width` cells at both ends (`both`) or at the far end only; and the largest d/kappa + alpha.
+std::vector<double> cpmlProfile(int nodes, int width, double h, double vp, double reflection, double kappa, double frequency,
+                                bool both);
+double cpmlRate(const std::vector<double> &profile);
 
 } // namespace swl::host

@@ -20,6 +20,8 @@ bool material(double vp, double vs, double rho) {
     return std::isfinite(vp) && std::isfinite(vs) && std::isfinite(rho) && vp > 0 && vs > 0 && rho > 0 &&
            vp * vp > 4 * vs * vs / 3 && std::isfinite(rho * vp * vp);
 }
+} // namespace
+
 // src/two_d/CfsPml2D.hpp:31-41
 std::vector<double> cpmlProfile(int nodes, int width, double h, double vp, double reflection, double kappa, double frequency,
                                 bool both) {
@@ -39,7 +41,7 @@ double cpmlRate(const std::vector<double> &profile) {
     for (std::size_t i = 0; i < profile.size(); i += 3) rate = std::max(rate, profile[i] / profile[i + 1] + profile[i + 2]);
     return rate;
 }
-} // namespace
+
 
 Model2D buildModel2D(const Params2D &requested) {
     Params2D p = requested;

@@ -54,6 +54,12 @@ Model3D buildModel3D(const Params3D &p) {
     require(std::isfinite(p.absorbingStrength) && p.absorbingStrength >= 0.1 && p.absorbingStrength <= 10.0,
             "Sponge strength must be in 0.1..10.");
     for (int w : p.absorbingCells) require(w >= 1 && w <= 64, "Sponge widths must be 1..64 cells.");
+    require(p.absorber == 0 || p.absorber == 1, "Unknown 3D absorber (0 sponge, 1 CFS-PML).");
+    if (p.absorbing && p.absorber == 1) // the 2D CFS-PML limits (CurvilinearSolver2D.cpp validation)
+        require(std::isfinite(p.cpmlReflection) && p.cpmlReflection >= 1e-8 && p.cpmlReflection <= .1 &&
+                    std::isfinite(p.cpmlKappaMax) && p.cpmlKappaMax >= 1 && p.cpmlKappaMax <= 20 &&
+                    std::isfinite(p.cpmlFrequency) && p.cpmlFrequency >= 0 && p.cpmlFrequency <= 1e6,
+                "CFS-PML reflection must be in 1e-8..0.1, kappa max in 1..20 and frequency in 0..1e6.");
     for (double v : {p.spacing, p.vp, p.vs, p.density, p.frequency, p.duration, p.relief, p.wavelength, p.flattenDepth})
         require(std::isfinite(v), "Simulation parameters must be finite.");
     require(!(p.nx < 8 || p.ny < 8 || p.nz < 8 || p.nx > 4096 || p.ny > 4096 || p.nz > 4096 || p.spacing <= 0 || p.vp <= 0 ||
@@ -279,6 +285,23 @@ Model3D buildModel3D(const Params3D &p) {
     const int nodes[3]{p.nx, p.ny, p.nz};
     if (p.absorbing)
         for (int a = 0; a < 3; ++a) widths[a] = std::min(p.absorbingCells[a], nodes[a] / 3);
+    const bool cpml = p.absorbing && p.absorber == 1;
+    if (cpml) { // CFS-PML slabs instead of the sponge: x and y on both sides, z at the bottom
+        const double frequency = p.cpmlFrequency > 0 ? p.cpmlFrequency : p.frequency;
+        g.cpmlX = cpmlProfile(p.nx, widths[0], p.spacing, maxVp, p.cpmlReflection, p.cpmlKappaMax, frequency, true);
+        g.cpmlY = cpmlProfile(p.ny, widths[1], p.spacing, maxVp, p.cpmlReflection, p.cpmlKappaMax, frequency, true);
+        g.cpmlZ = cpmlProfile(p.nz, widths[2], p.spacing, maxVp, p.cpmlReflection, p.cpmlKappaMax, frequency, false);
+        g.cpmlWidth = widths;
+        // six memories per active axis: 2wx*ny*nz x slots, 2wy*nx*nz y slots, wz*nx*ny z slots
+        g.cpmlCount = 6 * (2 * std::int64_t(widths[0]) * p.ny * p.nz + 2 * std::int64_t(widths[1]) * p.nx * p.nz +
+                           std::int64_t(widths[2]) * p.nx * p.ny);
+        const double rate = std::max({cpmlRate(g.cpmlX), cpmlRate(g.cpmlY), cpmlRate(g.cpmlZ)});
+        g.cpmlDt = rate > 0 ? .5 / rate : std::numeric_limits<double>::max();
+        widths = {0, 0, 0}; // no sponge
+    } else {
+        g.cpmlDt = std::numeric_limits<double>::max();
+    }
+    g.cpmlShape = {double(g.cpmlWidth[0]), double(g.cpmlWidth[1]), double(g.cpmlWidth[2]), double(g.cpmlCount)};
     for (int k = ghost; k < nz - ghost; ++k)
         for (int j = ghost; j < ny - ghost; ++j)
             for (int i = ghost; i < nx - ghost; ++i) {
@@ -297,7 +320,7 @@ Model3D buildModel3D(const Params3D &p) {
     g.waveDt = p.cfl * std::min(p.spacing / maxMetricNorm, minLength) / maxVp;
     g.dampingDt = maxDamping > 0 ? .5 / maxDamping : std::numeric_limits<double>::max();
     g.sourceDt = 1 / (50 * p.frequency);
-    const double safe = std::min({g.waveDt, g.dampingDt, g.sourceDt});
+    const double safe = std::min({g.waveDt, g.dampingDt, g.sourceDt, g.cpmlDt});
     const double durationSteps = std::max(1.0, std::ceil(p.duration / safe));
     require(std::isfinite(durationSteps) && !(p.maxSteps == 0 && durationSteps > 20000),
             "Time-step limit: at most 20,000 steps. Set a maximum step cap.");

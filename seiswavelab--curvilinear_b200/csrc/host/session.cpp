@@ -194,6 +194,8 @@ void swl3d_params_default(swl_params3d *c) {
     c->absorbing = p.absorbing;
     for (int a = 0; a < 3; ++a) c->absorbing_cells[a] = p.absorbingCells[a];
     c->absorbing_strength = p.absorbingStrength;
+    c->absorber = p.absorber;
+    c->cpml_reflection = p.cpmlReflection, c->cpml_kappa_max = p.cpmlKappaMax, c->cpml_frequency = p.cpmlFrequency;
 }
 swl_status swl3d_session_create(const swl_params3d *c, int32_t device, swl3d_session **out) {
     return guard([&] {

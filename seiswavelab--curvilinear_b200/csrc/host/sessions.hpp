@@ -281,6 +281,11 @@ struct Session3D {
             }
             m.source_amplitude = model.sourceAmplitude;
             m.precision = params.precision;
+            if (model.cpmlCount) {
+                m.cpml_x = model.cpmlX.data(), m.cpml_y = model.cpmlY.data(), m.cpml_z = model.cpmlZ.data();
+                m.cpml_width_x = model.cpmlWidth[0], m.cpml_width_y = model.cpmlWidth[1], m.cpml_width_z = model.cpmlWidth[2];
+                m.cpml_count = model.cpmlCount;
+            }
             ok(swl3d_create(&m, model.receiverNodes.data(), int32_t(model.receiverNodes.size()), device, &engine));
             ok(swl3d_reserve(engine, std::min(model.total, maxBatch))); // batch tables sized once, at creation
             ok(swl3d_diagnostics(engine, &diag));
@@ -358,6 +363,11 @@ struct Session3D {
         if (n == "materialLambda") return &m.materialLambda;
         if (n == "materialMu") return &m.materialMu;
         if (n == "materialDensity") return &m.materialDensity;
+        if (n == "cpmlX") return &m.cpmlX;
+        if (n == "cpmlY") return &m.cpmlY;
+        if (n == "cpmlZ") return &m.cpmlZ;
+        if (n == "cpmlShape") return &m.cpmlShape;
+        if (n == "cpmlShape") return &m.cpmlShape;
         for (int a = 0; a < 3; ++a)
             if (n == "sourceGradient" + std::to_string(a)) return &m.sourceGradient[a];
         return nullptr;
@@ -387,6 +397,8 @@ inline Params3D toParams(const swl_params3d &c) {
     p.absorbing = c.absorbing != 0;
     for (int a = 0; a < 3; ++a) p.absorbingCells[a] = c.absorbing_cells[a];
     p.absorbingStrength = c.absorbing_strength;
+    p.absorber = c.absorber;
+    p.cpmlReflection = c.cpml_reflection, p.cpmlKappaMax = c.cpml_kappa_max, p.cpmlFrequency = c.cpml_frequency;
     p.deviceGeometry = c.device_geometry != 0;
     if (c.layer_names)
         for (int l = 0; l < c.n_layers; ++l) p.layerNames.push_back(c.layer_names[l] ? c.layer_names[l] : "");

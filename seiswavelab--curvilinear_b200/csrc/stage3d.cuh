@@ -42,6 +42,13 @@ template <class Real> struct Mesh {
     Real sdir[3];
     int src_i0, src_i1, src_j0, src_j1, src_k0, src_k1;
     int dmp_i0, dmp_i1, dmp_j0, dmp_j1, dmp_k1; // damping is zero inside this box
+    // CFS-PML ADE (this library's 3D extension of the 2D ADE, src/two_d/PointKernels2D.hpp:50-64):
+    // slabs of wx computational nodes on both x sides, wy on both y sides and wz at the bottom;
+    // (d, kappa, alpha) per computational index along each axis; six memories per active axis of
+    // a node (the axis derivative of Vx, Vy, Vz, then the axis part of the three momentum sums).
+    int cpml;
+    int wx, wy, wz;
+    const Real *cpx, *cpy, *cpz;
 };
 
 using k2::Clock;
@@ -59,7 +66,49 @@ template <class Real> struct StageArgs {
     double *surfRate;    // stage 3: |traction rate| and rate norm per surface node (2 x px*ny)
     const Real *cin;     // FP32 only: Kahan compensation of U (read) and of the new state (written)
     Real *cout;
+    // CFS-PML memories, the same set scheme as the fields: stage input, stage output, U, A and the
+    // FP32 compensation of U (read) and of the new memories (written)
+    const Real *pin;
+    Real *pout;
+    const Real *pbase;
+    Real *pacc;
+    const Real *pcin;
+    Real *pcout;
 };
+
+// Compact memory slots of padded node (i, j, k) along each axis (-1 outside that axis's slab):
+// x slots 6*((kc*NY + jc)*2wx + s), then y slots 6*((kc*2wy + s)*NX + ic), then z slots
+// 6*(((kc - (NZ-wz))*NY + jc)*NX + ic), over the computational indices ic, jc, kc.
+template <class Real> __device__ __forceinline__ void cpmlSlots3(const Mesh<Real> &m, int i, int j, int k, long long (&slot)[3]) {
+    const int ic = i - 3, jc = j - 3, kc = k - 3, NX = m.nx - 6, NY = m.ny - 6, NZ = m.nz - 6;
+    const long long c0 = 6LL * 2 * m.wx * NY * NZ, c1 = 6LL * 2 * m.wy * NX * NZ;
+    int s = ic < m.wx ? ic : ic >= NX - m.wx ? m.wx + ic - (NX - m.wx) : -1;
+    slot[0] = s >= 0 ? 6 * (((long long)kc * NY + jc) * 2 * m.wx + s) : -1;
+    s = jc < m.wy ? jc : jc >= NY - m.wy ? m.wy + jc - (NY - m.wy) : -1;
+    slot[1] = s >= 0 ? c0 + 6 * (((long long)kc * 2 * m.wy + s) * NX + ic) : -1;
+    slot[2] = kc >= NZ - m.wz ? c0 + c1 + 6 * (((long long)(kc - (NZ - m.wz)) * NY + jc) * NX + ic) : -1;
+}
+
+// RK combine of one memory value (the fields' scheme, finish3).
+template <class Real, int STAGE> __device__ __forceinline__ void combineMemory3(const StageArgs<Real> &p, long long at, Real r) {
+    const Real u = (STAGE < 3 || k2::kahan<Real>()) ? k2::ld(p.pbase + at) : Real(0);
+    if (STAGE == 0) {
+        p.pacc[at] = k2::kahan<Real>() ? p.w6 * r : u + p.w6 * r;
+        p.pout[at] = u + p.weight * r;
+    } else if (STAGE < 3) {
+        const Real a = p.pacc[at];
+        p.pacc[at] = a + p.w3 * r;
+        p.pout[at] = u + p.weight * r;
+    } else if constexpr (k2::kahan<Real>()) {
+        const Real a = p.pacc[at], c = k2::ld(p.pcin + at);
+        const Real y = (a + p.w6 * r) - c;
+        const Real o = u + y;
+        p.pcout[at] = (o - u) - y;
+        p.pacc[at] = o;
+    } else {
+        p.pacc[at] = p.pacc[at] + p.w6 * r;
+    }
+}
 
 using k2::ld;
 
@@ -138,11 +187,14 @@ __device__ __forceinline__ Real tractionFlux(const Mesh<Real> &m, const Real *__
 }
 
 // src/three_d/PointKernels3D.hpp:73-91 (surface rows only; reads the stage input from global memory)
+// `only` >= 0: that axis's part alone (the CFS-PML split).
 template <class Real, int DX, int DY, int DZ>
-__device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, Real rho) {
+__device__ __noinline__ Real surfaceMomentum(const Mesh<Real> &m, const Real *__restrict__ w, long long q, int comp, int depth, Real rho,
+                                             int only = -1) {
     const Real C[5] = {Real(-.30874), Real(-.6326), Real(1.233), Real(-.3334), Real(.04168)};
     Real sum = Real(0);
     for (int axis = 0; axis < 3; ++axis) {
+        if (only >= 0 && axis != only) continue;
         const int dir = axis == 0 ? DX : axis == 1 ? DY : DZ;
         const long long s = axis == 0 ? 1 : axis == 1 ? m.px : m.plane;
         for (int l = 0; l < 5; ++l) {
@@ -251,7 +303,7 @@ __device__ __forceinline__ void finish3(const StageArgs<Real> &p, const Real (&r
 
 // The general node: surface rows (traction-free derivative, traction-image momentum,
 // projection) and the source support, with sponge damping where it applies.
-template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool CPML>
 __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,12 +322,23 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) M[c] = ld(m.metric[c] + q);
 
-    // raw xi / eta derivatives of the velocities (also used by the surface solve)
+    // CFS-PML: the node's memory slots and the rates of its memories
+    long long slot[3] = {-1, -1, -1};
+    if constexpr (CPML) cpmlSlots3(m, i, j, k, slot);
+    const bool split = CPML && (slot[0] >= 0 || slot[1] >= 0 || slot[2] >= 0);
+    Real prate[3][6];
+    auto stretchAxis = [&](int a, int f, Real d) -> Real {
+        if (slot[a] < 0) return d;
+        const Real *prof = (a == 0 ? m.cpx + 3 * (i - 3) : a == 1 ? m.cpy + 3 * (j - 3) : m.cpz + 3 * (k - 3));
+        return k2::stretch(prof, ld(p.pin + slot[a] + f), d, prate[a][f]);
+    };
+    // raw xi / eta derivatives of the velocities (also used by the surface solve), stretched in a slab
     Real dv[3][2];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         dv[v][0] = gd5<Real, DX, EXACT>(w + v * n, q, 1, m);
         dv[v][1] = gd5<Real, DY, EXACT>(w + v * n, q, nx, m);
+        if (split) dv[v][0] = stretchAxis(0, v, dv[v][0]), dv[v][1] = stretchAxis(1, v, dv[v][1]);
     }
     Real dzs[3] = {0, 0, 0};
     if (depth == 0) { // src/three_d/PointKernels3D.hpp:52-66
@@ -307,6 +370,9 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
             else if (depth == 1) dz = gd2<Real, DZ, EXACT>(w + f * n, q, plane, m);
             else if (depth == 2) dz = gd3<Real, DZ, EXACT>(w + f * n, q, plane, m);
             else dz = gd5<Real, DZ, EXACT>(w + f * n, q, plane, m);
+            if (split) dz = stretchAxis(2, f, dz);
+        } else if (split) {
+            continue; // a slab node takes its stress derivatives per axis, below
         } else {
             dx = gd5<Real, DX, EXACT>(w + f * n, q, 1, m);
             dy = gd5<Real, DY, EXACT>(w + f * n, q, nx, m);
@@ -316,11 +382,36 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
         for (int a = 0; a < 3; ++a) gr[f][a] = M[a] * dx + M[3 + a] * dy + M[6 + a] * dz;
     }
     Real r[9];
-    if (depth <= (DZ ? 3 : 1)) {
+    const bool near = depth <= (DZ ? 3 : 1);
+    if (!split) {
+        if (near) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, a, depth, rho);
+            for (int a = 0; a < 3; ++a) r[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, a, depth, rho);
+        } else {
+            byRho3(m, rho, r, (gr[3][0] + gr[6][1]) + gr[7][2], (gr[6][0] + gr[4][1]) + gr[8][2], (gr[7][0] + gr[8][1]) + gr[5][2]);
+        }
     } else {
-        byRho3(m, rho, r, (gr[3][0] + gr[6][1]) + gr[7][2], (gr[6][0] + gr[4][1]) + gr[8][2], (gr[7][0] + gr[8][1]) + gr[5][2]);
+        // the momentum of a slab node summed per axis: for axis a the part
+        // (d(xi_a)/dx dS_c0 + d(xi_a)/dy dS_c1 + d(xi_a)/dz dS_c2)/rho of the a-derivatives, each part
+        // stretched where the axis is active, then x + y + z
+        const int F[3][3] = {{3, 6, 7}, {6, 4, 8}, {7, 8, 5}};
+        const Real rinv = m.rhoRecip ? Real(1) / rho : Real(0);
+        auto byRho = [&](Real x) { return m.rhoRecip ? k2::divBy(x, rho, rinv) : x / rho; };
+        auto gda = [&](int a, int f) {
+            return a == 0 ? gd5<Real, DX, EXACT>(w + f * n, q, 1, m) : a == 1 ? gd5<Real, DY, EXACT>(w + f * n, q, nx, m)
+                                                                         : gd5<Real, DZ, EXACT>(w + f * n, q, plane, m);
+        };
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c) {
+            Real part[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (near) part[a] = surfaceMomentum<Real, DX, DY, DZ>(m, w, q, c, depth, rho, a);
+                else part[a] = byRho((M[3 * a] * gda(a, F[c][0]) + M[3 * a + 1] * gda(a, F[c][1])) + M[3 * a + 2] * gda(a, F[c][2]));
+                part[a] = stretchAxis(a, 3 + c, part[a]);
+            }
+            r[c] = (part[0] + part[1]) + part[2];
+        }
     }
     if (i >= m.src_i0 && i < m.src_i1 && j >= m.src_j0 && j < m.src_j1 && k >= m.src_k0 && k < m.src_k1) {
         const Real s = p.forcing[3 * (clk->step - clk->first) + (STAGE == 0 ? 0 : STAGE == 3 ? 2 : 1)];
@@ -354,6 +445,11 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
         p.surfRate[plane + sq] = sqrt(norm2);
     }
     finish3<Real, STAGE>(p, r, q, depth, sq);
+    if (split)
+        for (int a = 0; a < 3; ++a)
+            if (slot[a] >= 0)
+#pragma unroll
+                for (int f = 0; f < 6; ++f) combineMemory3<Real, STAGE>(p, slot[a] + f, prate[a][f]);
 }
 
 // The interior node (below the surface rows, outside the source support), with the sponge's
@@ -418,9 +514,9 @@ __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
     finish3<Real, STAGE>(p, r, q, 4, i + nx * j);
 }
 
-template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT>
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool CPML>
 __device__ __forceinline__ void stageNode3(const StageArgs<Real> &p, bool general, bool sponge) {
-    if (general) stageBody3<Real, DX, DY, DZ, STAGE, EXACT>(p);
+    if (general) stageBody3<Real, DX, DY, DZ, STAGE, EXACT, CPML>(p);
     else if (sponge) stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, true>(p);
     else stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, false>(p);
 }
@@ -428,8 +524,9 @@ __device__ __forceinline__ void stageNode3(const StageArgs<Real> &p, bool genera
 // One RK stage of a 3D shot: block 32x8 nodes of one z layer.  CTAs on the surface rows or on
 // the source support run the general form; the others run the interior form, with the damping
 // term when the CTA reaches into the sponge (so the sponge costs nine multiply-adds, not the
-// general form).
-template <class Real, int DX, int DY, int DZ, int STAGE>
+// general form).  CPML: the mesh has CFS-PML slabs; their CTAs run the general form with the ADE
+// terms.  Meshes without them launch the CPML = false kernels, which hold none of that code.
+template <class Real, int DX, int DY, int DZ, int STAGE, bool CPML>
 __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __grid_constant__ StageArgs<Real> p) {
     const Mesh<Real> &m = p.m;
     if (p.clock->faulted) return;
@@ -438,10 +535,13 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __gri
     const bool surface = k < 7;
     const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
     const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
-    const bool general = surface || source;
-    if constexpr (sizeof(Real) == 4) stageNode3<Real, DX, DY, DZ, STAGE, true>(p, general, sponge);
-    else if (m.hinvExact) stageNode3<Real, DX, DY, DZ, STAGE, true>(p, general, sponge);
-    else stageNode3<Real, DX, DY, DZ, STAGE, false>(p, general, sponge);
+    // CTAs reaching into a CFS-PML slab run the general form (it holds the ADE terms)
+    const bool slab = CPML && (i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || j0 - 3 < m.wy || j1 - 3 > m.ny - 6 - m.wy ||
+                               k - 3 >= m.nz - 6 - m.wz);
+    const bool general = surface || source || slab;
+    if constexpr (sizeof(Real) == 4) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);
+    else if (m.hinvExact) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);
+    else stageNode3<Real, DX, DY, DZ, STAGE, false, CPML>(p, general, sponge);
 }
 
 struct Partial {

@@ -75,6 +75,8 @@ class Params3D(C.Structure):
                                    "receiver_limit")],
         ("absorbing", C.c_int32), ("absorbing_cells", C.c_int32 * 3), ("absorbing_strength", C.c_double),
         ("device_geometry", C.c_int32), ("layer_names", C.POINTER(C.c_char_p)),
+        ("absorber", C.c_int32), ("cpml_reflection", C.c_double), ("cpml_kappa_max", C.c_double),
+        ("cpml_frequency", C.c_double),
     ]
 
 
@@ -162,7 +164,8 @@ _MAP3D = {
     "sourceForce": "source_force", "sourceMoment": "source_moment", "duration": "duration", "maxSteps": "max_steps",
     "cfl": "cfl", "relief": "relief", "wavelength": "wavelength", "flattenDepth": "flatten_depth",
     "absorbing": "absorbing", "absorbingStrength": "absorbing_strength", "receiverLimit": "receiver_limit",
-    "deviceGeometry": "device_geometry",
+    "deviceGeometry": "device_geometry", "absorber": "absorber", "cpmlReflection": "cpml_reflection",
+    "cpmlKappaMax": "cpml_kappa_max", "cpmlFrequency": "cpml_frequency",
 }
 
 
@@ -368,6 +371,12 @@ class Simulation3D:
         return t
 
     def field(self, f: int) -> np.ndarray:
+        """Field f (0..8), or f = -1: the CFS-PML memories (model('cpmlShape')[3] of them)."""
+        if f == -1:
+            n = int(self.model("cpmlShape")[3])
+            out = np.zeros(max(n, 1))
+            _check(library().swl3d_session_snapshot(self._h, f, out.ctypes.data_as(_dp)))
+            return out[:n]
         out = np.zeros(self.info()["count"])
         _check(library().swl3d_session_snapshot(self._h, f, out.ctypes.data_as(_dp)))
         return out
@@ -403,7 +412,9 @@ def read_model3d(path):
     try:
         p, c, dt = Params3D(), ModelCompute(), C.c_double()
         _check(L.swl3d_model_document_params(h, C.byref(p), C.byref(c), C.byref(dt)))
-        out = {k: getattr(p, f) for k, f in _MAP3D.items() if k not in ("deviceGeometry", "precision", "receiverLimit")}
+        out = {k: getattr(p, f) for k, f in _MAP3D.items()
+               if k not in ("deviceGeometry", "precision", "receiverLimit", "absorber", "cpmlReflection", "cpmlKappaMax",
+                            "cpmlFrequency")}
         out["sourceDirection"] = list(p.source_direction)
         out["layers"] = [[p.layers[i].thickness, p.layers[i].vp, p.layers[i].vs, p.layers[i].density]
                          for i in range(p.n_layers)]

@@ -118,7 +118,7 @@ def grf_dem(nx: int, ny: int, spacing: float, correlation: float, relief: float,
 
 
 def elastic_3d(precision: int = 0, steps: int = 1500, nx: int = 400, ny: int = 288, nz: int = 200,
-               receivers: int = 40, relief: float = 150.0, flatten_depth: float = 800.0) -> dict:
+               receivers: int = 40, relief: float = 150.0, flatten_depth: float = 800.0, absorber: int = 0) -> dict:
     """400x288x200 3D elastic, h=10 m, DEM terrain (seed 4, correlation 500 m, relief 150 m on a
     25 m lattice), blend depth 800 m, layers 200 m / 600 m / basement below the surface, 15 Hz
     explosive source 5 nodes deep, 20-cell sponge, 40x40 areal surface receivers.  Reduced grids
@@ -136,7 +136,7 @@ def elastic_3d(precision: int = 0, steps: int = 1500, nx: int = 400, ny: int = 2
                 demShape=[dnx, dny, dem_dx, 0.0, 0.0, 0.0], demElevations=elev.ravel().tolist(),
                 flattenDepth=float(flatten_depth), layered=1, layerDepthMode=1,
                 layers=[200, 1200, 600, 1800, 600, 2400, 1300, 2100, 0, 3800, 2200, 2400],
-                absorbing=1, absorbingCells=[20, 20, 20], absorbingStrength=3.0,
+                absorbing=1, absorbingCells=[20, 20, 20], absorbingStrength=3.0, absorber=int(absorber),
                 receiverArray=[3, (nx - (receivers - 1) * sx) // 2, (ny - (receivers - 1) * sy) // 2, 0,
                                receivers, receivers, sx, sy],
                 receiverLimit=receivers * receivers)
