@@ -280,6 +280,12 @@ typedef struct swl_mesh3d {
     const double *cpml_x, *cpml_y, *cpml_z;
     int32_t cpml_width_x, cpml_width_y, cpml_width_z;
     int64_t cpml_count;
+    /* GSLS (no counterpart in the reference's 3D path): mechanisms 0..3; the fields become
+     * 9 + 6*mechanisms, the memories of mechanism l (xx, yy, zz, xy, xz, yz) at 9 + 6l; relaxation
+     * rates and per-node strengths (count values each) as swl_mesh2d has them. */
+    int32_t mechanisms;
+    double rates[3];
+    const double *delta_p[3], *delta_s[3];
 } swl_mesh3d;
 
 typedef struct swl_diag3d {

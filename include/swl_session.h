@@ -112,6 +112,11 @@ typedef struct swl_params3d {
      * bottom) with the 2D profiles per axis.  No counterpart in the reference's 3D path. */
     int32_t absorber;
     double cpml_reflection, cpml_kappa_max, cpml_frequency; /* frequency 0: the source frequency */
+    /* GSLS viscoelasticity with 1..3 mechanisms (the 2D settings of swl_params2d; no counterpart in
+     * the reference's 3D path).  layer_q: qp, qs per layer (2 * n_layers values), or null: qp, qs. */
+    int32_t attenuation, mechanisms;
+    double q_min_frequency, q_max_frequency, q_reference_frequency, qp, qs;
+    const double *layer_q;
 } swl_params3d;
 
 typedef struct swl_info3d {

@@ -47,6 +47,8 @@ class Mesh3D(C.Structure):
         ("source_direction", C.c_double * 3), ("source_amplitude", C.c_double), ("source_gradient", _dp * 3),
         ("cpml_x", _dp), ("cpml_y", _dp), ("cpml_z", _dp), ("cpml_width_x", C.c_int32), ("cpml_width_y", C.c_int32),
         ("cpml_width_z", C.c_int32), ("cpml_count", C.c_int64),
+        ("mechanisms", C.c_int32), ("field_count", C.c_int32), ("rates", C.c_double * 3), ("delta_p", _dp * 3),
+        ("delta_s", _dp * 3),
     ]
 
 
@@ -178,12 +180,19 @@ class Oracle:
         g.cpml_x, g.cpml_y, g.cpml_z = arr("cpmlX"), arr("cpmlY"), arr("cpmlZ")
         g.cpml_width_x, g.cpml_width_y = int(m.get("cpmlWidthX", 0)), int(m.get("cpmlWidthY", 0))
         g.cpml_width_z, g.cpml_count = int(m.get("cpmlWidthZ", 0)), int(m.get("cpmlCount", 0))
+        # GSLS (absent: elastic, nine fields)
+        g.mechanisms = int(m.get("mechanisms", 0))
+        g.field_count = 9 + 6 * g.mechanisms
+        for l in range(3):
+            g.rates[l] = float(np.atleast_1d(m.get("rates", (0, 0, 0)))[l]) if l < g.mechanisms else 0.0
+            g.delta_p[l] = arr(f"deltaP{l}") if l < g.mechanisms else None
+            g.delta_s[l] = arr(f"deltaS{l}") if l < g.mechanisms else None
         return g, keep
 
     def run3d(self, m: dict, steps: int, first: int = 0, state=None, receivers=(), pml=None, with_pml=False):
         g, keep = self.mesh3d(m)
-        n = g.count
-        state = np.zeros(9 * n) if state is None else np.array(state, dtype=np.float64, copy=True)
+        n, fc = g.count, g.field_count
+        state = np.zeros(fc * n) if state is None else np.array(state, dtype=np.float64, copy=True)
         pml = np.zeros(max(g.cpml_count, 1)) if pml is None else np.array(pml, dtype=np.float64, copy=True)
         rec = np.ascontiguousarray(receivers, dtype=np.int64)
         tr = [np.zeros((len(rec), steps)) for _ in range(3)]
@@ -192,18 +201,18 @@ class Oracle:
         if rc:
             raise MemoryError("oracle 3D run failed")
         if with_pml:
-            return state.reshape(9, n), tr, pml[: g.cpml_count]
-        return state.reshape(9, n), tr
+            return state.reshape(fc, n), tr, pml[: g.cpml_count]
+        return state.reshape(fc, n), tr
 
     def rhs3d(self, m: dict, state, source, step, stage, pml=None):
         g, keep = self.mesh3d(m)
-        n = g.count
-        state = np.ascontiguousarray(state, dtype=np.float64).reshape(9, n)
-        out = np.zeros((9, n))
+        n, fc = g.count, g.field_count
+        state = np.ascontiguousarray(state, dtype=np.float64).reshape(fc, n)
+        out = np.zeros((fc, n))
         pml = np.ascontiguousarray(pml if pml is not None and len(pml) else np.zeros(max(g.cpml_count, 1)), dtype=np.float64)
         out_pml = np.zeros(max(g.cpml_count, 1))
-        ins = (_dp * 9)(*[_ptr(state[f]) for f in range(9)])
-        outs = (_dp * 9)(*[_ptr(out[f]) for f in range(9)])
+        ins = (_dp * fc)(*[_ptr(state[f]) for f in range(fc)])
+        outs = (_dp * fc)(*[_ptr(out[f]) for f in range(fc)])
         self.lib.swlo3d_rhs(C.byref(g), ins, _ptr(pml), outs, _ptr(out_pml), float(source), step, stage)
         return out
 

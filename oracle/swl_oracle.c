@@ -377,6 +377,14 @@ static void surface_derivative3(const swlo_mesh3d *g, double *const *w, ptrdiff_
     const double trace = gr[0] + gr[4] + gr[8];
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) t[a] += ((a == b ? lambda * trace : 0) + mu * (gr[3 * a + b] + gr[3 * b + a])) * c[b];
+    /* GSLS: the memory stresses' traction, as the 2D surfaceDerivative subtracts it
+     * (src/two_d/PointKernels2D.hpp:84) */
+    static const int T[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}}; /* tensor (a, b) -> memory component */
+    for (int l = 0; l < g->mechanisms; ++l) {
+        const int mm = 9 + 6 * l;
+        for (int a = 0; a < 3; ++a)
+            t[a] -= (w[mm + T[a][0]][q] * c[0] + w[mm + T[a][1]][q] * c[1]) + w[mm + T[a][2]][q] * c[2];
+    }
     const double normal = t[0] * n[0] + t[1] * n[1] + t[2] * n[2];
     for (int a = 0; a < 3; ++a) res[a] = -(t[a] - n[a] * normal) / (mu * c2) - n[a] * normal / ((lambda + 2 * mu) * c2);
 }
@@ -472,13 +480,26 @@ static void rhs3_point(const swlo_mesh3d *g, double *const *w, const double *in_
     out[6][q] = mu * (gr[0][1] + gr[1][0]);
     out[7][q] = mu * (gr[0][2] + gr[2][0]);
     out[8][q] = mu * (gr[1][2] + gr[2][1]);
-    for (int f = 0; f < 9; ++f) out[f][q] -= g->damping[q] * w[f][q];
+    /* GSLS (the 2D form of src/two_d/PointKernels2D.hpp:161-168 with all six stress components):
+     * drive = dl*div + 2 ds*e_aa on the normal components, ds*(g_ab + g_ba) on the shear ones,
+     * dl = dP - 2 dS; the stresses subtract the memories; memory rate = rate_l (drive - memory). */
+    for (int l = 0; l < g->mechanisms; ++l) {
+        const int mm = 9 + 6 * l;
+        const double dp = g->delta_p[l][q], ds = g->delta_s[l][q], dl = dp - 2 * ds;
+        const double drive[6] = {dl * div + 2 * ds * gr[0][0], dl * div + 2 * ds * gr[1][1], dl * div + 2 * ds * gr[2][2],
+                                 ds * (gr[0][1] + gr[1][0]),  ds * (gr[0][2] + gr[2][0]),  ds * (gr[1][2] + gr[2][1])};
+        for (int c = 0; c < 6; ++c) out[3 + c][q] -= w[mm + c][q];
+        for (int c = 0; c < 6; ++c) out[mm + c][q] = g->rates[l] * (drive[c] - w[mm + c][q]);
+    }
+    const int fc = g->field_count ? g->field_count : 9;
+    for (int f = 0; f < fc; ++f) out[f][q] -= g->damping[q] * w[f][q];
 }
 
 /* src/three_d/CurvilinearSolver.cpp:70-89 */
 void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, const double *in_pml, double *const *out, double *out_pml,
                 double source, int step, int stage) {
-    for (int f = 0; f < 9; ++f) memset(out[f], 0, sizeof(double) * (size_t)g->count);
+    const int fc = g->field_count ? g->field_count : 9;
+    for (int f = 0; f < fc; ++f) memset(out[f], 0, sizeof(double) * (size_t)g->count);
     if (g->cpml_count) memset(out_pml, 0, sizeof(double) * (size_t)g->cpml_count);
     for (int k = 3; k < g->nz - 3; ++k)
         for (int j = 3; j < g->ny - 3; ++j)
@@ -505,37 +526,38 @@ static void combine3(double *out, const double *base, const double *a, double wa
 int swlo3d_run(const swlo_mesh3d *g, double *state, double *pml, int first, int steps, double dt, double frequency,
                const int64_t *receivers, int nreceivers, double *trace_vx, double *trace_vy, double *trace_vz) {
     const size_t n = (size_t)g->count, np = (size_t)(pml ? g->cpml_count : 0);
-    if (g->cpml_count && !pml) return -1;
-    double *mem = (double *)calloc(6 * 9 * n + 6 * (np + 1), sizeof(double));
+    const int fc = g->field_count ? g->field_count : 9;
+    if ((g->cpml_count && !pml) || fc != 9 + 6 * g->mechanisms || fc > 27) return -1;
+    double *mem = (double *)calloc(6 * (size_t)fc * n + 6 * (np + 1), sizeof(double));
     if (!mem) return -1;
-    double *st[9], *base[9], *k[4][9], *sg[9];
-    for (int f = 0; f < 9; ++f) {
+    double *st[27], *base[27], *k[4][27], *sg[27];
+    for (int f = 0; f < fc; ++f) {
         st[f] = state + f * n;
         base[f] = mem + f * n;
-        for (int s = 0; s < 4; ++s) k[s][f] = mem + (size_t)(1 + s) * 9 * n + f * n;
-        sg[f] = mem + 5 * 9 * n + f * n;
+        for (int s = 0; s < 4; ++s) k[s][f] = mem + (size_t)(1 + s) * fc * n + f * n;
+        sg[f] = mem + 5 * (size_t)fc * n + f * n;
     }
-    double *pb = mem + 6 * 9 * n, *pk[4], *ps = pb + 5 * (np + 1);
+    double *pb = mem + 6 * (size_t)fc * n, *pk[4], *ps = pb + 5 * (np + 1);
     for (int s = 0; s < 4; ++s) pk[s] = pb + (size_t)(1 + s) * (np + 1);
     for (int it = 0; it < steps; ++it) {
         const int step = first + it;
-        memcpy(mem, state, sizeof(double) * 9 * n);
+        memcpy(mem, state, sizeof(double) * fc * n);
         if (np) memcpy(pb, pml, sizeof(double) * np);
         const double t = step * dt;
         swlo3d_rhs(g, st, pml, k[0], pk[0], source3(g, t, frequency), step, 0);
-        for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[0][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
+        for (int f = 0; f < fc; ++f) combine3(sg[f], base[f], k[0][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
         if (np) combine3(ps, pb, pk[0], 0.5 * dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
         swlo3d_rhs(g, sg, ps, k[1], pk[1], source3(g, t + 0.5 * dt, frequency), step, 1);
-        for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[1][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
+        for (int f = 0; f < fc; ++f) combine3(sg[f], base[f], k[1][f], 0.5 * dt, 0, 0, 0, 0, 0, 0, n);
         if (np) combine3(ps, pb, pk[1], 0.5 * dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
         swlo3d_rhs(g, sg, ps, k[2], pk[2], source3(g, t + 0.5 * dt, frequency), step, 2);
-        for (int f = 0; f < 9; ++f) combine3(sg[f], base[f], k[2][f], dt, 0, 0, 0, 0, 0, 0, n);
+        for (int f = 0; f < fc; ++f) combine3(sg[f], base[f], k[2][f], dt, 0, 0, 0, 0, 0, 0, n);
         if (np) combine3(ps, pb, pk[2], dt, 0, 0, 0, 0, 0, 0, np);
         swlo3d_project(g, sg);
         swlo3d_rhs(g, sg, ps, k[3], pk[3], source3(g, t + dt, frequency), step, 3);
-        for (int f = 0; f < 9; ++f)
+        for (int f = 0; f < fc; ++f)
             combine3(st[f], base[f], k[0][f], dt / 6.0, k[1][f], dt / 3.0, k[2][f], dt / 3.0, k[3][f], dt / 6.0, n);
         if (np) combine3(pml, pb, pk[0], dt / 6.0, pk[1], dt / 3.0, pk[2], dt / 3.0, pk[3], dt / 6.0, np);
         swlo3d_project(g, st);

@@ -45,6 +45,12 @@ typedef struct swlo_mesh3d {
     const double *cpml_x, *cpml_y, *cpml_z;
     int32_t cpml_width_x, cpml_width_y, cpml_width_z;
     int64_t cpml_count;
+    /* GSLS in 3D (the reference's 3D path is elastic; this build extends its 2D GSLS, see
+     * swl_oracle.c): mechanisms 0..3, fields 9 + 6*mechanisms (the memories of mechanism l at
+     * 9 + 6l: xx, yy, zz, xy, xz, yz), relaxation rates and per-node strengths. */
+    int32_t mechanisms, field_count;
+    double rates[3];
+    const double *delta_p[3], *delta_s[3];
 } swlo_mesh3d;
 
 int swlo_direction(int step, int stage, int axis);
@@ -64,8 +70,8 @@ int swlo2d_run(const swlo_mesh2d *g, double *state, double *pml, int first, int 
 void swlo3d_rhs(const swlo_mesh3d *g, double *const *in, const double *in_pml, double *const *out, double *out_pml,
                 double source, int step, int stage);
 void swlo3d_project(const swlo_mesh3d *g, double *const *fields);
-/* state: 9*count doubles; pml: cpml_count doubles (null without CFS-PML).  traces: receivers x
- * steps for Vx, Vy, Vz. */
+/* state: field_count*count doubles (9 when field_count is 0); pml: cpml_count doubles (null
+ * without CFS-PML).  traces: receivers x steps for Vx, Vy, Vz. */
 int swlo3d_run(const swlo_mesh3d *g, double *state, double *pml, int first, int steps, double dt, double frequency,
                const int64_t *receivers, int nreceivers, double *trace_vx, double *trace_vy, double *trace_vz);
 

@@ -67,6 +67,7 @@ class Mesh3D(C.Structure):
         ("precision", C.c_int32),
         ("cpml_x", _dp), ("cpml_y", _dp), ("cpml_z", _dp), ("cpml_width_x", C.c_int32), ("cpml_width_y", C.c_int32),
         ("cpml_width_z", C.c_int32), ("cpml_count", C.c_int64),
+        ("mechanisms", C.c_int32), ("rates", C.c_double * 3), ("delta_p", _dp * 3), ("delta_s", _dp * 3),
     ]
 
 
@@ -424,6 +425,11 @@ class Engine3D:
         g.cpml_x, g.cpml_y, g.cpml_z = arr("cpmlX"), arr("cpmlY"), arr("cpmlZ")
         g.cpml_width_x, g.cpml_width_y = int(mesh.get("cpmlWidthX", 0)), int(mesh.get("cpmlWidthY", 0))
         g.cpml_width_z, g.cpml_count = int(mesh.get("cpmlWidthZ", 0)), int(mesh.get("cpmlCount", 0))
+        g.mechanisms = int(mesh.get("mechanisms", 0))
+        for l in range(g.mechanisms):
+            g.rates[l] = float(np.atleast_1d(mesh["rates"])[l])
+            g.delta_p[l], g.delta_s[l] = arr(f"deltaP{l}"), arr(f"deltaS{l}")
+        self.field_count = 9 + 6 * g.mechanisms
         self.count, self.nrec = g.count, len(receivers)
         self.cpml_count = g.cpml_count
         rec = np.ascontiguousarray(receivers, dtype=np.int64)

@@ -56,7 +56,7 @@ template <class Real> struct Launch {
     }
     template <int DX, int DY, int DZ>
     static void st(int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
-        if (a.m.cpml) stc<DX, DY, DZ, true>(stage, g, b, s, a);
+        if (a.m.cpml || a.m.mech) stc<DX, DY, DZ, true>(stage, g, b, s, a);
         else stc<DX, DY, DZ, false>(stage, g, b, s, a);
     }
     static void stage(int dx, int dy, int dz, int stage, dim3 g, dim3 b, cudaStream_t s, const k3::StageArgs<Real> &a) {
@@ -90,6 +90,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     DeviceBuffer psets_;
     Real *pset_[6]{};
     long long pcount_{0};
+    int fc_{9}; // fields per set: 9, plus 6 GSLS memories per mechanism
     int u_{0}, a_{1};
     bool previous_{false};
     int nrec_{}, traceCap_{}, forcingCap_{};
@@ -197,14 +198,14 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     double bytesPerStep() const {
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
         const double F = 9 * s, M = (m_.mlambda ? 12 : 9) * s;
-        return points * (17 * F + 4 * M) + double(pcount_) * 17 * s;
+        return points * (17 * F * fc_ / 9 + 4 * (M + 2 * m_.mech * s)) + double(pcount_) * 17 * s;
     }
     // FP32 only: the last stage's compensation terms read and written (2 F); it also reads U, which
     // the count above already holds.
     double extraBytesPerStep() const {
         if (!k2::kahan<Real>()) return 0;
         const double s = sizeof(Real), points = double(m_.nx - 6) * (m_.ny - 6) * (m_.nz - 6);
-        return points * 2 * 9 * s + double(pcount_) * 2 * s;
+        return points * 2 * fc_ * s + double(pcount_) * 2 * s;
     }
     void ensureCapacity(int steps) {
         if (steps > forcingCap_) {
@@ -358,8 +359,19 @@ template <class Real> class TypedEngine3D final : public Engine3D {
                         }
             if (ok) m_.dmp_i0 = i0, m_.dmp_i1 = i1, m_.dmp_j0 = j0, m_.dmp_j1 = j1, m_.dmp_k1 = kk >= g.nz - 3 ? g.nz : kk;
         }
-        sets_.allocate(kSets * 9 * n * sizeof(Real));
-        for (int s = 0; s < kSets; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * 9 * n;
+        if (g.mechanisms < 0 || g.mechanisms > 3) throw Error(SWL_ERR_INVALID, "3D GSLS needs 0..3 mechanisms");
+        if (g.mechanisms) { // GSLS: the strengths, and 6 memory fields per mechanism beside the nine
+            for (int l = 0; l < g.mechanisms; ++l) {
+                if (!g.delta_p[l] || !g.delta_s[l] || !(g.rates[l] > 0)) throw Error(SWL_ERR_INVALID, "3D GSLS needs rates and strengths");
+                m_.rates[l] = static_cast<Real>(g.rates[l]);
+                m_.dP[l] = upload(conv(g.delta_p[l]));
+                m_.dS[l] = upload(conv(g.delta_s[l]));
+            }
+            m_.mech = g.mechanisms;
+        }
+        fc_ = 9 + 6 * g.mechanisms;
+        sets_.allocate(kSets * std::size_t(fc_) * n * sizeof(Real));
+        for (int s = 0; s < kSets; ++s) set_[s] = sets_.as<Real>() + std::size_t(s) * fc_ * n;
         if (g.cpml_count) { // CFS-PML slabs (swl_mesh3d)
             const int NX = g.nx - 6, NY = g.ny - 6, NZ = g.nz - 6;
             if (g.cpml_width_x < 0 || g.cpml_width_y < 0 || g.cpml_width_z < 0 || 2 * g.cpml_width_x > NX ||
@@ -655,7 +667,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             for (long long q = 0; q < pcount_; ++q) out[q] = double(tmp[q]);
             return;
         }
-        if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "snapshot field out of range");
+        if (field < 0 || field >= fc_) throw Error(SWL_ERR_INVALID, "snapshot field out of range");
         check(cudaStreamSynchronize(stream_), "snapshot ordering");
         std::vector<Real> tmp(count_);
         check(cudaMemcpy(tmp.data(), set_[u_] + std::size_t(field) * count_, count_ * sizeof(Real), cudaMemcpyDeviceToHost),
@@ -677,7 +689,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
             previous_ = false;
             return;
         }
-        if (field < 0 || field >= 9) throw Error(SWL_ERR_INVALID, "load field out of range");
+        if (field < 0 || field >= fc_) throw Error(SWL_ERR_INVALID, "load field out of range");
         clockStats_ = false;
         check(cudaStreamSynchronize(stream_), "load ordering");
         std::vector<Real> tmp(count_, Real(0));

@@ -107,6 +107,7 @@ Model2D buildModel2D(const Params2D &);
 // ------------------------------------------------------------------------- 3D parameters
 struct Layer3D {
     double thickness{}, vp{}, vs{}, density{};
+    double qp{-1}, qs{-1}; // GSLS quality factors of the layer (< 0: the session's attenuation.qp/qs)
 };
 struct SurfaceGrid3D {
     int nx{}, ny{};
@@ -144,6 +145,9 @@ struct Params3D {
     // in the reference's 3D path; the 2D profiles of src/two_d/CfsPml2D.hpp:31-41 per axis)
     int absorber{0};
     double cpmlReflection{1e-4}, cpmlKappaMax{3}, cpmlFrequency{};
+    // GSLS viscoelasticity (no counterpart in the reference's 3D path; the 2D fit and relaxation of
+    // src/common/Gsls.cpp and src/two_d/PointKernels2D.hpp:161-168 with all six stress components)
+    GslsSettings attenuation;
     int receiverLimit{1024}; // the reference caps traces at 1024; the engine has no such limit
     // FP64 node geometry built on this CUDA device (-1: the largest) instead of on the host
     bool deviceGeometry{false};
@@ -168,6 +172,12 @@ struct Model3D {
     std::int64_t cpmlCount{};
     std::vector<double> cpmlShape; // wx, wy, wz, memory count (as model array "cpmlShape")
     double cpmlDt{};
+    // GSLS: mechanisms (0: elastic), relaxation rates, per-node strengths, dt bound
+    int mechanisms{};
+    std::array<double, 3> rates{};
+    std::vector<double> deltaP[3], deltaS[3];
+    std::vector<double> gslsRates; // the `mechanisms` rates (as model array "gslsRates")
+    double relaxationDt{}, maxRelativeQError{};
     std::vector<std::int64_t> receiverNodes;
     std::vector<std::array<double, 3>> receiverPositions;
 };

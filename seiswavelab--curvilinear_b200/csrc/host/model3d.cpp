@@ -254,11 +254,43 @@ Model3D buildModel3D(const Params3D &p) {
     require(std::isfinite(g.lambda) && std::isfinite(g.mu) && g.mu > 0 && std::isfinite(maxMetricNorm),
             "Derived elastic coefficients or grid metrics are out of range.");
     double maxVp = p.vp, minVs = p.vs;
-    if (p.layered) { // include/Seis3D/MaterialModels3D.hpp:19-31
+    // GSLS: one fit per layer (or for the uniform model); the moduli become the unrelaxed ones
+    validateGsls(p.attenuation);
+    const int L = p.attenuation.enabled ? p.attenuation.mechanisms : 0;
+    std::vector<GslsMaterial> rheology;
+    if (L) {
+        auto q = [&](double v, double fallback) { return v >= 0 ? v : fallback; };
+        if (p.layered)
+            for (const auto &l : p.layers)
+                rheology.push_back(fitGsls(l.vp, l.vs, l.density, q(l.qp, p.attenuation.qp), q(l.qs, p.attenuation.qs), p.attenuation));
+        else
+            rheology.push_back(fitGsls(p.vp, p.vs, p.density, p.attenuation.qp, p.attenuation.qs, p.attenuation));
+        g.mechanisms = L;
+        g.rates = rheology.front().rates;
+        g.gslsRates.assign(g.rates.begin(), g.rates.begin() + L);
+        for (int l = 0; l < L; ++l) g.deltaP[l].assign(count, 0), g.deltaS[l].assign(count, 0);
+        for (const auto &r : rheology) g.maxRelativeQError = std::max(g.maxRelativeQError, r.maxRelativeQError);
+        g.relaxationDt = .25 / g.rates[L - 1];
+    } else {
+        g.relaxationDt = std::numeric_limits<double>::max();
+    }
+    if (p.layered || L) { // include/Seis3D/MaterialModels3D.hpp:19-31 (uniform: one layer)
+        const std::vector<Layer3D> uniform{Layer3D{0, p.vp, p.vs, p.density}};
+        const auto &layers = p.layered ? p.layers : uniform;
         maxVp = 0, minVs = std::numeric_limits<double>::max();
-        for (const auto &l : p.layers) maxVp = std::max(maxVp, l.vp), minVs = std::min(minVs, l.vs);
+        for (std::size_t l = 0; l < layers.size(); ++l) {
+            maxVp = std::max(maxVp, L ? std::sqrt(rheology[l].pUnrelaxed / layers[l].density) : layers[l].vp);
+            minVs = std::min(minVs, L ? std::sqrt(rheology[l].sRelaxed / layers[l].density) : layers[l].vs);
+        }
         g.materialLambda.resize(count), g.materialMu.resize(count), g.materialDensity.resize(count);
         for (std::size_t q = 0; q < count; ++q) {
+            if (!p.layered) { // uniform model with GSLS: the fitted unrelaxed moduli everywhere
+                const auto &r = rheology.front();
+                g.materialLambda[q] = r.pUnrelaxed - 2 * r.sUnrelaxed, g.materialMu[q] = r.sUnrelaxed;
+                g.materialDensity[q] = p.density;
+                for (int l = 0; l < L; ++l) g.deltaP[l][q] = r.deltaP[l], g.deltaS[l][q] = r.deltaS[l];
+                continue;
+            }
             double depth;
             if (p.layerDepthMode == 0) depth = (static_cast<int>(q / plane) - ghost) * dz;
             else if (p.layerDepthMode == 2) depth = g.coordinates[3 * q + 2];
@@ -276,6 +308,11 @@ Model3D buildModel3D(const Params3D &p) {
             g.materialLambda[q] = l.density * (l.vp * l.vp - 2 * l.vs * l.vs);
             g.materialMu[q] = l.density * l.vs * l.vs;
             g.materialDensity[q] = l.density;
+            if (L) {
+                const auto &r = rheology[id];
+                g.materialLambda[q] = r.pUnrelaxed - 2 * r.sUnrelaxed, g.materialMu[q] = r.sUnrelaxed;
+                for (int k = 0; k < L; ++k) g.deltaP[k][q] = r.deltaP[k], g.deltaS[k][q] = r.deltaS[k];
+            }
         }
     }
     // sponge (include/Seis3D/AbsorbingBoundary3D.hpp:6-21)
@@ -320,7 +357,7 @@ Model3D buildModel3D(const Params3D &p) {
     g.waveDt = p.cfl * std::min(p.spacing / maxMetricNorm, minLength) / maxVp;
     g.dampingDt = maxDamping > 0 ? .5 / maxDamping : std::numeric_limits<double>::max();
     g.sourceDt = 1 / (50 * p.frequency);
-    const double safe = std::min({g.waveDt, g.dampingDt, g.sourceDt, g.cpmlDt});
+    const double safe = std::min({g.waveDt, g.dampingDt, g.sourceDt, g.cpmlDt, g.relaxationDt});
     const double durationSteps = std::max(1.0, std::ceil(p.duration / safe));
     require(std::isfinite(durationSteps) && !(p.maxSteps == 0 && durationSteps > 20000),
             "Time-step limit: at most 20,000 steps. Set a maximum step cap.");

@@ -56,7 +56,9 @@ int64_t estimate(const Shot &s) {
     const double b = p.precision == SWL_FP32 ? 4 : 8, sets = p.precision == SWL_FP32 ? 6 : 4;
     const double receivers = double(std::max(1, p.receiverCountX)) * std::max(1, p.receiverCountY);
     const double traces = receivers * std::min(p.maxSteps, host::maxBatch) * 3 * 8;
-    return int64_t(n * b * (sets * 9 + 9 + 5 + (p.layered ? 3 : 0) + (p.sourceKind == 1 ? 3 : 0)) + traces + allowance);
+    const int L = p.attenuation.enabled ? p.attenuation.mechanisms : 0; // GSLS: 6 memory fields and 2 strengths each
+    const double material = (p.layered || L) ? 3 : 0;
+    return int64_t(n * b * (sets * (9 + 6 * L) + 9 + 5 + material + 2 * L + (p.sourceKind == 1 ? 3 : 0)) + traces + allowance);
 }
 
 class Server {

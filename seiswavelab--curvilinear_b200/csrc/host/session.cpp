@@ -196,6 +196,9 @@ void swl3d_params_default(swl_params3d *c) {
     c->absorbing_strength = p.absorbingStrength;
     c->absorber = p.absorber;
     c->cpml_reflection = p.cpmlReflection, c->cpml_kappa_max = p.cpmlKappaMax, c->cpml_frequency = p.cpmlFrequency;
+    c->attenuation = p.attenuation.enabled, c->mechanisms = p.attenuation.mechanisms;
+    c->q_min_frequency = p.attenuation.minFrequency, c->q_max_frequency = p.attenuation.maxFrequency;
+    c->q_reference_frequency = p.attenuation.referenceFrequency, c->qp = p.attenuation.qp, c->qs = p.attenuation.qs;
 }
 swl_status swl3d_session_create(const swl_params3d *c, int32_t device, swl3d_session **out) {
     return guard([&] {

@@ -281,6 +281,9 @@ struct Session3D {
             }
             m.source_amplitude = model.sourceAmplitude;
             m.precision = params.precision;
+            m.mechanisms = model.mechanisms;
+            for (int l = 0; l < model.mechanisms; ++l)
+                m.rates[l] = model.rates[l], m.delta_p[l] = model.deltaP[l].data(), m.delta_s[l] = model.deltaS[l].data();
             if (model.cpmlCount) {
                 m.cpml_x = model.cpmlX.data(), m.cpml_y = model.cpmlY.data(), m.cpml_z = model.cpmlZ.data();
                 m.cpml_width_x = model.cpmlWidth[0], m.cpml_width_y = model.cpmlWidth[1], m.cpml_width_z = model.cpmlWidth[2];
@@ -367,7 +370,11 @@ struct Session3D {
         if (n == "cpmlY") return &m.cpmlY;
         if (n == "cpmlZ") return &m.cpmlZ;
         if (n == "cpmlShape") return &m.cpmlShape;
-        if (n == "cpmlShape") return &m.cpmlShape;
+        if (n == "gslsRates") return &m.gslsRates;
+        for (int l = 0; l < 3; ++l) {
+            if (n == "deltaP" + std::to_string(l)) return &m.deltaP[l];
+            if (n == "deltaS" + std::to_string(l)) return &m.deltaS[l];
+        }
         for (int a = 0; a < 3; ++a)
             if (n == "sourceGradient" + std::to_string(a)) return &m.sourceGradient[a];
         return nullptr;
@@ -399,6 +406,11 @@ inline Params3D toParams(const swl_params3d &c) {
     p.absorbingStrength = c.absorbing_strength;
     p.absorber = c.absorber;
     p.cpmlReflection = c.cpml_reflection, p.cpmlKappaMax = c.cpml_kappa_max, p.cpmlFrequency = c.cpml_frequency;
+    p.attenuation.enabled = c.attenuation != 0, p.attenuation.mechanisms = c.mechanisms;
+    p.attenuation.minFrequency = c.q_min_frequency, p.attenuation.maxFrequency = c.q_max_frequency;
+    p.attenuation.referenceFrequency = c.q_reference_frequency, p.attenuation.qp = c.qp, p.attenuation.qs = c.qs;
+    if (c.layer_q)
+        for (int l = 0; l < c.n_layers; ++l) p.layers[l].qp = c.layer_q[2 * l], p.layers[l].qs = c.layer_q[2 * l + 1];
     p.deviceGeometry = c.device_geometry != 0;
     if (c.layer_names)
         for (int l = 0; l < c.n_layers; ++l) p.layerNames.push_back(c.layer_names[l] ? c.layer_names[l] : "");

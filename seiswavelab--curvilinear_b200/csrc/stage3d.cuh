@@ -49,6 +49,11 @@ template <class Real> struct Mesh {
     int cpml;
     int wx, wy, wz;
     const Real *cpx, *cpy, *cpz;
+    // GSLS (this library's 3D extension of the 2D relaxation, src/two_d/PointKernels2D.hpp:161-168):
+    // mech mechanisms, whose memories (xx, yy, zz, xy, xz, yz) are fields 9 + 6l .. 14 + 6l
+    int mech;
+    Real rates[3];
+    const Real *dP[3], *dS[3];
 };
 
 using k2::Clock;
@@ -89,25 +94,31 @@ template <class Real> __device__ __forceinline__ void cpmlSlots3(const Mesh<Real
     slot[2] = kc >= NZ - m.wz ? c0 + c1 + 6 * (((long long)(kc - (NZ - m.wz)) * NY + jc) * NX + ic) : -1;
 }
 
-// RK combine of one memory value (the fields' scheme, finish3).
-template <class Real, int STAGE> __device__ __forceinline__ void combineMemory3(const StageArgs<Real> &p, long long at, Real r) {
-    const Real u = (STAGE < 3 || k2::kahan<Real>()) ? k2::ld(p.pbase + at) : Real(0);
+// RK combine of one value of a set (the fields' scheme, finish3): base, acc, out and the FP32
+// compensation in and out.  Used for the CFS-PML memories and the GSLS memory fields.
+template <class Real, int STAGE>
+__device__ __forceinline__ void combineValue3(const StageArgs<Real> &p, const Real *base, Real *acc, Real *out, const Real *cin,
+                                              Real *cout, long long at, Real r) {
+    const Real u = (STAGE < 3 || k2::kahan<Real>()) ? k2::ld(base + at) : Real(0);
     if (STAGE == 0) {
-        p.pacc[at] = k2::kahan<Real>() ? p.w6 * r : u + p.w6 * r;
-        p.pout[at] = u + p.weight * r;
+        acc[at] = k2::kahan<Real>() ? p.w6 * r : u + p.w6 * r;
+        out[at] = u + p.weight * r;
     } else if (STAGE < 3) {
-        const Real a = p.pacc[at];
-        p.pacc[at] = a + p.w3 * r;
-        p.pout[at] = u + p.weight * r;
+        const Real a = acc[at];
+        acc[at] = a + p.w3 * r;
+        out[at] = u + p.weight * r;
     } else if constexpr (k2::kahan<Real>()) {
-        const Real a = p.pacc[at], c = k2::ld(p.pcin + at);
+        const Real a = acc[at], c = k2::ld(cin + at);
         const Real y = (a + p.w6 * r) - c;
         const Real o = u + y;
-        p.pcout[at] = (o - u) - y;
-        p.pacc[at] = o;
+        cout[at] = (o - u) - y;
+        acc[at] = o;
     } else {
-        p.pacc[at] = p.pacc[at] + p.w6 * r;
+        acc[at] = acc[at] + p.w6 * r;
     }
+}
+template <class Real, int STAGE> __device__ __forceinline__ void combineMemory3(const StageArgs<Real> &p, long long at, Real r) {
+    combineValue3<Real, STAGE>(p, p.pbase, p.pacc, p.pout, p.pcin, p.pcout, at, r);
 }
 
 using k2::ld;
@@ -324,7 +335,8 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
 
     // CFS-PML: the node's memory slots and the rates of its memories
     long long slot[3] = {-1, -1, -1};
-    if constexpr (CPML) cpmlSlots3(m, i, j, k, slot);
+    if constexpr (CPML)
+        if (m.cpml) cpmlSlots3(m, i, j, k, slot);
     const bool split = CPML && (slot[0] >= 0 || slot[1] >= 0 || slot[2] >= 0);
     Real prate[3][6];
     auto stretchAxis = [&](int a, int f, Real d) -> Real {
@@ -355,6 +367,15 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) t[a] += ((a == b ? lam * trace : Real(0)) + mu * (g[3 * a + b] + g[3 * b + a])) * c[b];
+        if constexpr (CPML) { // GSLS: the memory stresses' traction (the 2D surfaceDerivative's, PointKernels2D.hpp:84)
+            const int T[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+            for (int l = 0; l < m.mech; ++l) {
+                const Real *mw = w + (9 + 6 * l) * n + q;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    t[a] -= (ld(mw + T[a][0] * n) * c[0] + ld(mw + T[a][1] * n) * c[1]) + ld(mw + T[a][2] * n) * c[2];
+            }
+        }
         const Real normal = t[0] * nn[0] + t[1] * nn[1] + t[2] * nn[2];
 #pragma unroll
         for (int a = 0; a < 3; ++a) dzs[a] = -(t[a] - nn[a] * normal) / (mu * c2) - nn[a] * normal / ((lam + 2 * mu) * c2);
@@ -426,7 +447,28 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
     r[6] = mu * (gr[0][1] + gr[1][0]);
     r[7] = mu * (gr[0][2] + gr[2][0]);
     r[8] = mu * (gr[1][2] + gr[2][1]);
-    if (!(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1)) {
+    const bool damped = !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1);
+    if constexpr (CPML) { // GSLS: the stresses subtract the memories; memory rate = rate (drive - memory)
+        for (int l = 0; l < m.mech; ++l) {
+            const long long mm = (9 + 6 * l) * n + q;
+            const Real dp = ld(m.dP[l] + q), ds = ld(m.dS[l] + q), dl = dp - 2 * ds;
+            const Real drive[6] = {dl * div + 2 * ds * gr[0][0], dl * div + 2 * ds * gr[1][1], dl * div + 2 * ds * gr[2][2],
+                                   ds * (gr[0][1] + gr[1][0]),  ds * (gr[0][2] + gr[2][0]),  ds * (gr[1][2] + gr[2][1])};
+            Real wm[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) wm[c] = ld(w + mm + c * n);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) r[3 + c] -= wm[c];
+            const Real d = damped ? ld(m.damping + q) : Real(0);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                Real rm = m.rates[l] * (drive[c] - wm[c]);
+                if (damped) rm -= d * wm[c];
+                combineValue3<Real, STAGE>(p, p.base, p.acc, STAGE < 3 ? p.out : p.acc, p.cin, p.cout, mm + c * n, rm);
+            }
+        }
+    }
+    if (damped) {
         const Real d = ld(m.damping + q);
 #pragma unroll
         for (int f = 0; f < 9; ++f) r[f] -= d * ld(w + f * n + q);
@@ -524,8 +566,9 @@ __device__ __forceinline__ void stageNode3(const StageArgs<Real> &p, bool genera
 // One RK stage of a 3D shot: block 32x8 nodes of one z layer.  CTAs on the surface rows or on
 // the source support run the general form; the others run the interior form, with the damping
 // term when the CTA reaches into the sponge (so the sponge costs nine multiply-adds, not the
-// general form).  CPML: the mesh has CFS-PML slabs; their CTAs run the general form with the ADE
-// terms.  Meshes without them launch the CPML = false kernels, which hold none of that code.
+// general form).  CPML: the mesh has CFS-PML slabs or GSLS memories; slab CTAs (every CTA with
+// GSLS) run the general form with those terms.  Plain meshes launch the CPML = false kernels, which
+// hold none of that code.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool CPML>
 __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __grid_constant__ StageArgs<Real> p) {
     const Mesh<Real> &m = p.m;
@@ -536,8 +579,8 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __gri
     const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
     const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
     // CTAs reaching into a CFS-PML slab run the general form (it holds the ADE terms)
-    const bool slab = CPML && (i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || j0 - 3 < m.wy || j1 - 3 > m.ny - 6 - m.wy ||
-                               k - 3 >= m.nz - 6 - m.wz);
+    const bool slab = CPML && (m.mech > 0 || (m.cpml && (i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || j0 - 3 < m.wy ||
+                                                      j1 - 3 > m.ny - 6 - m.wy || k - 3 >= m.nz - 6 - m.wz)));
     const bool general = surface || source || slab;
     if constexpr (sizeof(Real) == 4) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);
     else if (m.hinvExact) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);

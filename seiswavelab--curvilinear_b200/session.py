@@ -77,6 +77,9 @@ class Params3D(C.Structure):
         ("device_geometry", C.c_int32), ("layer_names", C.POINTER(C.c_char_p)),
         ("absorber", C.c_int32), ("cpml_reflection", C.c_double), ("cpml_kappa_max", C.c_double),
         ("cpml_frequency", C.c_double),
+        ("attenuation", C.c_int32), ("mechanisms", C.c_int32),
+        *[(k, C.c_double) for k in ("q_min_frequency", "q_max_frequency", "q_reference_frequency", "qp", "qs")],
+        ("layer_q", _dp),
     ]
 
 
@@ -165,7 +168,9 @@ _MAP3D = {
     "cfl": "cfl", "relief": "relief", "wavelength": "wavelength", "flattenDepth": "flatten_depth",
     "absorbing": "absorbing", "absorbingStrength": "absorbing_strength", "receiverLimit": "receiver_limit",
     "deviceGeometry": "device_geometry", "absorber": "absorber", "cpmlReflection": "cpml_reflection",
-    "cpmlKappaMax": "cpml_kappa_max", "cpmlFrequency": "cpml_frequency",
+    "cpmlKappaMax": "cpml_kappa_max", "cpmlFrequency": "cpml_frequency", "attenuation": "attenuation",
+    "mechanisms": "mechanisms", "qMinFrequency": "q_min_frequency", "qMaxFrequency": "q_max_frequency",
+    "qReferenceFrequency": "q_reference_frequency", "qp": "qp", "qs": "qs",
 }
 
 
@@ -211,10 +216,17 @@ def params3d(params: dict):
         for a in range(3):
             p.source_direction[a] = float(params["sourceDirection"][a])
     if "layers" in params:
-        rows = np.asarray(params["layers"], dtype=np.float64).reshape(-1, 4)
-        arr = (Layer3D * len(rows))(*[Layer3D(*r) for r in rows])
+        # rows of (thickness, vp, vs, density), or of six with the layer's GSLS qp, qs
+        flat = np.asarray(params["layers"], dtype=np.float64)
+        cols = 6 if params.get("layerColumns", 4) == 6 else 4
+        rows = flat.reshape(-1, cols)
+        arr = (Layer3D * len(rows))(*[Layer3D(*r[:4]) for r in rows])
         keep.append(arr)
         p.layers, p.n_layers = arr, len(rows)
+        if cols == 6:
+            q = np.ascontiguousarray(rows[:, 4:6]).ravel()
+            keep.append(q)
+            p.layer_q = q.ctypes.data_as(_dp)
     if "layerNames" in params:
         names = (C.c_char_p * len(params["layerNames"]))(*[n.encode() for n in params["layerNames"]])
         keep.append(names)
@@ -414,7 +426,8 @@ def read_model3d(path):
         _check(L.swl3d_model_document_params(h, C.byref(p), C.byref(c), C.byref(dt)))
         out = {k: getattr(p, f) for k, f in _MAP3D.items()
                if k not in ("deviceGeometry", "precision", "receiverLimit", "absorber", "cpmlReflection", "cpmlKappaMax",
-                            "cpmlFrequency")}
+                            "cpmlFrequency", "attenuation", "mechanisms", "qMinFrequency", "qMaxFrequency",
+                            "qReferenceFrequency", "qp", "qs")}
         out["sourceDirection"] = list(p.source_direction)
         out["layers"] = [[p.layers[i].thickness, p.layers[i].vp, p.layers[i].vs, p.layers[i].density]
                          for i in range(p.n_layers)]

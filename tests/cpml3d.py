@@ -21,6 +21,11 @@ def mesh_from_session(S, sim, params):
         v = sim.model(k)
         if v.size:
             m[k] = v
+    rates = sim.model("gslsRates")
+    if rates.size:  # GSLS: mechanisms, rates and strengths
+        m["mechanisms"], m["rates"] = int(rates.size), rates.tolist()
+        for l in range(rates.size):
+            m[f"deltaP{l}"], m[f"deltaS{l}"] = sim.model(f"deltaP{l}"), sim.model(f"deltaS{l}")
     shape = sim.model("cpmlShape")
     if shape.size and shape[3] > 0:
         m.update(cpmlX=sim.model("cpmlX"), cpmlY=sim.model("cpmlY"), cpmlZ=sim.model("cpmlZ"), cpmlWidthX=int(shape[0]),
