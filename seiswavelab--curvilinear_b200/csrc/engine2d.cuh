@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -149,6 +150,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
     // state / accumulator sets 0-1 and of their compensation sets 4-5, model words without / with J
     CUtensorMap ringMap_[4]{}, pwMap_[2]{}, compMap_[2]{}, modelMap_[2]{};
     CUtensorMap gslsIn_[4]{}, gslsComp_[2]{}, strengthMap_{}; // GSLS L2 prefetch boxes (per set)
+    int gslsLead_{2}; // GSLS prefetch lead in row blocks (SWL_GSLS_PREFETCH overrides: 0 off, 1, 2, 3)
     DeviceBuffer strengths_;
     // Sets 0-1: state / accumulator (roles u_, a_); 2-3: stage states; FP32 only, 4-5: the Kahan
     // compensation of sets 0-1 (set 4 + r compensates set r, so a role swap moves both).
@@ -229,7 +231,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
                 p.gslsAMap = gslsIn_[a_];
                 p.gslsCompMap = gslsComp_[u_];
                 p.strengthMap = strengthMap_;
-                p.gslsPrefetch = 1;
+                p.gslsPrefetch = gslsLead_;
             }
         }
         return p;
@@ -440,6 +442,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
         // GSLS relaxation strengths: one allocation of 2L pitched arrays (dP0, dS0, dP1, ...), so one
         // tensor box covers a row block's strengths
         if (mech_) strengths_.allocate(2 * std::size_t(mech_) * n * sizeof(Real));
+        if (const char *e = std::getenv("SWL_GSLS_PREFETCH")) gslsLead_ = std::clamp(std::atoi(e), 0, 3);
         for (int l = 0; l < mech_; ++l) {
             m_.rates[l] = static_cast<Real>(g.rates[l]);
             Real *dp = strengths_.as<Real>() + std::size_t(2 * l) * n, *ds = dp + n;

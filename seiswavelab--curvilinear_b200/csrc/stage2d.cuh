@@ -98,8 +98,9 @@ template <class Real> struct StageArgs {
     // GSLS only: the per-node words the node arithmetic reads from global memory -- Syy and the
     // 4L memories of the stage input, of U and of A (and their FP32 compensation), and the 2L
     // relaxation strengths -- as 32x8x(4L+1) and 32x8x2L boxes.  The CTA's copy thread prefetches a
-    // row block's boxes into L2 with the tensor copies of its stencil rows, two blocks ahead of the
-    // arithmetic, so the per-node loads hit L2 instead of waiting on DRAM.  gslsPrefetch = 0: off.
+    // row block's boxes into L2, so the per-node loads hit L2 instead of waiting on DRAM:
+    // gslsPrefetch = 2 with the block's tensor copies (two blocks ahead of its arithmetic), 3 with the
+    // copies of the block before it (three ahead), 1 when the block before it starts (one ahead), 0 off.
     CUtensorMap gslsInMap, gslsUMap, gslsAMap, gslsCompMap, strengthMap;
     int gslsPrefetch;
 };
@@ -713,6 +714,14 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
     const int iEnd = m.nx - 3, kEnd = m.nz - 3;
     const int blocks = min(m.seg, (kEnd - z0 + SB - 1) / SB);
     __shared__ int stop;
+    // thread 0: L2 prefetch of row block g's GSLS words (x of the word boxes: node i0)
+    auto prefetchGsls = [&](int g) {
+        const int x = i0 + m.xoff, y = z0 + SB * g;
+        tmaPrefetch3(&p.gslsInMap, x, y, 0);
+        if (STAGE > 0) tmaPrefetch3(&p.gslsUMap, x, y, 0), tmaPrefetch3(&p.gslsAMap, x, y, 0);
+        if (STAGE == 3 && kahan<Real>()) tmaPrefetch3(&p.gslsCompMap, x, y, 0);
+        tmaPrefetch3(&p.strengthMap, x, y, 0);
+    };
     // thread 0: issue copy group g (x of the ring box: node i0 - 4; of the word boxes: node i0)
     auto issue = [&](int g) {
         uint64_t *b = bar + (g & 1);
@@ -727,12 +736,8 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
         }
         tmaLoad3(dst + PW_a * T, &p.modelMap, x, y, 0, b);
         if (STAGE == 3 && kahan<Real>()) tmaLoad3(dst + PW_C * T, &p.compMap, x, y, 0, b);
-        if (MECH > 0 && p.gslsPrefetch) {
-            tmaPrefetch3(&p.gslsInMap, x, y, 0);
-            if (STAGE > 0) tmaPrefetch3(&p.gslsUMap, x, y, 0), tmaPrefetch3(&p.gslsAMap, x, y, 0);
-            if (STAGE == 3 && kahan<Real>()) tmaPrefetch3(&p.gslsCompMap, x, y, 0);
-            tmaPrefetch3(&p.strengthMap, x, y, 0);
-        }
+        if (MECH > 0 && p.gslsPrefetch == 2) prefetchGsls(g);
+        if (MECH > 0 && p.gslsPrefetch == 3 && g + 1 < blocks) prefetchGsls(g + 1);
     };
     if (tid == 0) {
         stop = 0;
@@ -755,6 +760,7 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
         __syncthreads();
         if (stop) break;
         waited = blk + 1;
+        if (MECH > 0 && p.gslsPrefetch == 1 && tid == 0 && blk + 1 < blocks) prefetchGsls(blk + 1); // one block ahead
         const int k = z0 + blk * SB + wy, i = i0 + lane;
         if (k < kEnd && i < iEnd) {
             StreamNode<Real, EXACT, STAGE> s;
