@@ -567,12 +567,24 @@ def gpu_arm(args):
     if not args.no_fp32:
         sim32, r32 = measure(1)
         del sim32
-    base = parity = None
+    base = parity = parity_long = None
     if rank == 0 and world == 1 and not args.no_cpu:
         base, ref_run = cpu_baseline(r64["params"], dim, args.cpu_steps, 1, keep=True)
         if ref_run is not None:
             parity = error_vs_reference(S, r64["params"], dim, ref_run, local)
             del ref_run
+        if args.parity_steps > 0:
+            # a run long enough for the waves to cross the grid (the headline shot's 7 steps reach only the
+            # source's neighbourhood): the 500x200 plain workload, the reference CPU solver on all threads
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import oracle as O
+            import importlib
+            W = importlib.import_module("swl_b200.workloads")
+            pp = W.plain_small(precision=0, steps=args.parity_steps)
+            ref_long = O.run_reference_2d(pp, steps=args.parity_steps, threads=min(64, os.cpu_count() or 1), dump_mesh=False)
+            parity_long = error_vs_reference(S, pp, 2, ref_long, local)
+            parity_long["workload"] = "plain_small (500x200 h=2, 20-cell CFS-PML, surface force)"
+            del ref_long
     ref_gpu = None
     if rank == 0 and world == 1 and dim == 2 and not args.no_ref_gpu:
         ref_gpu = reference_gpu(r64["params"], args.ref_gpu_steps, 2)
@@ -594,6 +606,7 @@ def gpu_arm(args):
                        "init_s": round(r64["init_s"], 3)},
             "roofline": r64["roofline"], "e2e": e2e, "gpu_launches": int(args.steps * r64["profile"]["launches_per_step"]),
             "clocks": r64["clocks"], "cpu_baseline": base, "error_vs_reference": parity,
+            "error_vs_reference_long": parity_long,
         }
         if r32:
             line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],
@@ -642,6 +655,8 @@ def main():
                     choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d", "elastic_3d_cpml",
                              "small_3d"])
     ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
+    ap.add_argument("--parity-steps", type=int, default=600,
+                    help="steps of the long parity run against the reference (500x200 plain workload; 0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA engine")
     ap.add_argument("--ref-gpu-steps", type=int, default=10, help="timed steps of the reference CUDA engine")
