@@ -95,6 +95,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     bool previous_{false};
     int nrec_{}, traceCap_{}, forcingCap_{};
     dim3 grid_, block_{32, 8, 1};
+    dim3 statsGrid_; // stats3d: CTAs of 32 x 8 columns over k3::STATS_LAYERS z layers
     int nparts_{};
     k2::Clock hostClock_{};
     PinnedBuffer pinnedForcing_, pinnedClock_, pinnedTraces_;
@@ -182,7 +183,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         check(cudaGetLastError(), "3D stage launch");
         if (verdict) {
             Real *fresh = set_[a_];
-            k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, fresh, surfRate_.as<double>(), clock_.as<k2::Clock>(),
+            k3::stats3d<Real><<<statsGrid_, block_, 0, stream_>>>(m_, fresh, surfRate_.as<double>(), clock_.as<k2::Clock>(),
                                                              partials_.as<k3::Partial>());
             if (ev) check(cudaEventRecord(ev[5], stream_), "record event");
             k3::verdict3d<Real><<<1, 512, 0, stream_>>>(partials_.as<k3::Partial>(), nparts_, fresh, count_,
@@ -400,7 +401,8 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
         grid_ = dim3((g.nx - 6 + 31) / 32, (g.ny - 6 + 7) / 8, g.nz - 6);
-        nparts_ = grid_.x * grid_.y * grid_.z;
+        statsGrid_ = dim3(grid_.x, grid_.y, (g.nz - 6 + k3::STATS_LAYERS - 1) / k3::STATS_LAYERS);
+        nparts_ = statsGrid_.x * statsGrid_.y * statsGrid_.z;
         partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
         clock_.allocate(sizeof(k2::Clock));
         pinnedClock_.reserve(sizeof(k2::Clock));
@@ -587,7 +589,7 @@ template <class Real> class TypedEngine3D final : public Engine3D {
     void diagnostics(swl_diag3d &d) override {
         settle();
         DeviceScope scope(device_);
-        k3::stats3d<Real><<<grid_, block_, 0, stream_>>>(m_, set_[u_], surfRate_.as<double>(), nullptr, partials_.as<k3::Partial>());
+        k3::stats3d<Real><<<statsGrid_, block_, 0, stream_>>>(m_, set_[u_], surfRate_.as<double>(), nullptr, partials_.as<k3::Partial>());
         check(cudaGetLastError(), "3D diagnostics");
         std::vector<k3::Partial> parts(nparts_);
         check(cudaMemcpyAsync(parts.data(), partials_.ptr, parts.size() * sizeof(k3::Partial), cudaMemcpyDeviceToHost, stream_),

@@ -175,11 +175,12 @@ template <class Real> __device__ __forceinline__ Real divBy(Real x, Real d, Real
 constexpr int SW = 32, SB = 8, MAX_SEG = 8, CHUNKS = 3, RC = SW + 8, RF = SB * RC, CH = 5 * RF;
 constexpr int RING = CHUNKS * SB, STREAM_THREADS = SW * SB;
 enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15, PW_C = 16 };
-// per-node words: U, A, five model words and J, plus the five compensation terms in FP32
-template <class Real> constexpr int pwWords() { return kahan<Real>() ? PW_C + 5 : PW_C; }
+// per-node words: U, A, five model words and J, plus the five compensation terms of the last FP32
+// stage (the only one that reads them)
+template <class Real, int STAGE = 3> constexpr int pwWords() { return kahan<Real>() && STAGE == 3 ? PW_C + 5 : PW_C; }
 // two mbarriers, then the ring and the two word buffers (128-byte aligned), plus alignment slack
-template <class Real> constexpr std::size_t streamBytes() {
-    return 128 + sizeof(Real) * (CHUNKS * CH + 2 * pwWords<Real>() * STREAM_THREADS) + 128;
+template <class Real, int STAGE = 3> constexpr std::size_t streamBytes() {
+    return 128 + sizeof(Real) * (CHUNKS * CH + 2 * pwWords<Real, STAGE>() * STREAM_THREADS) + 128;
 }
 
 template <class Real, bool EXACT, int STAGE> struct StreamNode {
@@ -680,8 +681,12 @@ __device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int 
                  : "memory");
 }
 
-// Resident CTAs per SM allowed by shared memory: 2 x 101.8 KB (FP64), 3 x 61 KB (FP32).
-template <class Real> constexpr int streamBlocks() { return sizeof(Real) == 8 ? 2 : 3; }
+// Resident CTAs per SM: 2 x 101.8 KB of shared memory in FP64.  FP32: 3 x 61 KB in the last stage
+// (it also stages the compensation terms); 4 x 51 KB in the others, which then hold 64 registers
+// (elastic: GSLS stages keep three CTAs and their 80 registers).
+template <class Real, int STAGE = 3, int MECH = 0> constexpr int streamBlocks() {
+    return sizeof(Real) == 8 ? 2 : STAGE < 3 && MECH == 0 ? 4 : 3;
+}
 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
 // strips, the sponge, the source support and the surface rows 3..6).  The host evaluates the
@@ -704,7 +709,7 @@ __device__ __forceinline__ void mbarInval(uint64_t *bar) {
 template <class Real, int DX, int DZ, int MECH, int STAGE, bool EXACT, bool FULL>
 __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *bar, Real *ring, Real *pw, int bx, int by, int slot,
                                            bool reinit) {
-    constexpr int T = STREAM_THREADS, PW = pwWords<Real>();
+    constexpr int T = STREAM_THREADS, PW = pwWords<Real, STAGE>();
     constexpr unsigned S = sizeof(Real);
     constexpr unsigned chunkBytes = S * CH, fiveBytes = S * 5 * T, modelBytes = S * (STAGE == 3 ? 6 : 5) * T;
     constexpr unsigned wordBytes = (STAGE > 0 ? 2 * fiveBytes : 0) + modelBytes + (STAGE == 3 && kahan<Real>() ? fiveBytes : 0);
@@ -807,7 +812,7 @@ __device__ __forceinline__ bool streamTile(const StageArgs<Real> &p, uint64_t *b
 // The streaming stage: grid (strips of 32 columns, segments of 64 rows), block 32x8.  DX/DZ:
 // MacCormack directions of this (step, stage); MECH: GSLS mechanisms (0: elastic); STAGE: 0..3.
 template <class Real, int DX, int DZ, int MECH, int STAGE>
-__global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real>())) stream2d(const __grid_constant__ StageArgs<Real> p) {
+__global__ void __launch_bounds__(STREAM_THREADS, (streamBlocks<Real, STAGE, MECH>())) stream2d(const __grid_constant__ StageArgs<Real> p) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     if (p.clock->faulted) return; // uniform across the grid
     unsigned char *base = smemRaw + ((128 - (smemAddr(smemRaw) & 127)) & 127);

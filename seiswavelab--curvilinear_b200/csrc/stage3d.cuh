@@ -593,60 +593,86 @@ struct Partial {
     int bad, pad;
 };
 
+// One partial per CTA from the per-thread diagnostics: warp shuffles, then the CTA's warps in order.
+__device__ __forceinline__ void reducePartial3(Partial s, Partial *out, int slot) {
+    for (int o = 16; o > 0; o >>= 1) {
+        s.energy += __shfl_down_sync(0xffffffffu, s.energy, o);
+        s.velocity = fmax(s.velocity, __shfl_down_sync(0xffffffffu, s.velocity, o));
+        s.rateTraction = fmax(s.rateTraction, __shfl_down_sync(0xffffffffu, s.rateTraction, o));
+        s.rateNorm = fmax(s.rateNorm, __shfl_down_sync(0xffffffffu, s.rateNorm, o));
+#pragma unroll
+        for (int c = 0; c < 5; ++c) s.peak[c] = fmax(s.peak[c], __shfl_down_sync(0xffffffffu, s.peak[c], o));
+        s.bad |= __shfl_down_sync(0xffffffffu, s.bad, o);
+    }
+    __shared__ Partial warps[8];
+    const int t = threadIdx.x + blockDim.x * threadIdx.y, lane = t & 31, wid = t >> 5, nw = (blockDim.x * blockDim.y) >> 5;
+    if (lane == 0) warps[wid] = s;
+    __syncthreads();
+    if (t == 0) {
+        Partial tot = warps[0];
+        for (int w = 1; w < nw; ++w) {
+            const Partial &y = warps[w];
+            tot.energy += y.energy;
+            tot.velocity = fmax(tot.velocity, y.velocity);
+            tot.rateTraction = fmax(tot.rateTraction, y.rateTraction);
+            tot.rateNorm = fmax(tot.rateNorm, y.rateNorm);
+            for (int c = 0; c < 5; ++c) tot.peak[c] = fmax(tot.peak[c], y.peak[c]);
+            tot.bad |= y.bad;
+        }
+        out[slot] = tot;
+    }
+}
+
 // Energy, peaks, finiteness and the traction-rate residual of a state
-// (src/three_d/CurvilinearSolver.cpp:214-250, CudaEngine3D.cu:36-55).
+// (src/three_d/CurvilinearSolver.cpp:214-250, CudaEngine3D.cu:36-55), one partial per CTA of 32 x 8
+// columns over STATS_LAYERS z layers (fewer partials for the one-block verdict to read).  Each
+// thread issues the thirteen loads of a node (nine fields, lambda, mu, rho, J) ahead of its
+// arithmetic; the CTA reduces by warp shuffles.
+constexpr int STATS_LAYERS = 8;
 template <class Real>
 __global__ void __launch_bounds__(256) stats3d(const Mesh<Real> m, const Real *__restrict__ w, const double *__restrict__ surfRate,
                                                const Clock *clk, Partial *out) {
-    __shared__ Partial sh[256];
-    const int t = threadIdx.x + blockDim.x * threadIdx.y;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = 3 + blockIdx.z;
+    const int k0 = 3 + blockIdx.z * STATS_LAYERS;
     Partial s{};
     if (i < m.nx - 3 && j < m.ny - 3 && !(clk && clk->faulted)) {
-        const long long n = m.count, q = i + (long long)m.px * j + m.plane * k;
-        double f[9];
-        for (int c = 0; c < 9; ++c) {
-            f[c] = double(ld(w + c * n + q));
-            if (!isfinite(f[c])) s.bad = 1;
-        }
-        const double lam = m.mlambda ? double(ld(m.mlambda + q)) : double(m.lambda);
-        const double mu = m.mmu ? double(ld(m.mmu + q)) : double(m.mu);
-        const double rho = m.mdensity ? double(ld(m.mdensity + q)) : double(m.density);
-        const double v2 = f[0] * f[0] + f[1] * f[1] + f[2] * f[2];
-        s.velocity = sqrt(v2);
-        s.peak[0] = fabs(f[2]), s.peak[1] = fabs(f[0]), s.peak[2] = fabs(f[1]), s.peak[3] = sqrt(v2);
-        s.peak[4] = fabs((f[3] + f[4] + f[5]) / 3.0);
-        const double mean = (f[3] + f[4] + f[5]) / 3;
-        double dev = 0;
-        for (int c = 0; c < 3; ++c) dev += (f[c + 3] - mean) * (f[c + 3] - mean);
-        for (int c = 6; c < 9; ++c) dev += 2 * f[c] * f[c];
+        const long long n = m.count;
         const double hh = double(m.h);
-        s.energy = (0.5 * rho * v2 + dev / (4 * mu) + mean * mean / (2 * (lam + 2 * mu / 3))) * double(ld(m.jac + q)) * hh * hh * hh;
-        if (!isfinite(s.energy)) s.bad = 1;
-        if (k == 3 && surfRate) {
+        for (int k = k0; k < k0 + STATS_LAYERS && k < m.nz - 3; ++k) {
+            const long long q = i + (long long)m.px * j + m.plane * k;
+            double f[9];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) f[c] = double(ld(w + c * n + q));
+            const double lam = m.mlambda ? double(ld(m.mlambda + q)) : double(m.lambda);
+            const double mu = m.mmu ? double(ld(m.mmu + q)) : double(m.mu);
+            const double rho = m.mdensity ? double(ld(m.mdensity + q)) : double(m.density);
+            const double jac = double(ld(m.jac + q));
+#pragma unroll
+            for (int c = 0; c < 9; ++c)
+                if (!isfinite(f[c])) s.bad = 1;
+            const double v2 = f[0] * f[0] + f[1] * f[1] + f[2] * f[2], v = sqrt(v2);
+            const double mean = (f[3] + f[4] + f[5]) / 3;
+            s.velocity = fmax(s.velocity, v);
+            s.peak[0] = fmax(s.peak[0], fabs(f[2])), s.peak[1] = fmax(s.peak[1], fabs(f[0]));
+            s.peak[2] = fmax(s.peak[2], fabs(f[1])), s.peak[3] = fmax(s.peak[3], v);
+            s.peak[4] = fmax(s.peak[4], fabs((f[3] + f[4] + f[5]) / 3.0));
+            double dev = 0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) dev += (f[c + 3] - mean) * (f[c + 3] - mean);
+#pragma unroll
+            for (int c = 6; c < 9; ++c) dev += 2 * f[c] * f[c];
+            const double e = (0.5 * rho * v2 + dev / (4 * mu) + mean * mean / (2 * (lam + 2 * mu / 3))) * jac * hh * hh * hh;
+            if (!isfinite(e)) s.bad = 1;
+            s.energy += e;
+        }
+        if (k0 == 3 && surfRate) {
             const long long sq = i + (long long)m.px * j;
             s.rateTraction = surfRate[sq];
             s.rateNorm = surfRate[m.plane + sq];
         }
     }
-    sh[t] = s;
-    __syncthreads();
-    for (int stride = 128; stride > 0; stride >>= 1) {
-        if (t < stride) {
-            Partial &x = sh[t];
-            const Partial y = sh[t + stride];
-            x.energy += y.energy;
-            x.velocity = fmax(x.velocity, y.velocity);
-            x.rateTraction = fmax(x.rateTraction, y.rateTraction);
-            x.rateNorm = fmax(x.rateNorm, y.rateNorm);
-            for (int c = 0; c < 5; ++c) x.peak[c] = fmax(x.peak[c], y.peak[c]);
-            x.bad |= y.bad;
-        }
-        __syncthreads();
-    }
-    if (t == 0) out[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = sh[0];
+    reducePartial3(s, out, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
 }
 
 struct Clock3 {

@@ -12,7 +12,7 @@
 namespace swl::detail2 {
 namespace {
 template <class Real, int MECH, int DX, int DZ, int ST> void go(dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
-    k2::stream2d<Real, DX, DZ, MECH, ST><<<g, b, k2::streamBytes<Real>(), s>>>(a);
+    k2::stream2d<Real, DX, DZ, MECH, ST><<<g, b, k2::streamBytes<Real, ST>(), s>>>(a);
 }
 template <class Real, int MECH, int DX, int DZ> void stages(int stage, dim3 g, dim3 b, cudaStream_t s, const k2::StageArgs<Real> &a) {
     switch (stage) {
@@ -22,15 +22,15 @@ template <class Real, int MECH, int DX, int DZ> void stages(int stage, dim3 g, d
     default: go<Real, MECH, DX, DZ, 3>(g, b, s, a); break;
     }
 }
-template <class Real, class K> void allow(K kernel) {
-    check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k2::streamBytes<Real>())),
+template <class Real, int ST, class K> void allow(K kernel) {
+    check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k2::streamBytes<Real, ST>())),
           "2D stage shared memory");
     check(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared)),
           "2D stage shared-memory carveout");
 }
 template <class Real, int MECH, int DX, int DZ> void allowStages() {
-    allow<Real>(k2::stream2d<Real, DX, DZ, MECH, 0>), allow<Real>(k2::stream2d<Real, DX, DZ, MECH, 1>);
-    allow<Real>(k2::stream2d<Real, DX, DZ, MECH, 2>), allow<Real>(k2::stream2d<Real, DX, DZ, MECH, 3>);
+    allow<Real, 0>(k2::stream2d<Real, DX, DZ, MECH, 0>), allow<Real, 1>(k2::stream2d<Real, DX, DZ, MECH, 1>);
+    allow<Real, 2>(k2::stream2d<Real, DX, DZ, MECH, 2>), allow<Real, 3>(k2::stream2d<Real, DX, DZ, MECH, 3>);
 }
 } // namespace
 
