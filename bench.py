@@ -71,6 +71,9 @@ def workload(name: str, precision: int) -> tuple[dict, str]:
     if name == "elastic_3d_cpml":
         return (W.elastic_3d(precision=precision, absorber=1),
                 "3D nine-field elastic 400x288x200 h=10 m, DEM terrain, 3 layers, 20-cell CFS-PML slabs")
+    if name == "gsls_3d":
+        return (W.elastic_3d(precision=precision, mechanisms=3),
+                "3D GSLS (3 mechanisms, 27 fields) 400x288x200 h=10 m, DEM terrain, 3 layers, 20-cell sponge")
     if name == "small_3d":
         return (W.elastic_3d(precision=precision, nx=200, ny=144, nz=100),
                 "3D nine-field elastic 200x144x100 (profiling size of elastic_3d)")
@@ -513,7 +516,7 @@ def gpu_arm(args):
     swl = load_package()
     import importlib
     S = importlib.import_module("swl_b200.session")
-    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "small_3d") else 2
+    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "gsls_3d", "small_3d") else 2
     Sim = S.Simulation2D if dim == 2 else S.Simulation3D
     peak, peak_src = measured_hbm_peak()
 
@@ -610,7 +613,8 @@ def gpu_arm(args):
         }
         if r32:
             line["fp32"] = {"value": r32["value"], "unit": UNIT, "ms_per_step": r32["ms_per_step"],
-                            "roofline": r32["roofline"], "speedup_vs_fp64": r32["value"] / r64["value"]}
+                            "roofline": r32["roofline"], "speedup_vs_fp64": r32["value"] / r64["value"],
+                            "profile": r32["profile"]}
         if ref_gpu:
             line["reference_gpu"] = ref_gpu
         if serving:
@@ -629,7 +633,7 @@ def reference_arm(args):
     if rank != 0:
         return
     load_package()
-    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "small_3d") else 2
+    dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "gsls_3d", "small_3d") else 2
     params, desc = workload(args.workload, 0)
     steps = min(args.steps, args.cpu_steps)
     base = cpu_baseline(params, dim, steps, min(args.warmup, 2))
@@ -653,7 +657,7 @@ def main():
     ap.add_argument("--impl", choices=["swl", "reference"], default="swl")
     ap.add_argument("--workload", default="curvilinear_large",
                     choices=["curvilinear_large", "small", "plain_small", "gsls_medium", "elastic_3d", "elastic_3d_cpml",
-                             "small_3d"])
+                             "gsls_3d", "small_3d"])
     ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the reference CPU sample")
     ap.add_argument("--parity-steps", type=int, default=600,
                     help="steps of the long parity run against the reference (500x200 plain workload; 0: skip)")

@@ -118,12 +118,14 @@ def grf_dem(nx: int, ny: int, spacing: float, correlation: float, relief: float,
 
 
 def elastic_3d(precision: int = 0, steps: int = 1500, nx: int = 400, ny: int = 288, nz: int = 200,
-               receivers: int = 40, relief: float = 150.0, flatten_depth: float = 800.0, absorber: int = 0) -> dict:
+               receivers: int = 40, relief: float = 150.0, flatten_depth: float = 800.0, absorber: int = 0,
+               mechanisms: int = 0) -> dict:
     """400x288x200 3D elastic, h=10 m, DEM terrain (seed 4, correlation 500 m, relief 150 m on a
     25 m lattice), blend depth 800 m, layers 200 m / 600 m / basement below the surface, 15 Hz
     explosive source 5 nodes deep, 20-cell sponge, 40x40 areal surface receivers.  Reduced grids
     need a smaller relief and blend depth (the blend must fit the model depth and exceed 2.6 times
-    the relief)."""
+    the relief).  `absorber` 1: 20-cell CFS-PML slabs instead of the sponge; `mechanisms` > 0: GSLS
+    viscoelasticity with that many mechanisms (Qp 100, Qs 60 over 2.5-37.5 Hz, referenced at 15 Hz)."""
     h = 10.0
     dem_dx = 25.0
     dnx = int(np.ceil((nx - 1) * h / dem_dx)) + 1
@@ -139,7 +141,9 @@ def elastic_3d(precision: int = 0, steps: int = 1500, nx: int = 400, ny: int = 2
                 absorbing=1, absorbingCells=[20, 20, 20], absorbingStrength=3.0, absorber=int(absorber),
                 receiverArray=[3, (nx - (receivers - 1) * sx) // 2, (ny - (receivers - 1) * sy) // 2, 0,
                                receivers, receivers, sx, sy],
-                receiverLimit=receivers * receivers)
+                receiverLimit=receivers * receivers,
+                **(dict(attenuation=1, mechanisms=int(mechanisms), qMinFrequency=2.5, qMaxFrequency=37.5,
+                        qReferenceFrequency=15.0, qp=100.0, qs=60.0) if mechanisms > 0 else {}))
 
 
 def serving_mix(n: int = 256, rate: float = 20.0, seed: int = 5, scale: float = 1.0, steps_scale: float = 1.0) -> list:
