@@ -500,7 +500,7 @@ __device__ __forceinline__ void stageBody3(const StageArgs<Real> &p) {
 // r0 = (gxx,x + gxy,y) + gxz,z, r1 = (gxy,x + gyy,y) + gyz,z, r2 = (gxz,x + gyz,y) + gzz,z
 // (src/three_d/PointKernels3D.hpp:92-112), so only a few gradients are live at a time.  The
 // damping term is subtracted after all nine rates, as in the general form.
-template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool DAMP>
+template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool DAMP, bool GSLS>
 __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
     const Mesh<Real> &m = p.m;
     const int i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -536,6 +536,27 @@ __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
         r[6] = mu * (gv[0][1] + gv[1][0]);
         r[7] = mu * (gv[0][2] + gv[2][0]);
         r[8] = mu * (gv[1][2] + gv[2][1]);
+        if constexpr (GSLS) { // the general form's relaxation, with the same operations in the same order
+            const bool damped = DAMP && !(i >= m.dmp_i0 && i < m.dmp_i1 && j >= m.dmp_j0 && j < m.dmp_j1 && k < m.dmp_k1);
+            for (int l = 0; l < m.mech; ++l) {
+                const long long mm = (9 + 6 * l) * n + q;
+                const Real dp = ld(m.dP[l] + q), ds = ld(m.dS[l] + q), dl = dp - 2 * ds;
+                const Real drive[6] = {dl * div + 2 * ds * gv[0][0], dl * div + 2 * ds * gv[1][1], dl * div + 2 * ds * gv[2][2],
+                                       ds * (gv[0][1] + gv[1][0]),  ds * (gv[0][2] + gv[2][0]),  ds * (gv[1][2] + gv[2][1])};
+                Real wm[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c) wm[c] = ld(w + mm + c * n);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) r[3 + c] -= wm[c];
+                const Real d = damped ? ld(m.damping + q) : Real(0);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    Real rm = m.rates[l] * (drive[c] - wm[c]);
+                    if (damped) rm -= d * wm[c];
+                    combineValue3<Real, STAGE>(p, p.base, p.acc, STAGE < 3 ? p.out : p.acc, p.cin, p.cout, mm + c * n, rm);
+                }
+            }
+        }
     }
     {
         Real g[3], m0, m1, m2, t41, t52, t70;
@@ -559,16 +580,19 @@ __device__ __forceinline__ void stageInterior3(const StageArgs<Real> &p) {
 template <class Real, int DX, int DY, int DZ, int STAGE, bool EXACT, bool CPML>
 __device__ __forceinline__ void stageNode3(const StageArgs<Real> &p, bool general, bool sponge) {
     if (general) stageBody3<Real, DX, DY, DZ, STAGE, EXACT, CPML>(p);
-    else if (sponge) stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, true>(p);
-    else stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, false>(p);
+    else if (CPML && p.m.mech > 0) { // GSLS outside the CFS-PML slabs
+        if (sponge) stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, true, CPML>(p);
+        else stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, false, CPML>(p);
+    } else if (sponge) stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, true, false>(p);
+    else stageInterior3<Real, DX, DY, DZ, STAGE, EXACT, false, false>(p);
 }
 
 // One RK stage of a 3D shot: block 32x8 nodes of one z layer.  CTAs on the surface rows or on
 // the source support run the general form; the others run the interior form, with the damping
 // term when the CTA reaches into the sponge (so the sponge costs nine multiply-adds, not the
-// general form).  CPML: the mesh has CFS-PML slabs or GSLS memories; slab CTAs (every CTA with
-// GSLS) run the general form with those terms.  Plain meshes launch the CPML = false kernels, which
-// hold none of that code.
+// general form).  CPML: the mesh has CFS-PML slabs or GSLS memories; CTAs that reach into a slab
+// run the general form with the ADE terms, and with GSLS the interior form carries the relaxation
+// too.  Plain meshes launch the CPML = false kernels, which hold none of that code.
 template <class Real, int DX, int DY, int DZ, int STAGE, bool CPML>
 __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __grid_constant__ StageArgs<Real> p) {
     const Mesh<Real> &m = p.m;
@@ -579,8 +603,8 @@ __global__ void __launch_bounds__(256, (minBlocks3<Real>())) stage3d(const __gri
     const bool source = i0 < m.src_i1 && i1 > m.src_i0 && j0 < m.src_j1 && j1 > m.src_j0 && k >= m.src_k0 && k < m.src_k1;
     const bool sponge = !(i0 >= m.dmp_i0 && i1 <= m.dmp_i1 && j0 >= m.dmp_j0 && j1 <= m.dmp_j1 && k < m.dmp_k1);
     // CTAs reaching into a CFS-PML slab run the general form (it holds the ADE terms)
-    const bool slab = CPML && (m.mech > 0 || (m.cpml && (i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || j0 - 3 < m.wy ||
-                                                      j1 - 3 > m.ny - 6 - m.wy || k - 3 >= m.nz - 6 - m.wz)));
+    const bool slab = CPML && m.cpml &&
+                      (i0 - 3 < m.wx || i1 - 3 > m.nx - 6 - m.wx || j0 - 3 < m.wy || j1 - 3 > m.ny - 6 - m.wy || k - 3 >= m.nz - 6 - m.wz);
     const bool general = surface || source || slab;
     if constexpr (sizeof(Real) == 4) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);
     else if (m.hinvExact) stageNode3<Real, DX, DY, DZ, STAGE, true, CPML>(p, general, sponge);
