@@ -7,6 +7,7 @@
 #include "stage3d.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <vector>
@@ -400,7 +401,12 @@ template <class Real> class TypedEngine3D final : public Engine3D {
         }
         recIdx_.allocate(std::max(1, nrec) * sizeof(long long));
         if (nrec) check(cudaMemcpy(recIdx_.ptr, idx.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice), "upload receivers");
-        grid_ = dim3((g.nx - 6 + 31) / 32, (g.ny - 6 + 7) / 8, g.nz - 6);
+        // CTA shape: 256 nodes of one z layer, 32 x 8 unless SWL_3D_BLOCK names another width (16, 64 or 128)
+        if (const char *e = std::getenv("SWL_3D_BLOCK")) {
+            const int bx = std::atoi(e);
+            if (bx == 16 || bx == 32 || bx == 64 || bx == 128) block_ = dim3(bx, 256 / bx, 1);
+        }
+        grid_ = dim3((g.nx - 6 + block_.x - 1) / block_.x, (g.ny - 6 + block_.y - 1) / block_.y, g.nz - 6);
         statsGrid_ = dim3(grid_.x, grid_.y, (g.nz - 6 + k3::STATS_LAYERS - 1) / k3::STATS_LAYERS);
         nparts_ = statsGrid_.x * statsGrid_.y * statsGrid_.z;
         partials_.allocate(std::size_t(nparts_) * sizeof(k3::Partial));
