@@ -321,7 +321,10 @@ def time_engine(swl, sim, dim, params, steps, warmup, torch, dist, rank):
     else:
         swl._check(L.swl3d_profile(eng, step, 8, dt, f, C.byref(prof)))
     swl._check(set_stream(eng, None))
-    return ms, prof.as_dict()
+    out = prof.as_dict()
+    if dim == 2:
+        out["layout"] = swl.layout2d(eng)  # strip width, rows per block, the tuned segment, interior CTAs
+    return ms, out
 
 
 def serving_leg(args, device: int) -> dict:

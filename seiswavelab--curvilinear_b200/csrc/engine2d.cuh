@@ -543,7 +543,9 @@ template <class Real> class TypedEngine2D final : public Engine2D {
             }
         } else {
             // Each candidate is timed as an 8-step CUDA graph, the form a batch runs in: timing eager
-            // steps would measure the host's launch gaps, which dominate a small grid's step.
+            // steps would measure the host's launch gaps, which dominate a small grid's step.  The
+            // best of three replays counts, so that a clock ramp or a neighbour's burst during one
+            // replay does not decide the segment.
             cudaEvent_t e0{}, e1{};
             check(cudaEventCreate(&e0), "create event");
             check(cudaEventCreate(&e1), "create event");
@@ -552,13 +554,17 @@ template <class Real> class TypedEngine2D final : public Engine2D {
                 setSegment(seg);
                 launch(0, 8, 1e-6, 10.0, 0.0, 0.3); // records this segment's graph (and loads modules)
                 finish();
-                check(cudaEventRecord(e0, stream_), "record event");
-                launch(0, 8, 1e-6, 10.0, 0.0, 0.3);
-                check(cudaEventRecord(e1, stream_), "record event");
-                finish();
-                check(cudaEventSynchronize(e1), "tuning completion");
                 float ms = 0;
-                check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+                for (int rep = 0; rep < 3; ++rep) {
+                    check(cudaEventRecord(e0, stream_), "record event");
+                    launch(0, 8, 1e-6, 10.0, 0.0, 0.3);
+                    check(cudaEventRecord(e1, stream_), "record event");
+                    finish();
+                    check(cudaEventSynchronize(e1), "tuning completion");
+                    float one = 0;
+                    check(cudaEventElapsedTime(&one, e0, e1), "event time");
+                    ms = rep == 0 ? one : std::min(ms, one);
+                }
                 if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
             }
             cudaEventDestroy(e0);

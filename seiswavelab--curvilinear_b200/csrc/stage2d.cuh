@@ -186,7 +186,12 @@ constexpr int RING = CHUNKS * SB, STREAM_THREADS = SW * SB;
 enum : int { PW_U = 0, PW_A = 5, PW_a = 10, PW_b = 11, PW_lam = 12, PW_mu = 13, PW_rho = 14, PW_jac = 15, PW_C = 16 };
 // per-node words: U, A, five model words and J, plus the five compensation terms of the last FP32
 // stage (the only one that reads them)
-template <class Real, int STAGE = 3> constexpr int pwWords() { return kahan<Real>() && STAGE == 3 ? PW_C + 5 : PW_C; }
+// Stage 0 takes U from the ring and J from global memory, so it stages only the five model words
+// a, b, lambda, mu, rho: its buffers start at word PW_a.
+template <int STAGE> constexpr int firstWord() { return STAGE == 0 ? PW_a : 0; }
+template <class Real, int STAGE = 3> constexpr int pwWords() {
+    return STAGE == 0 ? PW_rho + 1 - PW_a : kahan<Real>() && STAGE == 3 ? PW_C + 5 : PW_C;
+}
 // two mbarriers, then the ring and the two word buffers (128-byte aligned), plus alignment slack
 template <class Real, int STAGE = 3> constexpr std::size_t streamBytes() {
     return 128 + sizeof(Real) * (CHUNKS * CH + 2 * pwWords<Real, STAGE>() * STREAM_THREADS) + 128;
@@ -221,7 +226,7 @@ template <class Real, bool EXACT, int STAGE> struct StreamNode {
         const unsigned u = unsigned(s);
         return col[(u / unsigned(SB)) * CH + f * RF + (u % unsigned(SB)) * RC + dx];
     }
-    __device__ __forceinline__ Real word(int w) const { return pw[w * STREAM_THREADS]; }
+    __device__ __forceinline__ Real word(int w) const { return pw[(w - firstWord<STAGE>()) * STREAM_THREADS]; }
     __device__ __forceinline__ Real u(const StageArgs<Real> &, int f) const { return STAGE == 0 ? at(f, 0, 0) : word(PW_U + f); }
     __device__ __forceinline__ Real acc(const StageArgs<Real> &, int f) const { return word(PW_A + f); }
     __device__ __forceinline__ Real comp(const StageArgs<Real> &, int f) const { return word(PW_C + f); }
@@ -690,11 +695,12 @@ __device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int 
                  : "memory");
 }
 
-// Resident CTAs per SM: 2 x 101.8 KB of shared memory in FP64.  FP32: 3 x 61 KB in the last stage
-// (it also stages the compensation terms); 4 x 51 KB in the others, which then hold 64 registers
-// (elastic: GSLS stages keep three CTAs and their 80 registers).
+// Resident CTAs per SM.  FP64: 2 x 101.8 KB of shared memory; elastic stage 0 (five model words
+// staged) 3 x 59 KB at 80 registers.  FP32: 3 x 61 KB in the last stage (it also stages the
+// compensation terms); 4 x 51 KB in the others, which then hold 64 registers (elastic: GSLS stages
+// keep three CTAs and their 80 registers).
 template <class Real, int STAGE = 3, int MECH = 0> constexpr int streamBlocks() {
-    return sizeof(Real) == 8 ? 2 : STAGE < 3 && MECH == 0 ? 4 : 3;
+    return sizeof(Real) == 8 ? (STAGE == 0 && MECH == 0 ? 3 : 2) : STAGE < 3 && MECH == 0 ? 4 : 3;
 }
 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
@@ -748,7 +754,7 @@ __device__ __forceinline__ bool streamBody(const StageArgs<Real> &p, uint64_t *b
             tmaLoad3(dst + PW_U * T, &p.uMap, x, y, 0, b);
             tmaLoad3(dst + PW_A * T, &p.aMap, x, y, 0, b);
         }
-        tmaLoad3(dst + PW_a * T, &p.modelMap, x, y, 0, b);
+        tmaLoad3(dst + (PW_a - firstWord<STAGE>()) * T, &p.modelMap, x, y, 0, b);
         if (STAGE == 3 && kahan<Real>()) tmaLoad3(dst + PW_C * T, &p.compMap, x, y, 0, b);
         if (MECH > 0 && p.gslsPrefetch == 2) prefetchGsls(g);
         if (MECH > 0 && p.gslsPrefetch == 3 && g + 1 < blocks) prefetchGsls(g + 1);
