@@ -565,7 +565,7 @@ template <class Real> class TypedEngine2D final : public Engine2D {
                     check(cudaEventElapsedTime(&one, e0, e1), "event time");
                     ms = rep == 0 ? one : std::min(ms, one);
                 }
-                if (seg == k2::MAX_SEG || ms < 0.97 * bestMs) best = seg, bestMs = ms; // shorter only if clearly faster
+                if (seg == k2::MAX_SEG || ms < 0.99 * bestMs) best = seg, bestMs = ms; // shorter only if faster by 1 %
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);

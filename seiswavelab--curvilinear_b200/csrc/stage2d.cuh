@@ -695,12 +695,12 @@ __device__ __forceinline__ void tmaLoad3(void *dst, const CUtensorMap *map, int 
                  : "memory");
 }
 
-// Resident CTAs per SM.  FP64: 2 x 101.8 KB of shared memory; elastic stage 0 (five model words
-// staged) 3 x 59 KB at 80 registers.  FP32: 3 x 61 KB in the last stage (it also stages the
-// compensation terms); 4 x 51 KB in the others, which then hold 64 registers (elastic: GSLS stages
-// keep three CTAs and their 80 registers).
+// Resident CTAs per SM.  FP64: 2 x 101.8 KB of shared memory; stage 0 (five model words staged)
+// 3 x 59 KB at 80 registers.  FP32: 3 x 61 KB in the last stage (it also stages the compensation
+// terms); 4 x 51 KB in the others, which then hold 64 registers (elastic: GSLS stages keep three
+// CTAs and their 80 registers).
 template <class Real, int STAGE = 3, int MECH = 0> constexpr int streamBlocks() {
-    return sizeof(Real) == 8 ? (STAGE == 0 && MECH == 0 ? 3 : 2) : STAGE < 3 && MECH == 0 ? 4 : 3;
+    return sizeof(Real) == 8 ? (STAGE == 0 ? 3 : 2) : STAGE < 3 && MECH == 0 ? 4 : 3;
 }
 
 // Whether every node of the CTA's strip and segment is an interior node (outside the CFS-PML
