@@ -1,4 +1,4 @@
-"""Model build on the terrain inputs the BASELINE workloads use, against the reference's own CPU
+"""Model build on the terrain inputs the benchmark workloads use, against the reference's own CPU
 solver run live (oracle/_ref, built from its sources; no GPU needed).
 
 * 2D imported surface: samples of a seeded terrain profile interpolated by PCHIP

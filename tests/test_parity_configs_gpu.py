@@ -1,4 +1,4 @@
-"""The BASELINE workloads on the GPU against the reference's own CPU solver, run live.
+"""The benchmark workloads on the GPU against the reference's own CPU solver, run live.
 
 The reference is oracle/_ref (compiled from its sources by oracle/Makefile; it travels with the
 repository, the reference checkout does not).  The golden fixtures of the other tests are small
