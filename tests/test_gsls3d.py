@@ -76,3 +76,21 @@ def test_lower_q_attenuates_more(S, orc):
         st, _ = orc.run3d(mesh_from_session(S, sim, params), steps)
         energy[name] = float(np.sum(st[:3] ** 2))
     assert energy["q20"] < 0.8 * energy["q200"] and energy["q200"] < energy["elastic"] * 1.05, energy
+
+
+def test_benchmark_workload_builds_with_three_mechanisms(S):
+    # the 3D GSLS benchmark workload (bench.py --workload gsls_3d) at a reduced grid: three relaxation
+    # rates, a strength per node and mechanism, and the relaxation bound in the dt plan
+    W = importlib.import_module("swl_b200.workloads")
+    p = W.elastic_3d(mechanisms=3, nx=40, ny=36, nz=30, relief=10.0, flatten_depth=100.0, receivers=8)
+    sim = S.Simulation3D(p, device=S.MODEL_ONLY)
+    rates = sim.model("gslsRates")
+    assert rates.size == 3 and np.all(np.diff(rates) > 0)
+    count = 46 * 42 * 36  # padded grid: three ghost nodes either side
+    for l in range(3):
+        assert sim.model(f"deltaP{l}").size == count and sim.model(f"deltaS{l}").size == count
+        assert np.all(sim.model(f"deltaS{l}") >= 0)
+    assert sim.info()["dt"] <= 0.25 / rates[-1]
+    elastic = S.Simulation3D(W.elastic_3d(nx=40, ny=36, nz=30, relief=10.0, flatten_depth=100.0, receivers=8),
+                             device=S.MODEL_ONLY)
+    assert elastic.model("gslsRates").size == 0
