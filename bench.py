@@ -198,6 +198,7 @@ def cpu_baseline(params: dict, dim: int, steps: int, warmup: int, keep: bool = F
     pts = float(np.prod([int(r[k]) - 6 for k in (("nx", "nz") if dim == 2 else ("nx", "ny", "nz"))]))
     sec = float(r["runMs"]) / 1e3
     base = {"value": pts * steps / sec / 1e6, "unit": UNIT, "cores": int(r["threads"]), "kind": "reference",
+            "ms_per_step": float(r["msPerStep"]),
             "sample": f"{steps} timed steps after {warmup} warm-up of the same shot (reference CPU solver, FP64, "
                       f"{int(r['threads'])} OpenMP threads); {float(r['msPerStep']):.1f} ms/step, init {float(r['initMs'])/1e3:.1f} s"}
     return (base, r) if keep else base
@@ -639,13 +640,14 @@ def reference_arm(args):
     dim = 3 if args.workload in ("elastic_3d", "elastic_3d_cpml", "gsls_3d", "small_3d") else 2
     params, desc = workload(args.workload, 0)
     steps = min(args.steps, args.cpu_steps)
-    base = cpu_baseline(params, dim, steps, min(args.warmup, 2))
+    warm = min(args.warmup, 3)  # untimed steps before the sample (a CPU step of the 5001x2001 shot is ~0.9 s)
+    base = cpu_baseline(params, dim, steps, warm)
     if base is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver binaries (oracle/_ref) are not built"}))
         return
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": 0, "steps": steps,
-        "warmup": min(args.warmup, 2), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "warmup": warm, "ms_per_step": base["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded terrain/layers/sources, PCG64)",
         "config": {"workload": args.workload, "description": desc, "precision": "fp64 plain"},
         "cpu_baseline": base, "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
